@@ -1,0 +1,428 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 iSVD hot path (one JSON line on rank 0).
+
+Workload (default): the plain-FP64-at-scale configuration -- A = U_r diag(sigma)
+V_r' + 1e-4 G with m = 100000, n = 20000 (16 GB FP64, row-major), r = 200,
+sigma_j = exp(-j/30); k = 50, p = 14 (l = 64), N = 64 sketches (sketch GEMM
+100000 x 20000 x 4096); Gramian orthogonalizer, row-block Gramian
+Kolmogorov-Nagumo integrator (tol 1e-6, at most 256 iterations), row-block
+Gramian former.  A step is one whole solve (Omega drawn on the device, sketch,
+orthogonalize, integrate, form) with A resident in HBM.  Synthetic data
+(seeded; no dataset exists for this path).  A (16 GB) is larger than L2, so no
+flush is needed between steps.
+
+Arms:
+  default            this build (libmcnla_b200.so); value = iSVD/s over all ranks
+  --impl reference   the reference's own CPU stages (oracle/_ref, built from the
+                     reference sources; the numpy restatement when absent) on a
+                     bounded row sample of the same workload, all host threads
+N > 1 runs independent replicas (one solve per GPU per step, no collective in
+the data path: the one-GPU solve does not shard); torch.distributed is used for
+the barrier and the max-over-ranks time only.
+"""
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "iSVD/s & A-read GB/s, mixed vs FP64 plain on B200 at σ err≤1e-6; p50/p99 ms"
+
+# dram bytes (read + write) per launch of the sketch GEMM from one ncu capture
+# of a 16384 x 20000 x 4096 case scaled by rows to m = 100000 (profiles/
+# dgemm_sketch_c2.md); None until captured.
+SKETCH_TRAFFIC_PER_ROW = None
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--m", type=int, default=100000)
+    ap.add_argument("--n", type=int, default=20000)
+    ap.add_argument("--k", type=int, default=50)
+    ap.add_argument("--p", type=int, default=14)
+    ap.add_argument("--N", type=int, default=64)
+    ap.add_argument("--rank-r", type=int, default=200)
+    ap.add_argument("--integrator", default="rb_gramian_kn")
+    ap.add_argument("--former", default="rb_gramian")
+    ap.add_argument("--tol", type=float, default=1e-6)
+    ap.add_argument("--maxit", type=int, default=256)
+    ap.add_argument("--colmajor", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-rows", type=int, default=0, help="row sample of the CPU baseline (0: auto)")
+    ap.add_argument("--quick", action="store_true", help="small shape for a smoke run")
+    args = ap.parse_args()
+    if args.quick:
+        args.m, args.n, args.k, args.p, args.N, args.rank_r = 8192, 4096, 16, 8, 16, 64
+    return args
+
+
+def workload(args):
+    l = args.k + args.p
+    return {
+        "workload": "plain FP64 iSVD, A = U diag(exp(-j/30)) V' + 1e-4 G, m=%d n=%d r=%d, k=%d p=%d N=%d"
+                    % (args.m, args.n, args.rank_r, args.k, args.p, args.N),
+        "m": args.m, "n": args.n, "k": args.k, "p": args.p, "l": l, "N": args.N,
+        "sketch_gemm": "%dx%dx%d" % (args.m, args.n, l * args.N),
+        "stages": "GaussianProjection(device Philox) / Gramian / %s (tol %g, maxit %d) / %s"
+                  % (args.integrator, args.tol, args.maxit, args.former),
+        "layout": "column-major" if args.colmajor else "row-major",
+        "l2": "inputs larger than L2 (A is %.1f GB)" % (args.m * args.n * 8 / 1e9),
+    }
+
+
+# ------------------------------------------------------------------------------------------------
+# distributed plumbing
+# ------------------------------------------------------------------------------------------------
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        if args.impl == "b200":
+            torch.cuda.set_device(local)
+        dist.init_process_group("nccl" if args.impl == "b200" else "gloo",
+                                timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ------------------------------------------------------------------------------------------------
+# clocks
+# ------------------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ["clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.hw_slowdown",
+              "clocks_event_reasons.hw_thermal_slowdown", "clocks_event_reasons.sw_thermal_slowdown",
+              "clocks_event_reasons.sw_power_cap"]
+
+    def __init__(self, device_index):
+        import torch
+        self.proc = None
+        try:
+            uuid = "GPU-" + str(torch.cuda.get_device_properties(device_index).uuid)
+        except Exception:
+            uuid = str(device_index)
+        self.cmd = ["nvidia-smi", "-i", uuid, "--query-gpu=" + ",".join(self.FIELDS),
+                    "--format=csv,noheader,nounits", "-lms", "200"]
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(self.cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            return None
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) != len(self.FIELDS):
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------------------------------
+# this build
+# ------------------------------------------------------------------------------------------------
+def fp64_peak_tflops():
+    """cuBLAS DGEMM throughput on this GPU (the FP64 roofline denominator; no FP64
+    figure is in the measured-peaks file).  Best of 5 at 8192^3, after warm-up."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    c = a @ b
+    torch.cuda.synchronize()
+    best = float("inf")
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b, out=c)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b, c
+    return 2 * n ** 3 / best / 1e12
+
+
+def run_b200(args, world, rank, local):
+    import numpy as np
+    import torch
+    from mcnla_b200 import isvd, synthetic, _lib
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    m, n, k, p, N = args.m, args.n, args.k, args.p, args.N
+    l = k + p
+    L = l * N
+    sigma = np.exp(-np.arange(1, args.rank_r + 1) / 30.0)
+    a = synthetic.lowrank_torch(m, n, sigma, seed=1000 + rank, noise=1e-4, device=dev, colmajor=args.colmajor)
+    torch.cuda.synchronize()
+    ctx = isvd.context(dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def one_solve(seed):
+        return isvd.solve(a, k, p, N, seed=seed, integrator=args.integrator, former=args.former, maxit=args.maxit,
+                          tol=args.tol, with_v=True)
+
+    # warm-up (also allocates the workspaces once)
+    for w in range(max(args.warmup, 1)):
+        s, u, v, it = one_solve(w)
+    torch.cuda.synchronize()
+
+    # ---- timed region: K whole solves, inputs resident in HBM
+    clocks = ClockSampler(local)
+    k0 = ctx.kernels_launched()
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    per_step = []
+    iters = []
+    ev0.record(stream)
+    for step in range(args.steps):
+        e_a, e_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e_a.record(stream)
+        s, u, v, it = one_solve(100 + step)
+        e_b.record(stream)
+        per_step.append((e_a, e_b))
+        iters.append(it)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    barrier(world)
+    launches = ctx.kernels_launched() - k0
+    total = ev0.elapsed_time(ev1) / 1e3
+    step_ms = sorted(x.elapsed_time(y) for x, y in per_step)
+    total = max_over_ranks(total, world)
+    value = world * args.steps / total
+
+    # ---- per-stage breakdown and the sketch roofline (stage API, CUDA events on the same stream)
+    prm = isvd.Parameters(device=dev).setSize(m, n).setRank(k).setOverRank(p).setNumSketch(N).sync()
+    sk = isvd.RowBlockGaussianProjectionSketcher(prm, 7) if not args.colmajor else \
+        isvd.ColBlockGaussianProjectionSketcher(prm, 7)
+    sk.initialize()
+    q = prm.createCollectionQ()
+    sketch_t = []
+    for _ in range(3):
+        sk(a, q)
+        sketch_t.append(sk.times()[1])      # "projection" part: the sketch GEMM alone
+    sketch_s = sum(sketch_t) / len(sketch_t)
+    orth = isvd.RowBlockGramianOrthogonalizer(prm)
+    orth.initialize()
+    orth(q)
+    integ_cls = {"kn": isvd.KolmogorovNagumoIntegrator, "rb_kn": isvd.RowBlockKolmogorovNagumoIntegrator,
+                 "rb_gramian_kn": isvd.RowBlockGramianKolmogorovNagumoIntegrator,
+                 "rb_wy": isvd.RowBlockWenYinIntegrator,
+                 "rb_gramian_wy": isvd.RowBlockGramianWenYinIntegrator}[args.integrator]
+    integ = integ_cls(prm, args.maxit, args.tol)
+    integ.initialize()
+    qbar = prm.createMatrixQbar()
+    integ(q, qbar)
+    former_cls = {"svd": isvd.SvdFormer, "gramian": isvd.GramianFormer, "rb_gramian": isvd.RowBlockGramianFormer,
+                  "cb_gramian": isvd.ColBlockGramianFormer}[args.former]
+    former = former_cls(prm)
+    former.initialize()
+    former(a, qbar)
+    stages = {"sketch_s": sk.time(), "sketch_gemm_s": sketch_s, "orthogonalize_s": orth.time(),
+              "integrate_s": integ.time(), "integrate_iterations": integ.iteration(), "form_s": former.time()}
+    peak64 = fp64_peak_tflops()
+    flops = 2.0 * m * n * L
+    achieved = flops / sketch_s / 1e12
+    traffic = None
+    if SKETCH_TRAFFIC_PER_ROW is not None:
+        traffic = SKETCH_TRAFFIC_PER_ROW * m
+    roofline = {"bound": "tensor", "kernel": "dgemm_kernel (sketch Y = A Omega, FP64 DMMA)",
+                "achieved": round(achieved, 3), "peak": round(peak64, 3), "unit": "TFLOP/s",
+                "frac": round(achieved / peak64, 4), "traffic": traffic,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 has no tcgen05 kind; the "
+                               "measured-peaks file holds bf16 and HBM only)",
+                "algorithmic": "2*m*n*N*l flops per launch"}
+
+    # ---- end to end through the host-buffer C-ABI call (copies inside the timed region)
+    e2e = None
+    if not args.no_e2e:
+        a_host = torch.empty(m, n, dtype=torch.float64, pin_memory=True) if not args.colmajor else \
+            torch.empty(n, m, dtype=torch.float64, pin_memory=True)
+        a_host.copy_(a.t() if args.colmajor else a)
+        om_host = torch.empty(n, L, dtype=torch.float64, pin_memory=True)
+        om_host.copy_(synthetic.omega_torch(n, L, seed=3, device=dev))
+        out = (torch.empty(k, dtype=torch.float64, pin_memory=True),
+               torch.empty(m, k, dtype=torch.float64, pin_memory=True),
+               torch.empty(n, k, dtype=torch.float64, pin_memory=True))
+        isvd.solve_host(a_host, om_host, k, p, N, integrator=args.integrator, former=args.former,
+                        maxit=args.maxit, tol=args.tol, out=out, colmajor=args.colmajor)
+        torch.cuda.synchronize()
+        barrier(world)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            isvd.solve_host(a_host, om_host, k, p, N, integrator=args.integrator, former=args.former,
+                            maxit=args.maxit, tol=args.tol, out=out, colmajor=args.colmajor)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3, world)
+        e2e = {"value": round(world * args.steps / t_e2e, 5), "unit": "iSVD/s",
+               "h2d_bytes_per_step": int(a_host.numel() * 8 + om_host.numel() * 8),
+               "d2h_bytes_per_step": int((k + m * k + n * k) * 8),
+               "path": "mcnla_b200_isvd_host (pinned host A and Omega in, S/U/V out)"}
+        del a_host, om_host
+
+    result = {
+        "metric": METRIC, "value": round(value, 5), "unit": "iSVD/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(total / args.steps * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, on device)",
+        "config": dict(workload(args), parallelism="replicas" if world > 1 else "single GPU"),
+        "a_read_gbs": round(2 * m * n * 8 * world * args.steps / total / 1e9, 2),
+        "p50_ms": round(step_ms[len(step_ms) // 2], 3),
+        "p99_ms": round(step_ms[min(len(step_ms) - 1, int(0.99 * len(step_ms)))], 3),
+        "iterations": iters[-1], "stages": stages, "roofline": roofline, "e2e": e2e,
+        "gpu_launches": int(launches), "clocks": clk,
+    }
+    return result
+
+
+# ------------------------------------------------------------------------------------------------
+# CPU: the reference's own stages on a bounded row sample
+# ------------------------------------------------------------------------------------------------
+def cpu_sample(args, rows=None):
+    """Runs the reference's CPU stages (oracle/_ref when built, else the numpy
+    restatement) on the first `rows` rows of a matrix with the workload's
+    spectrum and parameters.  Returns (estimated seconds per full solve, info)."""
+    import numpy as np
+    from mcnla_b200 import synthetic
+    from oracle import ref_lib
+    m, n, k, p, N = args.m, args.n, args.k, args.p, args.N
+    l = k + p
+    rows = rows or args.cpu_rows or min(m, max(4 * l, 1024))
+    sigma = np.exp(-np.arange(1, args.rank_r + 1) / 30.0)
+    a = synthetic.lowrank_np(rows, n, sigma[: min(len(sigma), rows)], seed=5, noise=1e-4)
+    omega = synthetic.omega_np(n, l * N, seed=5)
+    cores = os.cpu_count() or 1
+    scale = m / rows
+    kinds = {"kn": 0, "rb_kn": 1, "rb_gramian_kn": 2, "rb_wy": 3, "rb_gramian_wy": 4}
+    fkinds = {"svd": 0, "gramian": 1, "rb_gramian": 2, "cb_gramian": 3}
+    if ref_lib.available():
+        lib = ref_lib.load()
+        lib.mref_set_threads(cores)
+        t0 = time.perf_counter()
+        y, t_sketch = ref_lib.sketch(lib, a, omega)
+        q, t_orth = ref_lib.orthogonalize(lib, y, l, N, row_block=True, timing=True)
+        qbar, it, t_int = ref_lib.integrate(lib, q, l, N, kinds[args.integrator], args.maxit, args.tol, timing=True)
+        s, u, v, t_form = ref_lib.form(lib, a, qbar, k, p, fkinds[args.former], timing=True)
+        wall = time.perf_counter() - t0
+        # rows-proportional parts scale by m / rows; the Gramian integrators'
+        # iteration part works on (N l)^2 matrices and does not
+        if args.integrator.startswith("rb_gramian"):
+            t_int_scaled = t_int[1] * scale + t_int[2] + t_int[3] * scale
+        else:
+            t_int_scaled = t_int[0] * scale
+        est = t_sketch * scale + t_orth[0] * scale + t_int_scaled + t_form[0] * scale
+        kind = "reference"
+        detail = {"sketch_s": t_sketch, "orthogonalize_s": t_orth[0], "integrate_s": t_int[0],
+                  "integrate_iterations": it, "form_s": t_form[0], "sample_wall_s": wall}
+    else:
+        from oracle import isvd_oracle as O
+        t0 = time.perf_counter()
+        r = O.isvd(a, omega, k, p, N, integrator=args.integrator,
+                   former="svd" if args.former == "svd" else "gramian", maxit=args.maxit, tol=args.tol)
+        wall = time.perf_counter() - t0
+        est = wall * scale
+        kind = "port"
+        cores = 1 if os.environ.get("OMP_NUM_THREADS") == "1" else cores
+        detail = {"integrate_iterations": r["iterations"], "sample_wall_s": wall}
+    sample = ("first %d of %d rows (same n, k, p, N, spectrum); row-proportional stage times scaled by %.1f"
+              % (rows, m, scale))
+    return est, {"cores": cores, "kind": kind, "sample": sample, "detail": detail}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return None
+    steps = []
+    info = None
+    for i in range(args.warmup + args.steps):
+        est, info = cpu_sample(args)
+        if i >= args.warmup:
+            steps.append(est)
+    mean = sum(steps) / len(steps)
+    value = 1.0 / mean
+    return {
+        "metric": METRIC, "value": round(value, 6), "unit": "iSVD/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(mean * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
+        "config": dict(workload(args), parallelism="host CPU"),
+        "cpu_baseline": {"value": round(value, 6), "unit": "iSVD/s", "cores": info["cores"], "kind": info["kind"],
+                         "sample": info["sample"]},
+        "e2e": {"value": round(value, 6), "unit": "iSVD/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "detail": info["detail"],
+    }
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_init(args)
+    if args.impl == "reference":
+        res = run_reference(args, world, rank)
+    else:
+        res = run_b200(args, world, rank, local)
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            est, info = cpu_sample(args)
+            res["cpu_baseline"] = {"value": round(1.0 / est, 6), "unit": "iSVD/s", "cores": info["cores"],
+                                   "kind": info["kind"], "sample": info["sample"]}
+    if rank == 0 and res is not None:
+        print(json.dumps(res), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,203 @@
+/*
+ * mcnla_b200: the C ABI of a B200-native integrated randomized SVD (iSVD).
+ *
+ * It covers one pipeline of MCNLA 0.7.2 (emfomy/mcnla): Gaussian-projection
+ * sketching -> Gramian orthogonalization -> Kolmogorov-Nagumo or Wen-Yin
+ * integration -> SVD forming.  Each entry point below replaces the `runImpl`
+ * of one reference stage (cited per function; paths are relative to the
+ * reference project root).  The reference's MPI decomposition over sketches
+ * and row blocks collapses into on-device batching on one GPU, so the
+ * "row-block" and "column-block" variants differ here only in the layout of A
+ * and in the algorithm the stage runs, never in a collective.
+ *
+ * Conventions
+ *   - All matrix pointers are DEVICE pointers to double (FP64) unless stated.
+ *   - A is m x n, row-major (MCNLA_B200_ROW_MAJOR, leading dimension lda >= n)
+ *     or column-major (MCNLA_B200_COL_MAJOR, lda >= m).
+ *   - The sketch collection Q is "unfolded": one row-major m x (N*l) matrix
+ *     whose column block i is sketch i (the reference's
+ *     DenseMatrixCollectionColBlockRowMajor,
+ *     include/mcnla/core/matrix/collection/dense/dense_matrix_collection_col_block.hpp:44-55).
+ *   - Q-bar is row-major m x l; U is row-major m x k; V is row-major n x k;
+ *     S holds the k leading singular values in descending order.
+ *   - Every function returns MCNLA_B200_OK (0) or an error status; none aborts.
+ *     The reference has no error returns (it asserts); see
+ *     mcnla_b200_status_string() for the meanings.
+ *   - Work is enqueued on the context's stream.  Functions that must read a
+ *     device result to decide what to do next (the integrators' convergence
+ *     tests) synchronize that stream; all others return without waiting.
+ */
+#ifndef MCNLA_B200_H_
+#define MCNLA_B200_H_
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define MCNLA_B200_API __attribute__((visibility("default")))
+#else
+#define MCNLA_B200_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define MCNLA_B200_OK                  0
+#define MCNLA_B200_ERR_SHAPE           1  /* sizes non-positive, inconsistent or over a limit */
+#define MCNLA_B200_ERR_LAYOUT          2  /* a strided operand without a unit stride */
+#define MCNLA_B200_ERR_WORKSPACE       3  /* internal: a split-K GEMM was given no workspace */
+#define MCNLA_B200_ERR_CUDA            4  /* a CUDA runtime call failed (see mcnla_b200_last_error) */
+#define MCNLA_B200_ERR_NOMEM           5  /* device allocation failed */
+#define MCNLA_B200_ERR_ARG             6  /* null pointer or invalid enumerator */
+#define MCNLA_B200_ERR_UNSUPPORTED     7  /* shape beyond a kernel's stated limit (e.g. l > 160) */
+#define MCNLA_B200_ERR_SINGULAR        8  /* exact zero pivot in a small inverse */
+
+/* ---- enumerators -------------------------------------------------------- */
+#define MCNLA_B200_ROW_MAJOR 0
+#define MCNLA_B200_COL_MAJOR 1
+
+/* Integrators (include/mcnla/isvd/integrator/) */
+#define MCNLA_B200_KOLMOGOROV_NAGUMO                   0  /* kolmogorov_nagumo_integrator.hpp */
+#define MCNLA_B200_ROW_BLOCK_KOLMOGOROV_NAGUMO         1  /* row_block_kolmogorov_nagumo_integrator.hpp */
+#define MCNLA_B200_ROW_BLOCK_GRAMIAN_KOLMOGOROV_NAGUMO 2  /* row_block_gramian_kolmogorov_nagumo_integrator.hpp */
+#define MCNLA_B200_ROW_BLOCK_WEN_YIN                   3  /* row_block_wen_yin_integrator.hpp */
+#define MCNLA_B200_ROW_BLOCK_GRAMIAN_WEN_YIN           4  /* row_block_gramian_wen_yin_integrator.hpp */
+
+/* Formers (include/mcnla/isvd/former/) */
+#define MCNLA_B200_SVD_FORMER                0  /* svd_former.hpp (with V) */
+#define MCNLA_B200_GRAMIAN_FORMER            1  /* gramian_former.hpp (with V) */
+#define MCNLA_B200_ROW_BLOCK_GRAMIAN_FORMER  2  /* row_block_gramian_former.hpp (with V) */
+#define MCNLA_B200_COL_BLOCK_GRAMIAN_FORMER  3  /* col_block_gramian_former.hpp (with V) */
+
+/* Largest sketch dimension l = k + p the small on-chip solvers accept. */
+#define MCNLA_B200_MAX_DIM_SKETCH        160
+#define MCNLA_B200_MAX_DIM_SKETCH_WENYIN 80
+
+/* ---- parameters ----------------------------------------------------------
+ * Mirror of mcnla::isvd::Parameters<_Val>::params_
+ * (include/mcnla/isvd/core/parameters.hh:54-69): number of rows/columns of A,
+ * desired rank k, oversampling p (reference default 12) and number of
+ * sketches N (reference default 16).  dimSketch l = k + p.                     */
+typedef struct mcnla_b200_params {
+  int64_t nrow;
+  int64_t ncol;
+  int64_t rank;
+  int64_t over_rank;
+  int64_t num_sketch;
+} mcnla_b200_params;
+
+typedef struct mcnla_b200_ctx mcnla_b200_ctx;
+
+/* ---- context -------------------------------------------------------------
+ * Replaces mcnla::init()/gpuInit (include/mcnla/core/def.hpp:42-61,
+ * include/mcnla/core_gpu/def.hpp:42-47): binds one device and one stream.
+ * stream == NULL creates a private non-blocking stream; otherwise the given
+ * cudaStream_t is used (and not destroyed).                                  */
+MCNLA_B200_API int mcnla_b200_create(mcnla_b200_ctx** ctx, int device, void* stream);
+MCNLA_B200_API int mcnla_b200_destroy(mcnla_b200_ctx* ctx);
+MCNLA_B200_API int mcnla_b200_set_stream(mcnla_b200_ctx* ctx, void* stream);
+MCNLA_B200_API const char* mcnla_b200_status_string(int status);
+/* Text of the last CUDA error (thread-local). */
+MCNLA_B200_API const char* mcnla_b200_last_error(void);
+/* Number of kernels this context has launched (for launch accounting). */
+MCNLA_B200_API int64_t mcnla_b200_kernels_launched(const mcnla_b200_ctx* ctx);
+
+/* Stage timers: seconds per part of the last stage call, the reference's
+ * StageWrapper::times() (include/mcnla/isvd/core/stage_wrapper.hpp:128-135),
+ * measured with CUDA events.  Synchronizes the stream.  Returns the number of
+ * parts written (at most capacity) or a negative status.                     */
+MCNLA_B200_API int mcnla_b200_last_times(mcnla_b200_ctx* ctx, double* times, int capacity);
+
+/* Pre-allocates the workspaces a pipeline with these parameters, integrator
+ * and former will use, like StageWrapper::initialize()
+ * (include/mcnla/isvd/core/stage_wrapper.hpp:37-46).  Optional: stages grow
+ * the workspace on first use otherwise.                                      */
+MCNLA_B200_API int mcnla_b200_initialize(mcnla_b200_ctx* ctx, const mcnla_b200_params* params, int integrator, int former);
+
+/* ---- sketcher ------------------------------------------------------------
+ * Q := A * Omega on the unfolded collection, then `exponent` power
+ * iterations (Omega := A' Q; Q := A Omega).  Replaces
+ * GaussianProjectionSketcher::runImpl
+ * (include/mcnla/isvd/sketcher/gaussian_projection_sketcher.hpp:65-103), its
+ * row-block (row_block_gaussian_projection_sketcher.hpp:65-114) and
+ * column-block (col_block_gaussian_projection_sketcher.hpp:63-102) variants.
+ * omega: n x (N*l) row-major; it is overwritten when exponent > 0.           */
+MCNLA_B200_API int mcnla_b200_sketch(mcnla_b200_ctx* ctx, const mcnla_b200_params* params, const double* A, int a_layout,
+                      int64_t lda, double* omega, int exponent, double* Q);
+
+/* Fills out[0..count) with N(0,1) samples from a counter-based generator
+ * (Philox-4x32-10 + Box-Muller) keyed by seed; the on-device stand-in for
+ * random::gaussian (include/mcnla/core/random/routine/gaussian.hpp:39-56).
+ * The same (seed, count) always gives the same values.                       */
+MCNLA_B200_API int mcnla_b200_gaussian(mcnla_b200_ctx* ctx, uint64_t seed, int64_t count, double* out);
+
+/* ---- orthogonalizer --------------------------------------------------------
+ * In place on Q (m x N*l): W_i := Q_i' Q_i; eig(W_i) = V_i S_i V_i';
+ * Q_i := Q_i V_i S_i^(-1/2), eigenvalues in descending order.  Replaces
+ * GramianOrthogonalizer::runImpl
+ * (include/mcnla/isvd/orthogonalizer/gramian_orthogonalizer.hpp:62-104) and
+ * RowBlockGramianOrthogonalizer::runImpl
+ * (row_block_gramian_orthogonalizer.hpp:62-105).                            */
+MCNLA_B200_API int mcnla_b200_orthogonalize(mcnla_b200_ctx* ctx, const mcnla_b200_params* params, double* Q);
+
+/* ---- integrators -----------------------------------------------------------
+ * Qbar := the integrated basis of the N orthonormal bases in Q.  kind is one
+ * of the MCNLA_B200_*KOLMOGOROV_NAGUMO / *WEN_YIN enumerators; each runs the
+ * algorithm of the reference stage named beside it.  *iteration receives the
+ * number of iterations executed (the reference's iteration()).  Synchronizes
+ * the stream.                                                                */
+MCNLA_B200_API int mcnla_b200_integrate(mcnla_b200_ctx* ctx, const mcnla_b200_params* params, int kind, const double* Q,
+                         int max_iteration, double tolerance, double* Qbar, int* iteration);
+
+/* ---- formers ---------------------------------------------------------------
+ * Rank-k SVD of A from Qbar: S (k), U (m x k), V (n x k).  kind is one of the
+ * MCNLA_B200_*_FORMER enumerators.  Replaces SvdFormer<_,true>::runImpl
+ * (include/mcnla/isvd/former/svd_former.hpp:70-116) and the Gramian formers
+ * (gramian_former.hpp:72-132, row_block_gramian_former.hpp:78-146,
+ * col_block_gramian_former.hpp:73-131).  U or V may be NULL to skip them.     */
+MCNLA_B200_API int mcnla_b200_form(mcnla_b200_ctx* ctx, const mcnla_b200_params* params, int kind, const double* A, int a_layout,
+                    int64_t lda, const double* Qbar, double* S, double* U, double* V);
+
+/* ---- whole solve -----------------------------------------------------------
+ * Sketch -> orthogonalize -> integrate -> form, as the reference drivers wire
+ * the stages (src/isvd_dense_rb.cpp:46-286, src/isvd_dense_cb.cpp:46-303).
+ * mcnla_b200_isvd takes device buffers; omega may be NULL to draw it on the
+ * device from seed.  mcnla_b200_isvd_host takes HOST buffers (A, omega, S, U,
+ * V) and does the host<->device copies itself, the path of the reference's
+ * GPU drivers (src/isvd_dense_rb_gpu.cpp).                                    */
+MCNLA_B200_API int mcnla_b200_isvd(mcnla_b200_ctx* ctx, const mcnla_b200_params* params, int integrator, int former,
+                    const double* A, int a_layout, int64_t lda, const double* omega, uint64_t seed,
+                    int max_iteration, double tolerance, double* S, double* U, double* V, int* iteration);
+MCNLA_B200_API int mcnla_b200_isvd_host(mcnla_b200_ctx* ctx, const mcnla_b200_params* params, int integrator, int former,
+                         const double* A_host, int a_layout, const double* omega_host, int max_iteration,
+                         double tolerance, double* S_host, double* U_host, double* V_host, int* iteration);
+
+/* ---- building blocks (exposed for tests) ----------------------------------
+ * FP64 GEMM C := alpha*A*B + beta*C on strided device matrices (element (i,j)
+ * of X at X[i*x_rs + j*x_cs]); the reference's la::mm
+ * (include/mcnla/core/la/dense/routine/gemm.hpp:35-148).  force_splits > 0
+ * forces that many K splits.                                                  */
+MCNLA_B200_API int mcnla_b200_dgemm(mcnla_b200_ctx* ctx, int64_t M, int64_t N, int64_t K, double alpha, const double* A,
+                     int64_t a_rs, int64_t a_cs, const double* B, int64_t b_rs, int64_t b_cs, double beta, double* C,
+                     int64_t c_rs, int64_t c_cs, int force_splits);
+
+/* Batched symmetric eigendecomposition of `batch` row-major n x n matrices
+ * (consecutive in A): eigenvalues to W (n per matrix), eigenvectors as the
+ * columns of row-major V (n x n per matrix).  order 0 = ascending (dsyev,
+ * include/mcnla/core/la/dense/driver/syev.hpp:150-160), 1 = descending by
+ * absolute value (dgesvd of a symmetric positive semi-definite matrix,
+ * gesvd.hpp:159-193).                                                        */
+MCNLA_B200_API int mcnla_b200_syev_batched(mcnla_b200_ctx* ctx, int n, int batch, const double* A, double* W, double* V,
+                            int order);
+
+/* In-place inverse of `batch` row-major n x n matrices (consecutive in A),
+ * the reference's getrfi (include/mcnla/core/la/dense/driver/getrfi.hpp:117-124).
+ * n <= 2 * MCNLA_B200_MAX_DIM_SKETCH_WENYIN.                                 */
+MCNLA_B200_API int mcnla_b200_inverse_batched(mcnla_b200_ctx* ctx, int n, int batch, double* A);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+
+#endif  /* MCNLA_B200_H_ */

@@ -1,0 +1,113 @@
+// Shared definitions of the B200 iSVD library: status codes, error checks,
+// strided matrix references and the per-device context that owns workspaces.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstddef>
+#include <vector>
+#include <string>
+
+#include "../../include/mcnla_b200.h"
+
+namespace mb {
+
+// Status is returned by every host entry point; kernels report device-side
+// failures (non-convergence is not a failure; a bounded wait that ran out is)
+// through the context's device status word.
+#define MB_CHECK_CUDA(expr)                                            \
+  do {                                                                 \
+    cudaError_t _e = (expr);                                           \
+    if (_e != cudaSuccess) { ::mb::set_last_cuda_error(_e, #expr, __FILE__, __LINE__); \
+                             return MCNLA_B200_ERR_CUDA; }             \
+  } while (0)
+
+#define MB_CHECK(expr)                                                 \
+  do { int _s = (expr); if (_s != MCNLA_B200_OK) return _s; } while (0)
+
+void set_last_cuda_error(cudaError_t e, const char* what, const char* file, int line);
+void set_last_message(const std::string& msg);
+
+// Element (i, j) of a strided matrix lives at p[i * rs + j * cs].
+struct CMat { const double* p; int64_t rs, cs; };
+struct DMat { double* p; int64_t rs, cs; };
+
+inline CMat cm(const double* p, int64_t rs, int64_t cs) { return CMat{p, rs, cs}; }
+inline DMat dm(double* p, int64_t rs, int64_t cs) { return DMat{p, rs, cs}; }
+inline CMat cmc(DMat m) { return CMat{m.p, m.rs, m.cs}; }
+// Row-major and column-major helpers (leading dimension ld).
+inline CMat crow(const double* p, int64_t ld) { return CMat{p, ld, 1}; }
+inline CMat ccol(const double* p, int64_t ld) { return CMat{p, 1, ld}; }
+inline DMat drow(double* p, int64_t ld) { return DMat{p, ld, 1}; }
+inline CMat ctr(CMat a) { return CMat{a.p, a.cs, a.rs}; }
+
+// Device-resident scalars of one stage run (read back by the host between steps).
+struct DevScalars {
+  double norm;        // convergence norm (KN: ||e - 1||_2)
+  double phit;        // WY: 1/2N ||B+||_F^2 of the last trial
+  double mu;          // WY: tr(Dg) - ||D||_F^2
+  double t1, t2;      // WY: step-size inner products
+  double dot[16];     // scratch reductions
+  int status;         // device-side error code (0 = ok)
+  int sweeps;         // Jacobi sweeps used by the last small solve
+  int pad[2];
+};
+
+// Per-device context: one stream, a growable workspace arena, timing events.
+struct Context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int num_sms = 148;
+  size_t smem_optin = 0;
+  // workspace arena (grown on demand by reserve(); never shrunk until destroy)
+  void* arena = nullptr;
+  size_t arena_bytes = 0;
+  size_t arena_top = 0;
+  // pipeline arena: buffers that live across the stages of one whole solve
+  void* parena = nullptr;
+  size_t parena_bytes = 0;
+  // split-K workspace of the current stage (set by the stage; dgemm checks
+  // every split-K launch against its size)
+  double* gws = nullptr;
+  size_t gws_bytes = 0;
+  DevScalars* scal = nullptr;       // device scalars
+  DevScalars* scal_host = nullptr;  // pinned mirror
+  // stage part timers (CUDA events), filled by the last stage call
+  std::vector<cudaEvent_t> events;
+  int nevents_used = 0;
+  std::vector<double> last_times;   // seconds per part of the last stage call
+  bool timing = true;
+  // bookkeeping
+  int64_t kernels_launched = 0;
+};
+
+// Arena allocation: every call of a stage first computes the bytes it needs,
+// reserves them (one cudaMalloc at most, when the arena must grow), then
+// carves aligned sub-buffers in order.
+int ctx_reserve(Context* c, size_t bytes);
+int ctx_reserve_pipeline(Context* c, size_t bytes);
+// Returns nullptr when the carve would pass the reservation (callers check).
+template <class T>
+T* ctx_take(Context* c, size_t count) {
+  size_t off = (c->arena_top + 255) & ~size_t(255);
+  c->arena_top = off + count * sizeof(T);
+  if (c->arena_top > c->arena_bytes) return nullptr;
+  return reinterpret_cast<T*>(static_cast<char*>(c->arena) + off);
+}
+inline size_t arena_bytes_for(size_t count, size_t elem) { return ((count * elem + 255) & ~size_t(255)) + 256; }
+
+// Timing of stage parts (the reference's tic/toc moments,
+// include/mcnla/isvd/core/stage_wrapper.hpp:170-192, on CUDA events).
+int ctx_tic(Context* c);
+int ctx_toc(Context* c);
+int ctx_collect_times(Context* c);
+
+int ctx_sync_scalars(Context* c);   // copies DevScalars to the pinned mirror and waits
+
+inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+}  // namespace mb
+
+// The opaque handle of the C ABI is the context itself.
+struct mcnla_b200_ctx : public mb::Context {};

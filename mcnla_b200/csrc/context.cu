@@ -1,0 +1,193 @@
+// Context lifecycle, workspace arena, stage timers and status strings.
+#include "common.cuh"
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+namespace mb {
+
+namespace {
+thread_local char g_last_error[512] = "";
+}
+
+void set_last_cuda_error(cudaError_t e, const char* what, const char* file, int line) {
+  std::snprintf(g_last_error, sizeof(g_last_error), "%s: %s (%s:%d)", cudaGetErrorString(e), what, file, line);
+}
+
+void set_last_message(const std::string& msg) {
+  std::snprintf(g_last_error, sizeof(g_last_error), "%s", msg.c_str());
+}
+
+const char* last_error_text() { return g_last_error; }
+
+int ctx_reserve(Context* c, size_t bytes) {
+  c->arena_top = 0;
+  if (bytes <= c->arena_bytes) return MCNLA_B200_OK;
+  if (c->arena) {
+    MB_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+    MB_CHECK_CUDA(cudaFree(c->arena));
+    c->arena = nullptr;
+    c->arena_bytes = 0;
+  }
+  const size_t want = bytes + (bytes >> 3);   // grow with headroom
+  cudaError_t e = cudaMalloc(&c->arena, want);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    set_last_cuda_error(e, "workspace cudaMalloc", __FILE__, __LINE__);
+    c->arena = nullptr;
+    return MCNLA_B200_ERR_NOMEM;
+  }
+  c->arena_bytes = want;
+  return MCNLA_B200_OK;
+}
+
+int ctx_reserve_pipeline(Context* c, size_t bytes) {
+  if (bytes <= c->parena_bytes) return MCNLA_B200_OK;
+  if (c->parena) {
+    MB_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+    MB_CHECK_CUDA(cudaFree(c->parena));
+    c->parena = nullptr;
+    c->parena_bytes = 0;
+  }
+  cudaError_t e = cudaMalloc(&c->parena, bytes);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    set_last_cuda_error(e, "pipeline cudaMalloc", __FILE__, __LINE__);
+    c->parena = nullptr;
+    return MCNLA_B200_ERR_NOMEM;
+  }
+  c->parena_bytes = bytes;
+  return MCNLA_B200_OK;
+}
+
+int ctx_tic(Context* c) {
+  c->nevents_used = 0;
+  return ctx_toc(c);
+}
+
+int ctx_toc(Context* c) {
+  if (!c->timing) return MCNLA_B200_OK;
+  if (c->nevents_used >= int(c->events.size())) {
+    cudaEvent_t ev;
+    MB_CHECK_CUDA(cudaEventCreate(&ev));
+    c->events.push_back(ev);
+  }
+  MB_CHECK_CUDA(cudaEventRecord(c->events[c->nevents_used], c->stream));
+  c->nevents_used++;
+  return MCNLA_B200_OK;
+}
+
+int ctx_collect_times(Context* c) {
+  c->last_times.clear();
+  if (!c->timing || c->nevents_used < 2) return MCNLA_B200_OK;
+  MB_CHECK_CUDA(cudaEventSynchronize(c->events[c->nevents_used - 1]));
+  for (int i = 1; i < c->nevents_used; ++i) {
+    float ms = 0.f;
+    MB_CHECK_CUDA(cudaEventElapsedTime(&ms, c->events[i - 1], c->events[i]));
+    c->last_times.push_back(ms * 1e-3);
+  }
+  return MCNLA_B200_OK;
+}
+
+int ctx_sync_scalars(Context* c) {
+  MB_CHECK_CUDA(cudaMemcpyAsync(c->scal_host, c->scal, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->stream));
+  MB_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+  return MCNLA_B200_OK;
+}
+
+}  // namespace mb
+
+using mb::Context;
+
+extern "C" {
+
+const char* mcnla_b200_last_error(void) { return mb::last_error_text(); }
+
+const char* mcnla_b200_status_string(int status) {
+  switch (status) {
+    case MCNLA_B200_OK: return "ok";
+    case MCNLA_B200_ERR_SHAPE: return "invalid or inconsistent sizes";
+    case MCNLA_B200_ERR_LAYOUT: return "operand has no unit stride";
+    case MCNLA_B200_ERR_WORKSPACE: return "missing workspace";
+    case MCNLA_B200_ERR_CUDA: return "CUDA runtime error";
+    case MCNLA_B200_ERR_NOMEM: return "device out of memory";
+    case MCNLA_B200_ERR_ARG: return "invalid argument";
+    case MCNLA_B200_ERR_UNSUPPORTED: return "shape beyond a kernel limit";
+    case MCNLA_B200_ERR_SINGULAR: return "singular matrix in a small inverse";
+    default: return "unknown status";
+  }
+}
+
+int mcnla_b200_create(mcnla_b200_ctx** out, int device, void* stream) {
+  if (!out) return MCNLA_B200_ERR_ARG;
+  *out = nullptr;
+  mcnla_b200_ctx* c = new (std::nothrow) mcnla_b200_ctx();
+  if (!c) return MCNLA_B200_ERR_NOMEM;
+  c->device = device;
+  auto fail = [&](int st) { delete c; return st; };
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) { mb::set_last_cuda_error(e, "cudaSetDevice", __FILE__, __LINE__); return fail(MCNLA_B200_ERR_CUDA); }
+  cudaDeviceProp prop;
+  e = cudaGetDeviceProperties(&prop, device);
+  if (e != cudaSuccess) { mb::set_last_cuda_error(e, "cudaGetDeviceProperties", __FILE__, __LINE__); return fail(MCNLA_B200_ERR_CUDA); }
+  c->num_sms = prop.multiProcessorCount;
+  c->smem_optin = prop.sharedMemPerBlockOptin;
+  if (stream) {
+    c->stream = static_cast<cudaStream_t>(stream);
+    c->own_stream = false;
+  } else {
+    e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { mb::set_last_cuda_error(e, "cudaStreamCreate", __FILE__, __LINE__); return fail(MCNLA_B200_ERR_CUDA); }
+    c->own_stream = true;
+  }
+  e = cudaMalloc(&c->scal, sizeof(mb::DevScalars));
+  if (e != cudaSuccess) { mb::set_last_cuda_error(e, "cudaMalloc scalars", __FILE__, __LINE__); return fail(MCNLA_B200_ERR_NOMEM); }
+  e = cudaMallocHost(&c->scal_host, sizeof(mb::DevScalars));
+  if (e != cudaSuccess) { mb::set_last_cuda_error(e, "cudaMallocHost", __FILE__, __LINE__); return fail(MCNLA_B200_ERR_NOMEM); }
+  std::memset(c->scal_host, 0, sizeof(mb::DevScalars));
+  e = cudaMemsetAsync(c->scal, 0, sizeof(mb::DevScalars), c->stream);
+  if (e != cudaSuccess) { mb::set_last_cuda_error(e, "cudaMemset", __FILE__, __LINE__); return fail(MCNLA_B200_ERR_CUDA); }
+  *out = c;
+  return MCNLA_B200_OK;
+}
+
+int mcnla_b200_destroy(mcnla_b200_ctx* c) {
+  if (!c) return MCNLA_B200_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (auto ev : c->events) cudaEventDestroy(ev);
+  if (c->arena) cudaFree(c->arena);
+  if (c->parena) cudaFree(c->parena);
+  if (c->scal) cudaFree(c->scal);
+  if (c->scal_host) cudaFreeHost(c->scal_host);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return MCNLA_B200_OK;
+}
+
+int mcnla_b200_set_stream(mcnla_b200_ctx* c, void* stream) {
+  if (!c) return MCNLA_B200_ERR_ARG;
+  if (c->own_stream && c->stream) {
+    MB_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+    MB_CHECK_CUDA(cudaStreamDestroy(c->stream));
+  }
+  if (stream) { c->stream = static_cast<cudaStream_t>(stream); c->own_stream = false; }
+  else {
+    MB_CHECK_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    c->own_stream = true;
+  }
+  return MCNLA_B200_OK;
+}
+
+int64_t mcnla_b200_kernels_launched(const mcnla_b200_ctx* c) { return c ? c->kernels_launched : 0; }
+
+int mcnla_b200_last_times(mcnla_b200_ctx* c, double* times, int capacity) {
+  if (!c || (!times && capacity > 0)) return -MCNLA_B200_ERR_ARG;
+  int st = mb::ctx_collect_times(c);
+  if (st != MCNLA_B200_OK) return -st;
+  const int n = std::min<int>(capacity, int(c->last_times.size()));
+  for (int i = 0; i < n; ++i) times[i] = c->last_times[i];
+  return int(c->last_times.size()) < capacity ? int(c->last_times.size()) : n;
+}
+
+}  // extern "C"

@@ -1,0 +1,347 @@
+// FP64 DMMA GEMM (see dgemm.cuh).
+//
+// Tiling: a CTA computes a BM x BN tile of C; its warps own WM x WN sub-tiles
+// made of 8x8 DMMA fragments.  K advances in steps of BK = 16 through a
+// STAGES-deep cp.async ring.  Shared-memory rows are padded (K-contiguous
+// rows by 4 doubles, M/N-contiguous rows by 8) so every fragment load of a
+// warp touches each bank pair at most twice: the minimum two wavefronts for
+// 32 lanes x 8 bytes.
+#include "dgemm.cuh"
+#include <algorithm>
+
+namespace mb {
+namespace {
+
+constexpr int BK = 16;
+constexpr int PAD_K = 4;
+constexpr int PAD_MN = 8;
+
+struct KArgs {
+  int64_t M, N, K;
+  double alpha, beta;
+  const double* A; int64_t a_rs, a_cs, a_bs;
+  const double* B; int64_t b_rs, b_cs, b_bs;
+  double* C; int64_t c_rs, c_cs, c_bs;
+  double* ws;
+  int splits;
+  int64_t kps;
+};
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes) {
+  unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, int src_bytes) {
+  unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+template <int BM_, int BN_, int WM_, int WN_, bool AK_, bool BKM_, int VEC_, int STAGES_>
+struct Cfg {
+  static constexpr int BM = BM_, BN = BN_, WM = WM_, WN = WN_, VEC = VEC_, STAGES = STAGES_;
+  static constexpr bool AK = AK_, BKM = BKM_;
+  static constexpr int WARPS_M = BM / WM, WARPS_N = BN / WN;
+  static constexpr int THREADS = WARPS_M * WARPS_N * 32;
+  static constexpr int MT = WM / 8, NT = WN / 8;
+  static constexpr int LDA = AK ? (BK + PAD_K) : (BM + PAD_MN);
+  static constexpr int LDB = BKM ? (BK + PAD_K) : (BN + PAD_MN);
+  static constexpr int A_ELEMS = AK ? BM * LDA : BK * LDA;
+  static constexpr int B_ELEMS = BKM ? BN * LDB : BK * LDB;
+  static constexpr int STAGE_ELEMS = A_ELEMS + B_ELEMS;
+  static constexpr size_t SMEM = size_t(STAGES) * STAGE_ELEMS * sizeof(double);
+};
+
+template <class C>
+__device__ __forceinline__ void load_stage(double* sA, double* sB, const KArgs& g, const double* A,
+                                           const double* B, int64_t m0, int64_t n0, int64_t k0, int64_t kend,
+                                           int tid) {
+  constexpr int V = C::VEC;
+  if constexpr (C::AK) {  // rows of A along M, K contiguous
+    constexpr int CPR = BK / V, TOTAL = C::BM * CPR;
+#pragma unroll
+    for (int c = tid; c < TOTAL; c += C::THREADS) {
+      const int r = c / CPR, kc = (c % CPR) * V;
+      const int64_t gm = m0 + r, gk = k0 + kc;
+      int valid = 0;
+      if (gm < g.M) { int64_t v = kend - gk; valid = v <= 0 ? 0 : (v >= V ? V : int(v)); }
+      const double* src = valid ? A + gm * g.a_rs + gk : A;
+      double* dst = sA + r * C::LDA + kc;
+      if constexpr (V == 2) cp_async16(dst, src, valid * 8); else cp_async8(dst, src, valid * 8);
+    }
+  } else {  // rows of A along K, M contiguous
+    constexpr int CPR = C::BM / V, TOTAL = BK * CPR;
+#pragma unroll
+    for (int c = tid; c < TOTAL; c += C::THREADS) {
+      const int kr = c / CPR, mc = (c % CPR) * V;
+      const int64_t gk = k0 + kr, gm = m0 + mc;
+      int valid = 0;
+      if (gk < kend) { int64_t v = g.M - gm; valid = v <= 0 ? 0 : (v >= V ? V : int(v)); }
+      const double* src = valid ? A + gk * g.a_cs + gm : A;
+      double* dst = sA + kr * C::LDA + mc;
+      if constexpr (V == 2) cp_async16(dst, src, valid * 8); else cp_async8(dst, src, valid * 8);
+    }
+  }
+  if constexpr (C::BKM) {  // rows of B along N, K contiguous
+    constexpr int CPR = BK / V, TOTAL = C::BN * CPR;
+#pragma unroll
+    for (int c = tid; c < TOTAL; c += C::THREADS) {
+      const int r = c / CPR, kc = (c % CPR) * V;
+      const int64_t gn = n0 + r, gk = k0 + kc;
+      int valid = 0;
+      if (gn < g.N) { int64_t v = kend - gk; valid = v <= 0 ? 0 : (v >= V ? V : int(v)); }
+      const double* src = valid ? B + gn * g.b_cs + gk : B;
+      double* dst = sB + r * C::LDB + kc;
+      if constexpr (V == 2) cp_async16(dst, src, valid * 8); else cp_async8(dst, src, valid * 8);
+    }
+  } else {  // rows of B along K, N contiguous
+    constexpr int CPR = C::BN / V, TOTAL = BK * CPR;
+#pragma unroll
+    for (int c = tid; c < TOTAL; c += C::THREADS) {
+      const int kr = c / CPR, nc = (c % CPR) * V;
+      const int64_t gk = k0 + kr, gn = n0 + nc;
+      int valid = 0;
+      if (gk < kend) { int64_t v = g.N - gn; valid = v <= 0 ? 0 : (v >= V ? V : int(v)); }
+      const double* src = valid ? B + gk * g.b_rs + gn : B;
+      double* dst = sB + kr * C::LDB + nc;
+      if constexpr (V == 2) cp_async16(dst, src, valid * 8); else cp_async8(dst, src, valid * 8);
+    }
+  }
+}
+
+template <class C>
+__global__ void __launch_bounds__(C::THREADS) dgemm_kernel(KArgs g) {
+  extern __shared__ __align__(16) double smem[];
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  const int wm = warp / C::WARPS_N, wn = warp % C::WARPS_N;
+  const int gq = lane >> 2, t4 = lane & 3;
+
+  const int64_t n0 = int64_t(blockIdx.x) * C::BN;
+  const int64_t m0 = int64_t(blockIdx.y) * C::BM;
+  const int bz = blockIdx.z / g.splits;
+  const int split = blockIdx.z % g.splits;
+  const double* A = g.A + bz * g.a_bs;
+  const double* B = g.B + bz * g.b_bs;
+  const int64_t kbeg = split * g.kps;
+  const int64_t kend = min(g.K, kbeg + g.kps);
+  const int KT = kend > kbeg ? int((kend - kbeg + BK - 1) / BK) : 0;
+
+  double acc[C::MT][C::NT][2];
+#pragma unroll
+  for (int i = 0; i < C::MT; ++i)
+#pragma unroll
+    for (int j = 0; j < C::NT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+#pragma unroll
+  for (int s = 0; s < C::STAGES - 1; ++s) {
+    if (s < KT) {
+      double* st = smem + s * C::STAGE_ELEMS;
+      load_stage<C>(st, st + C::A_ELEMS, g, A, B, m0, n0, kbeg + int64_t(s) * BK, kend, tid);
+    }
+    cp_commit();
+  }
+
+  for (int kt = 0; kt < KT; ++kt) {
+    cp_wait<C::STAGES - 2>();
+    __syncthreads();
+    {
+      const int nt = kt + C::STAGES - 1;
+      if (nt < KT) {
+        double* st = smem + (nt % C::STAGES) * C::STAGE_ELEMS;
+        load_stage<C>(st, st + C::A_ELEMS, g, A, B, m0, n0, kbeg + int64_t(nt) * BK, kend, tid);
+      }
+      cp_commit();
+    }
+    const double* sA = smem + (kt % C::STAGES) * C::STAGE_ELEMS;
+    const double* sB = sA + C::A_ELEMS;
+#pragma unroll
+    for (int kk = 0; kk < BK / 4; ++kk) {
+      const int k = kk * 4 + t4;
+      double af[C::MT], bf[C::NT];
+#pragma unroll
+      for (int i = 0; i < C::MT; ++i) {
+        const int m = wm * C::WM + i * 8 + gq;
+        af[i] = C::AK ? sA[m * C::LDA + k] : sA[k * C::LDA + m];
+      }
+#pragma unroll
+      for (int j = 0; j < C::NT; ++j) {
+        const int n = wn * C::WN + j * 8 + gq;
+        bf[j] = C::BKM ? sB[n * C::LDB + k] : sB[k * C::LDB + n];
+      }
+#pragma unroll
+      for (int i = 0; i < C::MT; ++i)
+#pragma unroll
+        for (int j = 0; j < C::NT; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+    }
+  }
+  cp_wait<0>();
+
+  // Epilogue: direct strided stores (C) or raw partials (split-K workspace).
+  double* Cb = g.C + bz * g.c_bs;
+  double* W = g.ws ? g.ws + (int64_t(bz) * g.splits + split) * g.M * g.N : nullptr;
+#pragma unroll
+  for (int i = 0; i < C::MT; ++i) {
+    const int64_t row = m0 + wm * C::WM + i * 8 + gq;
+    if (row >= g.M) continue;
+#pragma unroll
+    for (int j = 0; j < C::NT; ++j) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int64_t col = n0 + wn * C::WN + j * 8 + 2 * t4 + h;
+        if (col >= g.N) continue;
+        if (g.splits == 1) {
+          double* cp = Cb + row * g.c_rs + col * g.c_cs;
+          double v = g.alpha * acc[i][j][h];
+          if (g.beta != 0.0) v += g.beta * *cp;
+          *cp = v;
+        } else {
+          W[row * g.N + col] = acc[i][j][h];
+        }
+      }
+    }
+  }
+}
+
+__global__ void splitk_reduce_kernel(const double* ws, int splits, int batch, int64_t M, int64_t N, double alpha,
+                                     double beta, double* C, int64_t c_rs, int64_t c_cs, int64_t c_bs) {
+  const int64_t MN = M * N;
+  const int64_t total = MN * batch;
+  for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total;
+       idx += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t b = idx / MN, e = idx % MN;
+    const int64_t r = e / N, c = e % N;
+    const double* w = ws + b * splits * MN + e;
+    double s = 0.0;
+    for (int k = 0; k < splits; ++k) s += w[k * MN];
+    double* cp = C + b * c_bs + r * c_rs + c * c_cs;
+    double v = alpha * s;
+    if (beta != 0.0) v += beta * *cp;
+    *cp = v;
+  }
+}
+
+template <class C>
+int launch(Context* ctx, const KArgs& g, int batch) {
+  static bool attr_set = false;
+  auto kern = dgemm_kernel<C>;
+  if (!attr_set) {
+    MB_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(C::SMEM)));
+    attr_set = true;
+  }
+  dim3 grid(unsigned(cdiv(g.N, C::BN)), unsigned(cdiv(g.M, C::BM)), unsigned(batch * g.splits));
+  kern<<<grid, C::THREADS, C::SMEM, ctx->stream>>>(g);
+  ctx->kernels_launched++;
+  MB_CHECK_CUDA(cudaGetLastError());
+  return MCNLA_B200_OK;
+}
+
+// Tile shape families, picked by the output shape.
+enum Shape { S128x128 = 0, S128x64 = 1, S64x64 = 2, S128x32 = 3, S64x32 = 4 };
+
+template <bool AK, bool BKM, int VEC>
+int dispatch_shape(Context* ctx, const KArgs& g, int batch, Shape s) {
+  switch (s) {
+    case S128x128: return launch<Cfg<128, 128, 64, 32, AK, BKM, VEC, 4>>(ctx, g, batch);
+    case S128x64: return launch<Cfg<128, 64, 32, 32, AK, BKM, VEC, 4>>(ctx, g, batch);
+    case S64x64: return launch<Cfg<64, 64, 32, 32, AK, BKM, VEC, 4>>(ctx, g, batch);
+    case S128x32: return launch<Cfg<128, 32, 32, 16, AK, BKM, VEC, 4>>(ctx, g, batch);
+    default: return launch<Cfg<64, 32, 32, 16, AK, BKM, VEC, 4>>(ctx, g, batch);
+  }
+}
+
+struct Plan {
+  Shape shape;
+  int bm, bn;
+  int splits;
+  int64_t kps;
+};
+
+Plan make_plan(const Context* ctx, int64_t M, int64_t N, int64_t K, int batch, int force_splits) {
+  Plan p;
+  if (N <= 32) { p.shape = M <= 64 ? S64x32 : S128x32; p.bn = 32; }
+  else if (N <= 64) { p.shape = M <= 64 ? S64x64 : S128x64; p.bn = 64; }
+  else { p.shape = M <= 64 ? S64x64 : S128x128; p.bn = M <= 64 ? 64 : 128; }
+  p.bm = (p.shape == S64x64 || p.shape == S64x32) ? 64 : 128;
+  const int64_t tiles = cdiv(M, p.bm) * cdiv(N, p.bn) * batch;
+  int splits = 1;
+  const int64_t target = 2 * int64_t(ctx->num_sms);
+  if (force_splits > 0) {
+    splits = force_splits;
+  } else if (tiles < target && K >= 8 * BK) {
+    int64_t want = cdiv(target, tiles);
+    int64_t maxs = K / (8 * BK);           // at least 128 of K per split
+    splits = int(std::max<int64_t>(1, std::min<int64_t>({want, maxs, 128})));
+  }
+  int64_t kps = cdiv(cdiv(K, splits), BK) * BK;
+  if (kps == 0) kps = BK;
+  splits = int(std::max<int64_t>(1, cdiv(K, kps)));
+  p.splits = splits;
+  p.kps = kps;
+  return p;
+}
+
+}  // namespace
+
+size_t dgemm_workspace_bytes(const Context* c, int64_t M, int64_t N, int64_t K, int batch) {
+  if (M <= 0 || N <= 0) return 0;
+  Plan p = make_plan(c, M, N, K, batch, 0);
+  return p.splits > 1 ? size_t(p.splits) * batch * M * N * sizeof(double) : 0;
+}
+
+int dgemm(Context* ctx, int64_t M, int64_t N, int64_t K, double alpha, CMat A, CMat B, double beta, DMat Cm,
+          GemmBatch batch, double* ws, int force_splits) {
+  if (M < 0 || N < 0 || K < 0 || batch.count < 1) return MCNLA_B200_ERR_SHAPE;
+  if (M == 0 || N == 0) return MCNLA_B200_OK;
+  bool AK, BKM;
+  if (A.cs == 1) AK = true; else if (A.rs == 1) AK = false; else return MCNLA_B200_ERR_LAYOUT;
+  if (B.cs == 1) BKM = false; else if (B.rs == 1) BKM = true; else return MCNLA_B200_ERR_LAYOUT;
+  const int64_t lda = AK ? A.rs : A.cs;
+  const int64_t ldb = BKM ? B.cs : B.rs;
+  auto al16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+  const bool vec2 = al16(A.p) && al16(B.p) && (lda % 2 == 0 || (AK ? M == 1 : K == 1)) &&
+                    (ldb % 2 == 0 || (BKM ? N == 1 : K == 1)) && batch.a % 2 == 0 && batch.b % 2 == 0;
+  Plan p = make_plan(ctx, M, N, K, batch.count, force_splits);
+  KArgs g;
+  g.M = M; g.N = N; g.K = K; g.alpha = alpha; g.beta = beta;
+  g.A = A.p; g.a_rs = A.rs; g.a_cs = A.cs; g.a_bs = batch.a;
+  g.B = B.p; g.b_rs = B.rs; g.b_cs = B.cs; g.b_bs = batch.b;
+  g.C = Cm.p; g.c_rs = Cm.rs; g.c_cs = Cm.cs; g.c_bs = batch.c;
+  g.splits = p.splits; g.kps = p.kps;
+  g.ws = nullptr;
+  if (p.splits > 1) {
+    const size_t need = size_t(p.splits) * batch.count * M * N * sizeof(double);
+    if (!ws || ws != ctx->gws || need > ctx->gws_bytes) return MCNLA_B200_ERR_WORKSPACE;
+    g.ws = ws;
+  }
+  int st;
+  if (AK && BKM) st = vec2 ? dispatch_shape<true, true, 2>(ctx, g, batch.count, p.shape)
+                           : dispatch_shape<true, true, 1>(ctx, g, batch.count, p.shape);
+  else if (AK) st = vec2 ? dispatch_shape<true, false, 2>(ctx, g, batch.count, p.shape)
+                         : dispatch_shape<true, false, 1>(ctx, g, batch.count, p.shape);
+  else if (BKM) st = vec2 ? dispatch_shape<false, true, 2>(ctx, g, batch.count, p.shape)
+                          : dispatch_shape<false, true, 1>(ctx, g, batch.count, p.shape);
+  else st = vec2 ? dispatch_shape<false, false, 2>(ctx, g, batch.count, p.shape)
+                 : dispatch_shape<false, false, 1>(ctx, g, batch.count, p.shape);
+  if (st != MCNLA_B200_OK) return st;
+  if (p.splits > 1) {
+    const int64_t total = M * N * batch.count;
+    const int threads = 256;
+    const int blocks = int(std::min<int64_t>(cdiv(total, threads), int64_t(ctx->num_sms) * 8));
+    splitk_reduce_kernel<<<blocks, threads, 0, ctx->stream>>>(ws, p.splits, batch.count, M, N, alpha, beta, Cm.p,
+                                                             Cm.rs, Cm.cs, batch.c);
+    ctx->kernels_launched++;
+    MB_CHECK_CUDA(cudaGetLastError());
+  }
+  return MCNLA_B200_OK;
+}
+
+}  // namespace mb

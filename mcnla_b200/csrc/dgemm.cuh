@@ -1,0 +1,33 @@
+// FP64 GEMM on the sm_100a double-precision MMA (mma.sync m8n8k4 f64), the
+// arithmetic core of the plain FP64 iSVD path.  tcgen05 has no f64 kind, so
+// the FP64 path runs on DMMA; operand tiles are staged global -> shared memory
+// with cp.async in a multi-stage pipeline.
+//
+//   C(M x N) := alpha * A(M x K) * B(K x N) + beta * C
+//
+// A, B, C are strided views (element (i, j) at p[i*rs + j*cs]).  Each of A and
+// B must have one unit stride; the kernel is specialised on which one.
+// Batched calls add a per-batch element stride to every pointer.  Split-K
+// (over the K = m reductions of tall-skinny products) writes raw partial tiles
+// to a workspace and reduces them in a fixed order, so results are
+// deterministic run to run.
+#pragma once
+#include "common.cuh"
+
+namespace mb {
+
+struct GemmBatch {
+  int count = 1;
+  int64_t a = 0, b = 0, c = 0;   // element strides between batch members
+};
+
+// Bytes of workspace dgemm() needs for this shape (0 when no split-K is used).
+size_t dgemm_workspace_bytes(const Context* c, int64_t M, int64_t N, int64_t K, int batch);
+
+// Launches C := alpha*A*B + beta*C on ctx->stream.  ws may be null when
+// dgemm_workspace_bytes() is 0.  force_splits > 0 overrides the split choice
+// (tests use it to cover the split-K path at small sizes).
+int dgemm(Context* ctx, int64_t M, int64_t N, int64_t K, double alpha, CMat A, CMat B, double beta, DMat C,
+          GemmBatch batch = GemmBatch(), double* ws = nullptr, int force_splits = 0);
+
+}  // namespace mb

@@ -1,0 +1,783 @@
+// Small and elementwise kernels of the iSVD stages (see kernels.cuh).
+#include "kernels.cuh"
+#include "small.cuh"
+#include <algorithm>
+
+namespace mb {
+namespace {
+
+constexpr int kSmallThreads = 512;
+constexpr int kMaxSweeps = 40;
+
+// Shared-memory carve-up shared by the one-CTA solvers.
+struct SmemCarve {
+  char* base;
+  size_t off = 0;
+  __device__ explicit SmemCarve(char* b) : base(b) {}
+  template <class T>
+  __device__ T* take(size_t n) {
+    off = (off + 15) & ~size_t(15);
+    T* p = reinterpret_cast<T*>(base + off);
+    off += n * sizeof(T);
+    return p;
+  }
+};
+
+__host__ __device__ inline size_t jacobi_scratch_bytes(int n) {
+  const int np = (n + 2) / 2;
+  return 6 * (np * 8 + 16) + 2 * (np * 4 + 16) + 16 + 32 * 8 + 16 + (n + 4) * 4 + 64;
+}
+
+__device__ small::JacobiScratch carve_jacobi(SmemCarve& sc, int n) {
+  const int np = (n + 2) / 2;
+  small::JacobiScratch js;
+  js.c = sc.take<double>(np);
+  js.s = sc.take<double>(np);
+  js.t = sc.take<double>(np);
+  js.apq = sc.take<double>(np);
+  js.app = sc.take<double>(np);
+  js.aqq = sc.take<double>(np);
+  js.p = sc.take<int>(np);
+  js.q = sc.take<int>(np);
+  js.count = sc.take<int>(1);
+  js.red = sc.take<double>(32);
+  return js;
+}
+
+// rank[j] = position of eigenvalue j in the requested order (ties by index).
+__device__ void eig_ranks(const double* a, int lda, int n, int order, int* rank) {
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    const double dj = order ? fabs(a[j * lda + j]) : a[j * lda + j];
+    int r = 0;
+    for (int i = 0; i < n; ++i) {
+      const double di = order ? fabs(a[i * lda + i]) : a[i * lda + i];
+      const bool before = order ? (di > dj || (di == dj && i < j)) : (di < dj || (di == dj && i < j));
+      r += before ? 1 : 0;
+    }
+    rank[j] = r;
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// batched symmetric eigendecomposition
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kSmallThreads) k_syev(int n, const double* A, int64_t lda, int64_t a_bs,
+                                                        double* W, double* V, int order, int v_smem,
+                                                        double* vwork_all) {
+  extern __shared__ __align__(16) char smem_raw[];
+  SmemCarve sc(smem_raw);
+  const int ld = n + 1;
+  double* a = sc.take<double>(size_t(n) * ld);
+  double* v;
+  int ldv;
+  if (v_smem) { v = sc.take<double>(size_t(n) * ld); ldv = ld; }
+  else { v = vwork_all + size_t(blockIdx.x) * n * n; ldv = n; }
+  small::JacobiScratch js = carve_jacobi(sc, n);
+  int* rank = sc.take<int>(n);
+  const double* Ab = A + blockIdx.x * a_bs;
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) a[(e / n) * ld + (e % n)] = Ab[(e / n) * lda + (e % n)];
+  __syncthreads();
+  small::cta_jacobi_eig(a, ld, v, ldv, n, true, js, kMaxSweeps);
+  eig_ranks(a, ld, n, order, rank);
+  double* Wb = W + size_t(blockIdx.x) * n;
+  double* Vb = V + size_t(blockIdx.x) * n * n;
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    const double d = a[j * ld + j];
+    Wb[rank[j]] = order ? fabs(d) : d;
+  }
+  if (v_smem) {
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+      const int i = e / n, j = e % n;
+      Vb[i * n + rank[j]] = v[i * ldv + j];
+    }
+  } else {
+    __syncthreads();
+    // permute columns out of the global work copy
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+      const int i = e / n, j = e % n;
+      Vb[i * n + rank[j]] = v[i * ldv + j];
+    }
+  }
+}
+
+__global__ void k_scale_cols_rsqrt(int n, int batch, const double* V, const double* W, double* T) {
+  const int64_t total = int64_t(batch) * n * n;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t b = e / (int64_t(n) * n);
+    const int j = int(e % n);
+    T[e] = V[e] / sqrt(W[b * n + j]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Kolmogorov-Nagumo step
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kSmallThreads) k_kn_step(int l, const double* z_in, const double* dd,
+                                                           double inv_n, double* out, double* outn,
+                                                           const double* ff, double* ffn, double* vwork,
+                                                           int v_smem, DevScalars* scal) {
+  extern __shared__ __align__(16) char smem_raw[];
+  SmemCarve sc(smem_raw);
+  const int ld = l + 1;
+  double* a = sc.take<double>(size_t(l) * ld);
+  double* v;
+  int ldv;
+  if (v_smem) { v = sc.take<double>(size_t(l) * ld); ldv = ld; }
+  else { v = vwork; ldv = l; }
+  small::JacobiScratch js = carve_jacobi(sc, l);
+  double* sv = sc.take<double>(l);    // sqrt(s)
+  const int tid = threadIdx.x, nt = blockDim.x;
+  // Z
+  if (dd == nullptr) {
+    for (int e = tid; e < l * l; e += nt) a[(e / l) * ld + (e % l)] = z_in[e];
+  } else {
+    // Z := Dgc - Dc * Dc'   (Dc = dd(:, 0:l), Dgc = dd(:, l:2l), row stride 2l)
+    // row_block_kolmogorov_nagumo_integrator.hpp:150-156
+    const int ldd = 2 * l;
+    for (int e = tid; e < l * l; e += nt) {
+      const int i = e / l, j = e % l;
+      double s = 0.0;
+      for (int k = 0; k < l; ++k) s = fma(dd[i * ldd + k], dd[j * ldd + k], s);
+      a[i * ld + j] = dd[i * ldd + l + j] - s;
+    }
+  }
+  __syncthreads();
+  const int sweeps = small::cta_jacobi_eig(a, ld, v, ldv, l, true, js, kMaxSweeps);
+  // s := sqrt(1/2 + sqrt(1/4 - lambda)); ss := sqrt(s)
+  double part = 0.0;
+  for (int i = tid; i < l; i += nt) {
+    const double s = sqrt(0.5 + sqrt(0.25 - a[i * ld + i]));
+    sv[i] = sqrt(s);
+    part += (s - 1.0) * (s - 1.0);
+  }
+  const double norm2 = small::cta_sum(part, js.red);
+  // C = V diag(s) V', inv(C) = V diag(1/s) V'  -> out rows [0, l) hold C or Fc,
+  // rows [l, 2l) hold inv(C).
+  double* cmat = out;                 // l x l, row-major (ld l)
+  double* cinv = out + size_t(l) * l;
+  for (int e = tid; e < l * l; e += nt) {
+    const int i = e / l, j = e % l;
+    double c = 0.0, ci = 0.0;
+    for (int k = 0; k < l; ++k) {
+      const double x = v[i * ldv + k] * sv[k], y = v[j * ldv + k] * sv[k];
+      const double xi = v[i * ldv + k] / sv[k], yi = v[j * ldv + k] / sv[k];
+      c = fma(x, y, c);
+      ci = fma(xi, yi, ci);
+    }
+    cmat[i * l + j] = c;
+    cinv[i * l + j] = ci;
+  }
+  __syncthreads();
+  if (dd != nullptr) {
+    // Fc := C - Dc * inv(C)   (row_block_kolmogorov_nagumo_integrator.hpp:186)
+    // computed into the Jacobi matrix space, then written over C
+    const int ldd = 2 * l;
+    for (int e = tid; e < l * l; e += nt) {
+      const int i = e / l, j = e % l;
+      double s = 0.0;
+      for (int k = 0; k < l; ++k) s = fma(dd[i * ldd + k], cinv[k * l + j], s);
+      a[i * ld + j] = cmat[i * l + j] - s;
+    }
+    __syncthreads();
+    for (int e = tid; e < l * l; e += nt) cmat[e] = a[(e / l) * ld + (e % l)];
+    __syncthreads();
+    if (outn) {
+      for (int e = tid; e < l * l; e += nt) {
+        outn[e] = cmat[e];
+        outn[size_t(l) * l + e] = cinv[e] * inv_n;
+      }
+    }
+    if (ff && ffn) {
+      // F~+ := F~c * Fc  (row_block_gramian_kolmogorov_nagumo_integrator.hpp:197)
+      for (int e = tid; e < l * l; e += nt) {
+        const int i = e / l, j = e % l;
+        double s = 0.0;
+        for (int k = 0; k < l; ++k) s = fma(ff[i * l + k], a[k * ld + j], s);
+        ffn[i * l + j] = s;
+      }
+    }
+  }
+  if (tid == 0) {
+    scal->norm = sqrt(norm2);
+    scal->sweeps = sweeps;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Wen-Yin trial
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kSmallThreads) k_wy_trial(int l, const double* dd, double tau, double inv_n,
+                                                            double* F, double* FN, DevScalars* scal) {
+  extern __shared__ __align__(16) char smem_raw[];
+  SmemCarve sc(smem_raw);
+  const int n = 2 * l, ld = n + 1, ldd = 2 * l;
+  double* cm = sc.take<double>(size_t(n) * ld);
+  int* piv = sc.take<int>(n);
+  double* col = sc.take<double>(n);
+  double* rv = sc.take<double>(4);
+  int* ri = sc.take<int>(4);
+  int* flag = sc.take<int>(4);
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const double it = 1.0 / tau;
+  // C := [ Dc/2 - I/tau , I/2 ; -Dgc/2 , -Dc/2 - I/tau ]
+  // (row_block_wen_yin_integrator.hpp:176-183)
+  for (int e = tid; e < n * n; e += nt) {
+    const int i = e / n, j = e % n;
+    const int bi = i / l, bj = j / l, ii = i % l, jj = j % l;
+    double x;
+    if (bi == 0 && bj == 0) x = 0.5 * dd[ii * ldd + jj] - (ii == jj ? it : 0.0);
+    else if (bi == 0) x = (ii == jj) ? 0.5 : 0.0;
+    else if (bj == 0) x = -0.5 * dd[ii * ldd + l + jj];
+    else x = -0.5 * dd[ii * ldd + jj] - (ii == jj ? it : 0.0);
+    cm[i * ld + j] = x;
+  }
+  __syncthreads();
+  const int sing = small::cta_gj_inverse(cm, ld, n, piv, col, rv, ri, flag);
+  if (sing) {
+    if (tid == 0) scal->status = MCNLA_B200_ERR_SINGULAR;
+    return;
+  }
+  // T := inv(C)(:, l:2l) * Dc - inv(C)(:, 0:l); Fgc = T(0:l, :), Fc = T(l:2l, :) + I
+  // F = [Fc; Fgc]   (row_block_wen_yin_integrator.hpp:189-193)
+  for (int e = tid; e < n * l; e += nt) {
+    const int i = e / l, j = e % l;
+    double s = 0.0;
+    for (int k = 0; k < l; ++k) s = fma(cm[i * ld + l + k], dd[k * ldd + j], s);
+    s -= cm[i * ld + j];
+    if (i >= l) {   // Fc row
+      const int r = i - l;
+      const double fc = s + (r == j ? 1.0 : 0.0);
+      F[r * l + j] = fc;
+      if (FN) FN[r * l + j] = fc;
+    } else {        // Fgc row
+      F[size_t(l) * l + i * l + j] = s;
+      if (FN) FN[size_t(l) * l + i * l + j] = s * inv_n;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// one-sided Jacobi SVD of a small square matrix
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kSmallThreads) k_svd_small(int n, const double* M, double* W, double* sig,
+                                                             double* Z, double* zwork, int z_smem) {
+  extern __shared__ __align__(16) char smem_raw[];
+  SmemCarve sc(smem_raw);
+  const int ld = n + 1;
+  double* a = sc.take<double>(size_t(n) * ld);
+  double* z;
+  int ldz;
+  if (z_smem) { z = sc.take<double>(size_t(n) * ld); ldz = ld; }
+  else { z = zwork; ldz = n; }
+  int* count = sc.take<int>(4);
+  int* rank = sc.take<int>(n);
+  double* nrm = sc.take<double>(n);
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
+  for (int e = tid; e < n * n; e += nt) {
+    const int i = e / n, j = e % n;
+    a[i * ld + j] = M[e];
+    z[i * ldz + j] = (i == j) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  const int P = (n + 1) & ~1, npairs = P / 2;
+  for (int sweep = 0; sweep < 40 && n > 1; ++sweep) {
+    if (tid == 0) *count = 0;
+    __syncthreads();
+    for (int r = 0; r < P - 1; ++r) {
+      for (int k = warp; k < npairs; k += nwarps) {
+        int p, q;
+        small::rr_pair(P, r, k, p, q);
+        if (q >= n) continue;
+        double al = 0.0, be = 0.0, ga = 0.0;
+        for (int i = lane; i < n; i += 32) {
+          const double x = a[i * ld + p], y = a[i * ld + q];
+          al = fma(x, x, al);
+          be = fma(y, y, be);
+          ga = fma(x, y, ga);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+          al += __shfl_xor_sync(0xffffffffu, al, o);
+          be += __shfl_xor_sync(0xffffffffu, be, o);
+          ga += __shfl_xor_sync(0xffffffffu, ga, o);
+        }
+        if (fabs(ga) > 1e-15 * sqrt(al * be) && ga * ga > 1e-300) {
+          const double zeta = (be - al) / (2.0 * ga);
+          const double az = fabs(zeta);
+          const double t = (az > 1e150) ? 0.5 / zeta : ((zeta >= 0.0 ? 1.0 : -1.0) / (az + sqrt(1.0 + zeta * zeta)));
+          const double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
+          for (int i = lane; i < n; i += 32) {
+            const double x = a[i * ld + p], y = a[i * ld + q];
+            a[i * ld + p] = c * x - s * y;
+            a[i * ld + q] = s * x + c * y;
+            const double zx = z[i * ldz + p], zy = z[i * ldz + q];
+            z[i * ldz + p] = c * zx - s * zy;
+            z[i * ldz + q] = s * zx + c * zy;
+          }
+          if (lane == 0) atomicAdd(count, 1);
+        }
+      }
+      __syncthreads();
+    }
+    const int cnt = *count;
+    __syncthreads();
+    if (cnt == 0) break;
+  }
+  for (int j = warp; j < n; j += nwarps) {
+    double s = 0.0;
+    for (int i = lane; i < n; i += 32) s = fma(a[i * ld + j], a[i * ld + j], s);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) nrm[j] = sqrt(s);
+  }
+  __syncthreads();
+  for (int j = tid; j < n; j += nt) {
+    int r = 0;
+    for (int i = 0; i < n; ++i) r += (nrm[i] > nrm[j] || (nrm[i] == nrm[j] && i < j)) ? 1 : 0;
+    rank[j] = r;
+    sig[r] = nrm[j];
+  }
+  __syncthreads();
+  for (int e = tid; e < n * n; e += nt) {
+    const int i = e / n, j = e % n;
+    const double sj = nrm[j];
+    W[i * n + rank[j]] = sj > 0.0 ? a[i * ld + j] / sj : 0.0;
+    Z[i * n + rank[j]] = z[i * ldz + j];
+  }
+}
+
+__global__ void k_rsqrt_rows_t(int n, const double* Ue, const double* w, double* P) {
+  const double floor = (n * 2.220446049250313e-16) * (n * 2.220446049250313e-16) * fabs(w[0]);
+  for (int e = threadIdx.x + blockIdx.x * blockDim.x; e < n * n; e += blockDim.x * gridDim.x) {
+    const int i = e / n, j = e % n;
+    const double wi = w[i];
+    P[e] = (wi > floor && wi > 0.0) ? Ue[j * n + i] / sqrt(wi) : 0.0;
+  }
+}
+
+__global__ void k_scale_cols(int64_t rows, int64_t cols, const double* X, int64_t ldx, const double* s, int mode,
+                             double* Y, int64_t ldy) {
+  const int64_t total = rows * cols;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t r = e / cols, c = e % cols;
+    const double f = mode == 0 ? 1.0 / s[c] : (mode == 1 ? s[c] : 1.0 / sqrt(s[c]));
+    Y[r * ldy + c] = X[r * ldx + c] * f;
+  }
+}
+
+__global__ void k_sqrt_vec(int n, const double* w, double* out) {
+  for (int i = threadIdx.x + blockIdx.x * blockDim.x; i < n; i += blockDim.x * gridDim.x) out[i] = sqrt(w[i]);
+}
+
+__global__ void __launch_bounds__(kSmallThreads) k_inverse(int n, double* A, DevScalars* scal) {
+  extern __shared__ __align__(16) char smem_raw[];
+  SmemCarve sc(smem_raw);
+  const int ld = n + 1;
+  double* a = sc.take<double>(size_t(n) * ld);
+  int* piv = sc.take<int>(n);
+  double* col = sc.take<double>(n);
+  double* rv = sc.take<double>(4);
+  int* ri = sc.take<int>(4);
+  int* flag = sc.take<int>(4);
+  double* Ab = A + size_t(blockIdx.x) * n * n;
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) a[(e / n) * ld + (e % n)] = Ab[e];
+  __syncthreads();
+  const int sing = small::cta_gj_inverse(a, ld, n, piv, col, rv, ri, flag);
+  if (sing) {
+    if (threadIdx.x == 0) scal->status = MCNLA_B200_ERR_SINGULAR;
+    return;
+  }
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) Ab[e] = a[(e / n) * ld + (e % n)];
+}
+
+// ---------------------------------------------------------------------------
+// deterministic reductions
+// ---------------------------------------------------------------------------
+constexpr int kRedThreads = 256;
+
+__device__ inline double block_sum(double v) {
+  __shared__ double red[32];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0) {
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+  }
+  __syncthreads();
+  return t;
+}
+
+__global__ void k_dot_partial(const double* X, int64_t ldx, const double* Y, int64_t ldy, int64_t rows,
+                              int64_t cols, double* partials) {
+  const int64_t total = rows * cols;
+  double s = 0.0;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t r = e / cols, c = e % cols;
+    s = fma(X[r * ldx + c], Y[r * ldy + c], s);
+  }
+  s = block_sum(s);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+__global__ void k_wy_delta_partial(const double* qc, const double* qp, int64_t ldq, const double* xc,
+                                   const double* xp, int64_t ldx, int64_t rows, int64_t cols, double* partials) {
+  const int64_t total = rows * cols;
+  double s11 = 0.0, s12 = 0.0, s22 = 0.0;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t r = e / cols, c = e % cols;
+    const double d1 = qc[r * ldq + c] - qp[r * ldq + c];
+    const double d2 = xc[r * ldx + c] - xp[r * ldx + c];
+    s11 = fma(d1, d1, s11);
+    s12 = fma(d1, d2, s12);
+    s22 = fma(d2, d2, s22);
+  }
+  s11 = block_sum(s11);
+  s12 = block_sum(s12);
+  s22 = block_sum(s22);
+  if (threadIdx.x == 0) {
+    partials[3 * blockIdx.x + 0] = s11;
+    partials[3 * blockIdx.x + 1] = s12;
+    partials[3 * blockIdx.x + 2] = s22;
+  }
+}
+
+// Sums `count` groups of `width` partials in a fixed order: out[w] = scale * sum_b p[b*width + w].
+__global__ void k_final_sum(const double* partials, int count, int width, double scale, double* out) {
+  for (int w = 0; w < width; ++w) {
+    double s = 0.0;
+    for (int b = threadIdx.x; b < count; b += blockDim.x) s += partials[b * width + w];
+    s = block_sum(s);
+    if (threadIdx.x == 0) out[w] = scale * s;
+  }
+}
+
+__global__ void k_gwy_small_dots(int l, const double* p1, const double* p2, const double* bcu, double* out) {
+  double s[7] = {0, 0, 0, 0, 0, 0, 0};
+  const int ldb = 2 * l;
+  for (int e = threadIdx.x; e < l * l; e += blockDim.x) {
+    const int i = e / l, j = e % l;
+    const double a = p1[e], b = p2[e], u1 = bcu[i * ldb + j], u2 = bcu[i * ldb + l + j];
+    s[0] = fma(a, a, s[0]);
+    s[1] = fma(a, b, s[1]);
+    s[2] = fma(b, b, s[2]);
+    s[3] = fma(a, u1, s[3]);
+    s[4] = fma(a, u2, s[4]);
+    s[5] = fma(b, u1, s[5]);
+    s[6] = fma(b, u2, s[6]);
+  }
+  for (int k = 0; k < 7; ++k) {
+    const double t = block_sum(s[k]);
+    if (threadIdx.x == 0) out[k] = t;
+  }
+}
+
+__global__ void k_wy_mu(int l, const double* dd, double* out) {
+  // mu := asum(diag(Dgc)) - ||Dc||_F^2   (row_block_wen_yin_integrator.hpp:143)
+  const int ldd = 2 * l;
+  double s = 0.0;
+  for (int e = threadIdx.x; e < l * l; e += blockDim.x) {
+    const int i = e / l, j = e % l;
+    const double d = dd[i * ldd + j];
+    s -= d * d;
+    if (i == j) s += fabs(dd[i * ldd + l + j]);
+  }
+  s = block_sum(s);
+  if (threadIdx.x == 0) *out = s;
+}
+
+// ---------------------------------------------------------------------------
+// elementwise
+// ---------------------------------------------------------------------------
+__global__ void k_axpby(int64_t rows, int64_t cols, double alpha, const double* X, int64_t ldx, double beta,
+                        double* Y, int64_t ldy) {
+  const int64_t total = rows * cols;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t r = e / cols, c = e % cols;
+    const double x = alpha * X[r * ldx + c];
+    Y[r * ldy + c] = (beta == 0.0) ? x : x + beta * Y[r * ldy + c];
+  }
+}
+
+__global__ void k_fill(int64_t rows, int64_t cols, double v, double* X, int64_t ld, int identity) {
+  const int64_t total = rows * cols;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t r = e / cols, c = e % cols;
+    X[r * ld + c] = identity ? (r == c ? 1.0 : 0.0) : v;
+  }
+}
+
+__global__ void k_gramian_prepare(int64_t L, int l, double* bs, double* bc, int64_t ldbc) {
+  // Bs(i, j) := Bs(j, i) for i < j (keep the lower triangle, as the reference's
+  // syrk into Bs.syml() does); Bc := Bs(:, 0:l) with the strict upper triangle
+  // of its top l x l block zero (row_block_gramian_kolmogorov_nagumo_integrator.hpp:112-125).
+  const int64_t total = L * L;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t i = e / L, j = e % L;
+    if (i < j) bs[i * L + j] = bs[j * L + i];
+    if (j < l) bc[i * ldbc + j] = (i < j) ? 0.0 : bs[(i >= j ? i * L + j : j * L + i)];
+  }
+}
+
+__global__ void k_wy_gramian_phis(int l, const double* F, const double* dc, int64_t lddc, const double* dp,
+                                  int64_t lddp, double* phi1, double* phi2) {
+  // Phi1 := Fc - I; Phi2 := Dc - Fc * D+  (row_block_gramian_wen_yin_integrator.hpp:261-266)
+  for (int e = threadIdx.x + blockIdx.x * blockDim.x; e < l * l; e += blockDim.x * gridDim.x) {
+    const int i = e / l, j = e % l;
+    const double* fc = F;  // rows [0, l) of F
+    double s = 0.0;
+    for (int k = 0; k < l; ++k) s = fma(fc[i * l + k], dp[k * lddp + j], s);
+    phi2[e] = dc[i * lddc + j] - s;
+    phi1[e] = fc[e] - (i == j ? 1.0 : 0.0);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Philox-4x32-10 (Salmon, Moraes, Dror, Shaw: "Parallel random numbers: as easy
+// as 1, 2, 3", SC'11) + Box-Muller.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void philox_round(uint32_t c[4], uint32_t k0, uint32_t k1) {
+  const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+  const uint32_t hi0 = __umulhi(M0, c[0]), lo0 = M0 * c[0];
+  const uint32_t hi1 = __umulhi(M1, c[2]), lo1 = M1 * c[2];
+  const uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+  c[0] = n0; c[1] = lo1; c[2] = n2; c[3] = lo0;
+}
+
+__global__ void k_gaussian(uint64_t seed, int64_t count, double* out) {
+  const int64_t pairs = (count + 1) / 2;
+  for (int64_t j = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; j < pairs; j += int64_t(gridDim.x) * blockDim.x) {
+    uint32_t c[4] = {uint32_t(j), uint32_t(uint64_t(j) >> 32), 0u, 0u};
+    uint32_t k0 = uint32_t(seed), k1 = uint32_t(seed >> 32);
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+      philox_round(c, k0, k1);
+      k0 += 0x9E3779B9u;
+      k1 += 0xBB67AE85u;
+    }
+    // two 53-bit uniforms in (0, 1)
+    const uint64_t b1 = ((uint64_t(c[0]) << 32) | c[1]) >> 11;
+    const uint64_t b2 = ((uint64_t(c[2]) << 32) | c[3]) >> 11;
+    const double u1 = (double(b1) + 0.5) * 0x1.0p-53;
+    const double u2 = (double(b2) + 0.5) * 0x1.0p-53;
+    const double r = sqrt(-2.0 * log(u1));
+    double sn, cs;
+    sincospi(2.0 * u2, &sn, &cs);
+    out[2 * j] = r * cs;
+    if (2 * j + 1 < count) out[2 * j + 1] = r * sn;
+  }
+}
+
+int grid_for(const Context* c, int64_t total, int threads) {
+  return int(std::max<int64_t>(1, std::min<int64_t>(cdiv(total, threads), int64_t(c->num_sms) * 16)));
+}
+
+size_t small_smem_syev(int n, bool v_smem) {
+  const size_t mat = size_t(n) * (n + 1) * sizeof(double) + 16;
+  return mat * (v_smem ? 2 : 1) + jacobi_scratch_bytes(n) + (n + 4) * sizeof(int) + 64;
+}
+
+int set_smem(const void* fn, size_t bytes) {
+  MB_CHECK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+  return MCNLA_B200_OK;
+}
+
+}  // namespace
+
+int reduce_partials(const Context* c) { return c->num_sms * 2; }
+
+int launch_syev(Context* c, int n, int batch, const double* A, int64_t lda, int64_t a_bs, double* W, double* V,
+                int order) {
+  if (n < 1 || n > MCNLA_B200_MAX_DIM_SKETCH || batch < 1) return MCNLA_B200_ERR_UNSUPPORTED;
+  bool v_smem = small_smem_syev(n, true) <= c->smem_optin;
+  double* vwork = nullptr;
+  if (!v_smem) {
+    // global eigenvector work copies (one n x n per matrix); from the arena
+    vwork = ctx_take<double>(c, size_t(batch) * n * n);
+    if (!vwork) return MCNLA_B200_ERR_WORKSPACE;
+  }
+  const size_t smem = small_smem_syev(n, v_smem);
+  if (smem > c->smem_optin) return MCNLA_B200_ERR_UNSUPPORTED;
+  MB_CHECK(set_smem(reinterpret_cast<const void*>(k_syev), smem));
+  k_syev<<<batch, kSmallThreads, smem, c->stream>>>(n, A, lda, a_bs, W, V, order, v_smem ? 1 : 0, vwork);
+  c->kernels_launched++;
+  MB_CHECK_CUDA(cudaGetLastError());
+  return MCNLA_B200_OK;
+}
+
+int launch_scale_cols_rsqrt(Context* c, int n, int batch, const double* V, const double* W, double* T) {
+  const int64_t total = int64_t(batch) * n * n;
+  k_scale_cols_rsqrt<<<grid_for(c, total, 256), 256, 0, c->stream>>>(n, batch, V, W, T);
+  c->kernels_launched++;
+  MB_CHECK_CUDA(cudaGetLastError());
+  return MCNLA_B200_OK;
+}
+
+int launch_kn_step(Context* c, int l, const double* z, const double* dd, double inv_n, double* out, double* outn,
+                   const double* ff, double* ffn, double* vwork) {
+  if (l < 1 || l > MCNLA_B200_MAX_DIM_SKETCH) return MCNLA_B200_ERR_UNSUPPORTED;
+  const bool v_smem = small_smem_syev(l, true) + l * 8 + 64 <= c->smem_optin;
+  const size_t smem = small_smem_syev(l, v_smem) + l * 8 + 64;
+  if (smem > c->smem_optin) return MCNLA_B200_ERR_UNSUPPORTED;
+  MB_CHECK(set_smem(reinterpret_cast<const void*>(k_kn_step), smem));
+  k_kn_step<<<1, kSmallThreads, smem, c->stream>>>(l, z, dd, inv_n, out, outn, ff, ffn, vwork, v_smem ? 1 : 0,
+                                                    c->scal);
+  c->kernels_launched++;
+  MB_CHECK_CUDA(cudaGetLastError());
+  return MCNLA_B200_OK;
+}
+
+int launch_wy_trial(Context* c, int l, const double* dd, double tau, double inv_n, double* F, double* FN) {
+  if (l < 1 || l > MCNLA_B200_MAX_DIM_SKETCH_WENYIN) return MCNLA_B200_ERR_UNSUPPORTED;
+  const int n = 2 * l;
+  const size_t smem = size_t(n) * (n + 1) * 8 + 16 + n * 4 + 16 + n * 8 + 16 + 3 * 64 + 64;
+  if (smem > c->smem_optin) return MCNLA_B200_ERR_UNSUPPORTED;
+  MB_CHECK(set_smem(reinterpret_cast<const void*>(k_wy_trial), smem));
+  k_wy_trial<<<1, kSmallThreads, smem, c->stream>>>(l, dd, tau, inv_n, F, FN, c->scal);
+  c->kernels_launched++;
+  MB_CHECK_CUDA(cudaGetLastError());
+  return MCNLA_B200_OK;
+}
+
+int launch_sumsq(Context* c, const double* X, int64_t rows, int64_t cols, int64_t ld, double scale, double* partials,
+                 double* out) {
+  const int nb = reduce_partials(c);
+  k_dot_partial<<<nb, kRedThreads, 0, c->stream>>>(X, ld, X, ld, rows, cols, partials);
+  k_final_sum<<<1, kRedThreads, 0, c->stream>>>(partials, nb, 1, scale, out);
+  c->kernels_launched += 2;
+  MB_CHECK_CUDA(cudaGetLastError());
+  return MCNLA_B200_OK;
+}
+
+int launch_dot(Context* c, const double* X, int64_t ldx, const double* Y, int64_t ldy, int64_t rows, int64_t cols,
+               double* partials, double* out) {
+  const int nb = reduce_partials(c);
+  k_dot_partial<<<nb, kRedThreads, 0, c->stream>>>(X, ldx, Y, ldy, rows, cols, partials);
+  k_final_sum<<<1, kRedThreads, 0, c->stream>>>(partials, nb, 1, 1.0, out);
+  c->kernels_launched += 2;
+  MB_CHECK_CUDA(cudaGetLastError());
+  return MCNLA_B200_OK;
+}
+
+int launch_wy_delta_dots(Context* c, const double* qc, const double* qp, int64_t ldq, const double* xc,
+                         const double* xp, int64_t ldx, int64_t rows, int64_t cols, double* partials, double* out) {
+  const int nb = reduce_partials(c);
+  k_wy_delta_partial<<<nb, kRedThreads, 0, c->stream>>>(qc, qp, ldq, xc, xp, ldx, rows, cols, partials);
+  k_final_sum<<<1, kRedThreads, 0, c->stream>>>(partials, nb, 3, 1.0, out);
+  c->kernels_launched += 2;
+  MB_CHECK_CUDA(cudaGetLastError());
+  return MCNLA_B200_OK;
+}
+
+int launch_wy_mu(Context* c, int l, const double* dd, double* out) {
+  k_wy_mu<<<1, kRedThreads, 0, c->stream>>>(l, dd, out);
+  c->kernels_launched++;
+  MB_CHECK_CUDA(cudaGetLastError());
+  return MCNLA_B200_OK;
+}
+
+int launch_axpby(Context* c, int64_t rows, int64_t cols, double alpha, const double* X, int64_t ldx, double beta,
+                 double* Y, int64_t ldy) {
+  if (rows <= 0 || cols <= 0) return MCNLA_B200_OK;
+  k_axpby<<<grid_for(c, rows * cols, 256), 256, 0, c->stream>>>(rows, cols, alpha, X, ldx, beta, Y, ldy);
+  c->kernels_launched++;
+  MB_CHECK_CUDA(cudaGetLastError());
+  return MCNLA_B200_OK;
+}
+
+int launch_set_identity(Context* c, int64_t n, double* X, int64_t ld) {
+  k_fill<<<grid_for(c, n * n, 256), 256, 0, c->stream>>>(n, n, 0.0, X, ld, 1);
+  c->kernels_launched++;
+  MB_CHECK_CUDA(cudaGetLastError());
+  return MCNLA_B200_OK;
+}
+
+int launch_fill(Context* c, int64_t rows, int64_t cols, double v, double* X, int64_t ld) {
+  if (rows <= 0 || cols <= 0) return MCNLA_B200_OK;
+  k_fill<<<grid_for(c, rows * cols, 256), 256, 0, c->stream>>>(rows, cols, v, X, ld, 0);
+  c->kernels_launched++;
+  MB_CHECK_CUDA(cudaGetLastError());
+  return MCNLA_B200_OK;
+}
+
+int launch_gramian_prepare(Context* c, int64_t L, int l, double* bs, double* bc, int64_t ldbc) {
+  k_gramian_prepare<<<grid_for(c, L * L, 256), 256, 0, c->stream>>>(L, l, bs, bc, ldbc);
+  c->kernels_launched++;
+  MB_CHECK_CUDA(cudaGetLastError());
+  return MCNLA_B200_OK;
+}
+
+int launch_wy_gramian_phis(Context* c, int l, const double* F, const double* dc, int64_t lddc, const double* dp,
+                           int64_t lddp, double* phi1, double* phi2) {
+  k_wy_gramian_phis<<<grid_for(c, int64_t(l) * l, 256), 256, 0, c->stream>>>(l, F, dc, lddc, dp, lddp, phi1, phi2);
+  c->kernels_launched++;
+  MB_CHECK_CUDA(cudaGetLastError());
+  return MCNLA_B200_OK;
+}
+
+int launch_svd_small(Context* c, int n, const double* M, double* W, double* sig, double* Z) {
+  if (n < 1 || n > MCNLA_B200_MAX_DIM_SKETCH) return MCNLA_B200_ERR_UNSUPPORTED;
+  const size_t mat = size_t(n) * (n + 1) * 8 + 16;
+  const size_t extra = 64 + n * 4 + 16 + n * 8 + 16 + 64;
+  const bool z_smem = 2 * mat + extra <= c->smem_optin;
+  const size_t smem = (z_smem ? 2 : 1) * mat + extra;
+  if (smem > c->smem_optin) return MCNLA_B200_ERR_UNSUPPORTED;
+  double* zwork = z_smem ? nullptr : ctx_take<double>(c, size_t(n) * n);
+  if (!z_smem && !zwork) return MCNLA_B200_ERR_WORKSPACE;
+  MB_CHECK(set_smem(reinterpret_cast<const void*>(k_svd_small), smem));
+  k_svd_small<<<1, kSmallThreads, smem, c->stream>>>(n, M, W, sig, Z, zwork, z_smem ? 1 : 0);
+  c->kernels_launched++;
+  MB_CHECK_CUDA(cudaGetLastError());
+  return MCNLA_B200_OK;
+}
+
+int launch_rsqrt_rows_t(Context* c, int n, const double* Ue, const double* w, double* P) {
+  k_rsqrt_rows_t<<<grid_for(c, int64_t(n) * n, 256), 256, 0, c->stream>>>(n, Ue, w, P);
+  c->kernels_launched++;
+  MB_CHECK_CUDA(cudaGetLastError());
+  return MCNLA_B200_OK;
+}
+
+int launch_scale_cols(Context* c, int64_t rows, int64_t cols, const double* X, int64_t ldx, const double* s,
+                      int mode, double* Y, int64_t ldy) {
+  if (rows <= 0 || cols <= 0) return MCNLA_B200_OK;
+  k_scale_cols<<<grid_for(c, rows * cols, 256), 256, 0, c->stream>>>(rows, cols, X, ldx, s, mode, Y, ldy);
+  c->kernels_launched++;
+  MB_CHECK_CUDA(cudaGetLastError());
+  return MCNLA_B200_OK;
+}
+
+int launch_sqrt_vec(Context* c, int n, const double* w, double* out) {
+  k_sqrt_vec<<<1, 256, 0, c->stream>>>(n, w, out);
+  c->kernels_launched++;
+  MB_CHECK_CUDA(cudaGetLastError());
+  return MCNLA_B200_OK;
+}
+
+int launch_gwy_small_dots(Context* c, int l, const double* phi1, const double* phi2, const double* bcu, double* out) {
+  k_gwy_small_dots<<<1, kRedThreads, 0, c->stream>>>(l, phi1, phi2, bcu, out);
+  c->kernels_launched++;
+  MB_CHECK_CUDA(cudaGetLastError());
+  return MCNLA_B200_OK;
+}
+
+int launch_inverse(Context* c, int n, int batch, double* A) {
+  if (n < 1 || n > 2 * MCNLA_B200_MAX_DIM_SKETCH_WENYIN || batch < 1) return MCNLA_B200_ERR_UNSUPPORTED;
+  const size_t smem = size_t(n) * (n + 1) * 8 + 16 + n * 4 + 16 + n * 8 + 16 + 3 * 64 + 64;
+  if (smem > c->smem_optin) return MCNLA_B200_ERR_UNSUPPORTED;
+  MB_CHECK(set_smem(reinterpret_cast<const void*>(k_inverse), smem));
+  k_inverse<<<batch, kSmallThreads, smem, c->stream>>>(n, A, c->scal);
+  c->kernels_launched++;
+  MB_CHECK_CUDA(cudaGetLastError());
+  return MCNLA_B200_OK;
+}
+
+int launch_gaussian(Context* c, uint64_t seed, int64_t count, double* out) {
+  if (count <= 0) return MCNLA_B200_OK;
+  k_gaussian<<<grid_for(c, (count + 1) / 2, 256), 256, 0, c->stream>>>(seed, count, out);
+  c->kernels_launched++;
+  MB_CHECK_CUDA(cudaGetLastError());
+  return MCNLA_B200_OK;
+}
+
+}  // namespace mb

@@ -1,0 +1,262 @@
+// CTA-level FP64 dense routines for the l x l (and 2l x 2l) steps of the iSVD
+// stages: symmetric eigendecomposition (the reference calls LAPACK dsyev /
+// dgesvd there, include/mcnla/core/la/dense/driver/syev.hpp:150-160,
+// gesvd.hpp:159-193), matrix inversion (dgetrf + dgetri,
+// include/mcnla/core/la/dense/driver/getrfi.hpp:117-124) and small products.
+//
+// One thread block owns one small problem.  The eigensolver is the cyclic
+// two-sided Jacobi method with a round-robin (tournament) ordering, so the
+// n/2 rotations of a round touch disjoint row/column pairs and run in
+// parallel (Golub & Van Loan, Matrix Computations, 4th ed., sec. 8.5:
+// Algorithm 8.5.2 for the 2 x 2 rotation, sec. 8.5.5 for the parallel
+// ordering).  The inverse is Gauss-Jordan elimination with partial pivoting,
+// done in place.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace mb {
+namespace small {
+
+// Round-robin pairing of P (even) players over P-1 rounds: pair 0 is
+// (r, P-1); pair k >= 1 is ((r+k) mod (P-1), (r-k) mod (P-1)).  Every pair of
+// distinct players meets exactly once per sweep.
+__device__ __forceinline__ void rr_pair(int P, int r, int k, int& p, int& q) {
+  if (k == 0) { p = r; q = P - 1; }
+  else {
+    p = (r + k) % (P - 1);
+    q = (r - k + (P - 1)) % (P - 1);
+  }
+  if (p > q) { int t = p; p = q; q = t; }
+}
+
+struct JacobiScratch {
+  double* c;    // npairs
+  double* s;    // npairs
+  double* t;    // npairs (tangent, for the exact diagonal update)
+  double* apq;  // npairs
+  double* app;  // npairs
+  double* aqq;  // npairs
+  int* p;       // npairs
+  int* q;       // npairs
+  int* count;   // 1 (rotations applied this round)
+  double* red;  // 32
+};
+
+// Frobenius norm^2 of the n x n matrix a (lda), all threads return it.
+__device__ inline double cta_frob2(const double* a, int lda, int n, double* red) {
+  double s = 0.0;
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    double v = a[(e / n) * lda + (e % n)];
+    s += v * v;
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  double tot = 0.0;
+  const int nw = (blockDim.x + 31) >> 5;
+  for (int w = 0; w < nw; ++w) tot += red[w];
+  __syncthreads();
+  return tot;
+}
+
+// Eigendecomposition of the symmetric n x n matrix a (row stride lda, any
+// memory space; shared memory is fastest).  On return diag(a) holds the
+// eigenvalues (unsorted) and the columns of v (row stride ldv) the
+// eigenvectors.  When init_v is false, v must hold an orthogonal starting
+// basis in which a is expressed (warm start); otherwise v is set to I.
+// Returns the number of sweeps.
+__device__ inline int cta_jacobi_eig(double* a, int lda, double* v, int ldv, int n, bool init_v,
+                                     const JacobiScratch& js, int max_sweeps) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  if (init_v) {
+    for (int e = tid; e < n * n; e += nt) v[(e / n) * ldv + (e % n)] = ((e / n) == (e % n)) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  if (n <= 1) return 0;
+  const int P = (n + 1) & ~1;
+  const int npairs = P / 2;
+  const double fro2 = cta_frob2(a, lda, n, js.red);
+  // Off-diagonal entries below this are treated as zero (absolute floor for
+  // exactly singular inputs); the relative test below drives convergence.
+  const double abs_floor = 1e-40 + 1e-34 * fro2;
+  int sweep = 0;
+  for (; sweep < max_sweeps; ++sweep) {
+    int rotated = 0;
+    for (int r = 0; r < P - 1; ++r) {
+      if (tid == 0) *js.count = 0;
+      __syncthreads();
+      // 1. angles, one thread per pair
+      for (int k = tid; k < npairs; k += nt) {
+        int p, q;
+        rr_pair(P, r, k, p, q);
+        double c = 1.0, s = 0.0, t = 0.0, apq = 0.0, app = 0.0, aqq = 0.0;
+        if (q < n) {
+          apq = a[p * lda + q];
+          app = a[p * lda + p];
+          aqq = a[q * lda + q];
+          const double thr = 2.220446049250313e-16 * sqrt(fabs(app) * fabs(aqq));
+          if (fabs(apq) > thr && apq * apq > abs_floor) {
+            const double theta = (aqq - app) / (2.0 * apq);
+            const double at = fabs(theta);
+            t = (at > 1e150) ? 0.5 / theta : ((theta >= 0.0 ? 1.0 : -1.0) / (at + sqrt(1.0 + theta * theta)));
+            c = 1.0 / sqrt(1.0 + t * t);
+            s = t * c;
+            atomicAdd(js.count, 1);
+          } else {
+            apq = 0.0;
+          }
+        }
+        js.c[k] = c; js.s[k] = s; js.t[k] = t; js.apq[k] = apq; js.app[k] = app; js.aqq[k] = aqq;
+        js.p[k] = p; js.q[k] = q;
+      }
+      __syncthreads();
+      const int cnt = *js.count;
+      if (cnt == 0) { __syncthreads(); continue; }
+      rotated += cnt;
+      // 2. rows: a <- J' a
+      for (int e = tid; e < npairs * n; e += nt) {
+        const int k = e / n, j = e % n;
+        if (js.s[k] == 0.0) continue;
+        const int p = js.p[k], q = js.q[k];
+        const double c = js.c[k], s = js.s[k];
+        const double x = a[p * lda + j], y = a[q * lda + j];
+        a[p * lda + j] = c * x - s * y;
+        a[q * lda + j] = s * x + c * y;
+      }
+      __syncthreads();
+      // 3. columns: a <- a J and v <- v J.  The 2x2 block of each pair is
+      //    written exactly: J' B J = diag(app - t apq, aqq + t apq).
+      for (int e = tid; e < npairs * n; e += nt) {
+        const int k = e / n, i = e % n;
+        if (js.s[k] == 0.0) continue;
+        const int p = js.p[k], q = js.q[k];
+        const double c = js.c[k], s = js.s[k];
+        if (i == p) {
+          a[p * lda + p] = js.app[k] - js.t[k] * js.apq[k];
+          a[p * lda + q] = 0.0;
+        } else if (i == q) {
+          a[q * lda + q] = js.aqq[k] + js.t[k] * js.apq[k];
+          a[q * lda + p] = 0.0;
+        } else {
+          const double x = a[i * lda + p], y = a[i * lda + q];
+          a[i * lda + p] = c * x - s * y;
+          a[i * lda + q] = s * x + c * y;
+        }
+        const double vx = v[i * ldv + p], vy = v[i * ldv + q];
+        v[i * ldv + p] = c * vx - s * vy;
+        v[i * ldv + q] = s * vx + c * vy;
+      }
+      __syncthreads();
+    }
+    if (rotated == 0) break;
+  }
+  return sweep;
+}
+
+// In-place inverse of the n x n matrix a (row stride lda) by Gauss-Jordan
+// elimination with partial pivoting.  piv (n ints) and col (n doubles) are
+// scratch.  Returns 0, or k+1 when the k-th pivot is exactly zero (the matrix
+// is singular; a is then left partially reduced, as LAPACK's getri would
+// refuse).  All threads return the same value.
+__device__ inline int cta_gj_inverse(double* a, int lda, int n, int* piv, double* col, double* red_v, int* red_i,
+                                     int* flag) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  if (tid == 0) *flag = 0;
+  __syncthreads();
+  for (int k = 0; k < n; ++k) {
+    // pivot: argmax_{i >= k} |a[i][k]| (first maximum wins, as idamax)
+    if (tid < 32) {
+      double best = -1.0;
+      int bi = k;
+      for (int i = k + tid; i < n; i += 32) {
+        const double v = fabs(a[i * lda + k]);
+        if (v > best) { best = v; bi = i; }
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+      }
+      if (tid == 0) { red_v[0] = best; red_i[0] = bi; piv[k] = bi; }
+    }
+    __syncthreads();
+    const int pr = red_i[0];
+    if (pr != k) {
+      for (int j = tid; j < n; j += nt) {
+        const double t = a[k * lda + j];
+        a[k * lda + j] = a[pr * lda + j];
+        a[pr * lda + j] = t;
+      }
+    }
+    __syncthreads();
+    const double pivot = a[k * lda + k];
+    if (pivot == 0.0) {
+      if (tid == 0) *flag = k + 1;
+      __syncthreads();
+      return k + 1;
+    }
+    const double inv = 1.0 / pivot;
+    // column k (original values) for the elimination
+    for (int i = tid; i < n; i += nt) col[i] = a[i * lda + k];
+    __syncthreads();
+    for (int j = tid; j < n; j += nt) a[k * lda + j] = (j == k) ? inv : a[k * lda + j] * inv;
+    __syncthreads();
+    for (int e = tid; e < n * n; e += nt) {
+      const int i = e / n, j = e % n;
+      if (i == k) continue;
+      const double f = col[i];
+      if (j == k) a[i * lda + k] = -f * inv;
+      else a[i * lda + j] -= f * a[k * lda + j];
+    }
+    __syncthreads();
+  }
+  // undo the row interchanges as column interchanges, last first
+  for (int k = n - 1; k >= 0; --k) {
+    const int pr = piv[k];
+    if (pr != k) {
+      for (int i = tid; i < n; i += nt) {
+        const double t = a[i * lda + k];
+        a[i * lda + k] = a[i * lda + pr];
+        a[i * lda + pr] = t;
+      }
+    }
+    __syncthreads();
+  }
+  return 0;
+}
+
+// C := alpha * op(A) * op(B) + beta * C for small matrices (any memory space),
+// all threads of the block cooperating; op(X) = X or X' (tA / tB).  C must not
+// alias A or B.  Ends with a block barrier.
+__device__ inline void cta_mm(int M, int N, int K, double alpha, const double* A, int lda, bool tA, const double* B,
+                              int ldb, bool tB, double beta, double* C, int ldc) {
+  for (int e = threadIdx.x; e < M * N; e += blockDim.x) {
+    const int i = e / N, j = e % N;
+    double s = 0.0;
+    for (int k = 0; k < K; ++k) {
+      const double x = tA ? A[k * lda + i] : A[i * lda + k];
+      const double y = tB ? B[j * ldb + k] : B[k * ldb + j];
+      s = fma(x, y, s);
+    }
+    C[i * ldc + j] = (beta == 0.0) ? alpha * s : alpha * s + beta * C[i * ldc + j];
+  }
+  __syncthreads();
+}
+
+// Block-wide sum of one value per thread; every thread gets the total.
+__device__ inline double cta_sum(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double tot = 0.0;
+  const int nw = (blockDim.x + 31) >> 5;
+  for (int w = 0; w < nw; ++w) tot += red[w];
+  __syncthreads();
+  return tot;
+}
+
+}  // namespace small
+}  // namespace mb

@@ -1,0 +1,848 @@
+// The iSVD stages on one B200: sketch, Gramian orthogonalizer, the five
+// integrators and the two former families, plus the whole-solve pipeline and
+// the C ABI entry points (declared in include/mcnla_b200.h).
+//
+// Each stage follows its reference runImpl step for step (citations inline);
+// the products run on the FP64 DMMA GEMM, the l x l work on the one-CTA
+// solvers, and the reference's MPI collectives disappear because every
+// sketch and every row lives on the one device.  Operands the reference keeps
+// in separate matrices are packed side by side where that turns two GEMMs
+// into one (e.g. [Qc | Gc] * [Fc; inv(C)] for Q+ := Qc Fc + Gc inv(C)).
+#include "common.cuh"
+#include "dgemm.cuh"
+#include "kernels.cuh"
+#include <algorithm>
+#include <array>
+#include <cmath>
+
+namespace mb {
+namespace {
+
+// Wen-Yin line-search constants (include/mcnla/isvd/integrator/row_block_wen_yin_integrator.hh:76-94).
+constexpr double kTau0 = 1.0, kTauMax = 1e14, kTauMin = 1e-14, kBeta = 0.5, kSigma = 1e-4, kEta = 0.85;
+constexpr int kTauMaxIter = 20;
+
+struct Dims {
+  int64_t m, n;
+  int k, p, l, N;
+  int64_t L;
+};
+
+int get_dims(const mcnla_b200_params* p, Dims& d) {
+  if (!p) return MCNLA_B200_ERR_ARG;
+  if (p->nrow <= 0 || p->ncol <= 0 || p->rank <= 0 || p->over_rank < 0 || p->num_sketch <= 0)
+    return MCNLA_B200_ERR_SHAPE;
+  const int64_t l = p->rank + p->over_rank;
+  if (l > MCNLA_B200_MAX_DIM_SKETCH) return MCNLA_B200_ERR_UNSUPPORTED;
+  if (p->num_sketch > (int64_t(1) << 24)) return MCNLA_B200_ERR_SHAPE;
+  d.m = p->nrow; d.n = p->ncol;
+  d.k = int(p->rank); d.p = int(p->over_rank); d.l = int(l); d.N = int(p->num_sketch);
+  d.L = l * p->num_sketch;
+  return MCNLA_B200_OK;
+}
+
+// Workspace planner: accumulates the sizes of the buffers a stage will carve.
+struct Plan {
+  size_t bytes = 0;
+  void add(size_t count, size_t elem = sizeof(double)) { bytes += arena_bytes_for(count, elem); }
+};
+
+size_t gemm_ws(const Context* c, std::initializer_list<std::array<int64_t, 4>> shapes) {
+  size_t w = 0;
+  for (auto& s : shapes) w = std::max(w, dgemm_workspace_bytes(c, s[0], s[1], s[2], int(s[3])));
+  return w;
+}
+
+// Every stage carves its buffers after one ctx_reserve(); a carve past the
+// reservation is a planning bug and is reported instead of corrupting memory.
+int check_arena(const Context* c) {
+  return c->arena_top <= c->arena_bytes ? MCNLA_B200_OK : MCNLA_B200_ERR_WORKSPACE;
+}
+
+// Carves the split-K workspace of a stage and registers it with the context.
+double* take_ws(Context* c, size_t bytes) {
+  double* p = ctx_take<double>(c, bytes / 8 + 1);
+  c->gws = p;
+  c->gws_bytes = p ? bytes + 8 : 0;
+  return p;
+}
+
+int copy2d(Context* c, double* dst, int64_t ldd, const double* src, int64_t lds, int64_t rows, int64_t cols) {
+  if (rows <= 0 || cols <= 0) return MCNLA_B200_OK;
+  MB_CHECK_CUDA(cudaMemcpy2DAsync(dst, ldd * sizeof(double), src, lds * sizeof(double), cols * sizeof(double), rows,
+                                  cudaMemcpyDeviceToDevice, c->stream));
+  return MCNLA_B200_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Sketcher
+// ---------------------------------------------------------------------------
+int run_sketch(Context* c, const Dims& d, const double* A, int layout, int64_t lda, double* omega, int exponent,
+               double* Q, bool timed_generation) {
+  if (layout != MCNLA_B200_ROW_MAJOR && layout != MCNLA_B200_COL_MAJOR) return MCNLA_B200_ERR_ARG;
+  if (layout == MCNLA_B200_ROW_MAJOR ? lda < d.n : lda < d.m) return MCNLA_B200_ERR_SHAPE;
+  if (exponent < 0) return MCNLA_B200_ERR_ARG;
+  const CMat Am = layout == MCNLA_B200_ROW_MAJOR ? crow(A, lda) : ccol(A, lda);
+  Plan pl;
+  pl.add(gemm_ws(c, {{d.m, d.L, d.n, 1}, {d.n, d.L, d.m, 1}}) / 8 + 1);
+  MB_CHECK(ctx_reserve(c, pl.bytes));
+  double* ws = take_ws(c, gemm_ws(c, {{d.m, d.L, d.n, 1}, {d.n, d.L, d.m, 1}}));
+  MB_CHECK(check_arena(c));
+  if (!timed_generation) { MB_CHECK(ctx_tic(c)); MB_CHECK(ctx_toc(c)); }   // "random generating" part
+  // Q := A * Omega   (gaussian_projection_sketcher.hpp:96)
+  MB_CHECK(dgemm(c, d.m, d.L, d.n, 1.0, Am, crow(omega, d.L), 0.0, drow(Q, d.L), GemmBatch(), ws));
+  // power iterations (gaussian_projection_sketcher.hpp:97-100)
+  for (int i = 0; i < exponent; ++i) {
+    MB_CHECK(dgemm(c, d.n, d.L, d.m, 1.0, ctr(Am), crow(Q, d.L), 0.0, drow(omega, d.L), GemmBatch(), ws));
+    MB_CHECK(dgemm(c, d.m, d.L, d.n, 1.0, Am, crow(omega, d.L), 0.0, drow(Q, d.L), GemmBatch(), ws));
+  }
+  MB_CHECK(ctx_toc(c));
+  return MCNLA_B200_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Gramian orthogonalizer (gramian_orthogonalizer.hpp:62-104)
+// ---------------------------------------------------------------------------
+int run_orthogonalize(Context* c, const Dims& d, double* Q) {
+  const int l = d.l, N = d.N;
+  const int64_t m = d.m, L = d.L;
+  const size_t ll = size_t(l) * l;
+  const size_t wsb = gemm_ws(c, {{l, l, m, N}, {m, l, l, N}});
+  Plan pl;
+  pl.add(ll * N); pl.add(size_t(l) * N); pl.add(ll * N); pl.add(ll * N); pl.add(size_t(m) * L);
+  pl.add(wsb / 8 + 1); pl.add(ll * N);
+  MB_CHECK(ctx_reserve(c, pl.bytes));
+  double* W = ctx_take<double>(c, ll * N);
+  double* S = ctx_take<double>(c, size_t(l) * N);
+  double* V = ctx_take<double>(c, ll * N);
+  double* T = ctx_take<double>(c, ll * N);
+  double* tmp = ctx_take<double>(c, size_t(m) * L);
+  double* ws = take_ws(c, wsb);
+  MB_CHECK(check_arena(c));
+  MB_CHECK(ctx_tic(c));
+  // W_i := Q_i' Q_i   (:84-86)
+  MB_CHECK(dgemm(c, l, l, m, 1.0, cm(Q, 1, L), cm(Q, L, 1), 0.0, drow(W, l), GemmBatch{N, l, l, int64_t(ll)}, ws));
+  // eig(W_i) = V_i S_i V_i', descending (gesvd<'N','O'> of an SPD matrix, :89-91)
+  MB_CHECK(launch_syev(c, l, N, W, l, int64_t(ll), S, V, 1));
+  // T_i := V_i diag(S_i)^(-1/2)   (:94-99)
+  MB_CHECK(launch_scale_cols_rsqrt(c, l, N, V, S, T));
+  // Q_i := tmp_i T_i   (:97-101, the reference also copies Q to a temporary first)
+  MB_CHECK_CUDA(cudaMemcpyAsync(tmp, Q, size_t(m) * L * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  MB_CHECK(dgemm(c, m, l, l, 1.0, crow(tmp, L), crow(T, l), 0.0, drow(Q, L), GemmBatch{N, l, int64_t(ll), l}, ws));
+  MB_CHECK(ctx_toc(c));
+  return MCNLA_B200_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Integrators
+// ---------------------------------------------------------------------------
+bool kn_converged(double norm, double tol) { return !(norm >= tol); }
+
+// KolmogorovNagumoIntegrator (kolmogorov_nagumo_integrator.hpp:76-185)
+int run_kn(Context* c, const Dims& d, const double* Qs, int maxit, double tol, double* Qbar, int* iters) {
+  const int l = d.l;
+  const int64_t m = d.m, L = d.L;
+  const double inv_n = 1.0 / d.N;
+  const size_t wsb = gemm_ws(c, {{L, l, m, 1}, {l, l, L, 1}, {m, l, L, 1}, {m, l, l, 1}, {l, l, m, 1}, {m, l, 2 * l, 1}});
+  Plan pl;
+  pl.add(size_t(m) * 2 * l); pl.add(size_t(m) * 2 * l); pl.add(size_t(L) * l); pl.add(size_t(l) * l);
+  pl.add(size_t(l) * l); pl.add(size_t(2) * l * l); pl.add(size_t(l) * l); pl.add(wsb / 8 + 1);
+  MB_CHECK(ctx_reserve(c, pl.bytes));
+  double* QX[2] = {ctx_take<double>(c, size_t(m) * 2 * l), ctx_take<double>(c, size_t(m) * 2 * l)};
+  double* B = ctx_take<double>(c, size_t(L) * l);
+  double* D = ctx_take<double>(c, size_t(l) * l);
+  double* Z = ctx_take<double>(c, size_t(l) * l);
+  double* CC = ctx_take<double>(c, size_t(2) * l * l);
+  double* vwork = ctx_take<double>(c, size_t(l) * l);
+  double* ws = take_ws(c, wsb);
+  MB_CHECK(check_arena(c));
+  const int64_t lq = 2 * l;
+  MB_CHECK(ctx_tic(c));
+  // Qc := Q0   (:105)
+  MB_CHECK(copy2d(c, QX[0], lq, Qs, L, m, l));
+  MB_CHECK(ctx_toc(c));
+  int cur = 0, it = 0;
+  bool converged = false;
+  for (; it < maxit && !converged;) {
+    double* Qc = QX[cur];
+    double* X = QX[cur] + l;
+    // B := Qs' Qc   (:117)
+    MB_CHECK(dgemm(c, L, l, m, 1.0, cm(Qs, 1, L), crow(Qc, lq), 0.0, drow(B, l), GemmBatch(), ws));
+    // D := B' B   (:123)
+    MB_CHECK(dgemm(c, l, l, L, 1.0, cm(B, 1, l), crow(B, l), 0.0, drow(D, l), GemmBatch(), ws));
+    // X := Qs B / N;  X -= Qc D / N   (:126-129)
+    MB_CHECK(dgemm(c, m, l, L, inv_n, crow(Qs, L), crow(B, l), 0.0, drow(X, lq), GemmBatch(), ws));
+    MB_CHECK(dgemm(c, m, l, l, -inv_n, crow(Qc, lq), crow(D, l), 1.0, drow(X, lq), GemmBatch(), ws));
+    // Z := X' X   (:143)
+    MB_CHECK(dgemm(c, l, l, m, 1.0, cm(X, 1, lq), crow(X, lq), 0.0, drow(Z, l), GemmBatch(), ws));
+    // eig(Z); C, inv(C)   (:146-164)
+    MB_CHECK(launch_kn_step(c, l, Z, nullptr, inv_n, CC, nullptr, nullptr, nullptr, vwork));
+    // Qc := Qc C + X inv(C) = [Qc X] [C; inv(C)]   (:170-171)
+    MB_CHECK(dgemm(c, m, l, 2 * l, 1.0, crow(QX[cur], lq), crow(CC, l), 0.0, drow(QX[1 - cur], lq), GemmBatch(), ws));
+    cur = 1 - cur;
+    ++it;
+    MB_CHECK(ctx_sync_scalars(c));
+    converged = kn_converged(c->scal_host->norm, tol);   // (:174-181)
+  }
+  MB_CHECK(copy2d(c, Qbar, l, QX[cur], lq, m, l));
+  MB_CHECK(ctx_toc(c));
+  *iters = it;
+  return MCNLA_B200_OK;
+}
+
+// RowBlockKolmogorovNagumoIntegrator (row_block_kolmogorov_nagumo_integrator.hpp:79-208)
+int run_rb_kn(Context* c, const Dims& d, const double* Qs, int maxit, double tol, double* Qbar, int* iters) {
+  const int l = d.l;
+  const int64_t m = d.m, L = d.L;
+  const double inv_n = 1.0 / d.N;
+  const size_t wsb = gemm_ws(c, {{L, l, m, 1}, {m, l, L, 1}, {l, 2 * l, L, 1}, {m, l, 2 * l, 1}, {L, l, 2 * l, 1}});
+  Plan pl;
+  for (int i = 0; i < 2; ++i) { pl.add(size_t(m) * 2 * l); pl.add(size_t(L) * 2 * l); }
+  pl.add(size_t(2) * l * l); pl.add(size_t(2) * l * l); pl.add(size_t(l) * l); pl.add(wsb / 8 + 1);
+  MB_CHECK(ctx_reserve(c, pl.bytes));
+  double* QG[2] = {ctx_take<double>(c, size_t(m) * 2 * l), ctx_take<double>(c, size_t(m) * 2 * l)};
+  double* BB[2] = {ctx_take<double>(c, size_t(L) * 2 * l), ctx_take<double>(c, size_t(L) * 2 * l)};
+  double* DD = ctx_take<double>(c, size_t(2) * l * l);
+  double* FC = ctx_take<double>(c, size_t(2) * l * l);
+  double* vwork = ctx_take<double>(c, size_t(l) * l);
+  double* ws = take_ws(c, wsb);
+  MB_CHECK(check_arena(c));
+  const int64_t l2 = 2 * l;
+  MB_CHECK(ctx_tic(c));
+  // Qc := Q0; Bc := Qs' Qc   (:110-113)
+  MB_CHECK(copy2d(c, QG[0], l2, Qs, L, m, l));
+  MB_CHECK(dgemm(c, L, l, m, 1.0, cm(Qs, 1, L), crow(QG[0], l2), 0.0, drow(BB[0], l2), GemmBatch(), ws));
+  MB_CHECK(ctx_toc(c));
+  int cur = 0, it = 0;
+  bool converged = false;
+  for (; it < maxit && !converged;) {
+    // Gc := 1/N Qs Bc   (:138)
+    MB_CHECK(dgemm(c, m, l, L, inv_n, crow(Qs, L), crow(BB[cur], l2), 0.0, drow(QG[cur] + l, l2), GemmBatch(), ws));
+    // Bgc := Qs' Gc   (:141)
+    MB_CHECK(dgemm(c, L, l, m, 1.0, cm(Qs, 1, L), crow(QG[cur] + l, l2), 0.0, drow(BB[cur] + l, l2), GemmBatch(), ws));
+    // [Dc | Dgc] := 1/N Bc' [Bc | Bgc]   (:147-150)
+    MB_CHECK(dgemm(c, l, l2, L, inv_n, cm(BB[cur], 1, l2), crow(BB[cur], l2), 0.0, drow(DD, l2), GemmBatch(), ws));
+    // Z := Dgc - Dc^2; eig; C, inv(C); Fc := C - Dc inv(C)   (:156-186)
+    MB_CHECK(launch_kn_step(c, l, nullptr, DD, inv_n, FC, nullptr, nullptr, nullptr, vwork));
+    // Q+ := [Qc Gc] [Fc; inv(C)];  B+ := [Bc Bgc] [Fc; inv(C)]   (:189-194)
+    MB_CHECK(dgemm(c, m, l, l2, 1.0, crow(QG[cur], l2), crow(FC, l), 0.0, drow(QG[1 - cur], l2), GemmBatch(), ws));
+    MB_CHECK(dgemm(c, L, l, l2, 1.0, crow(BB[cur], l2), crow(FC, l), 0.0, drow(BB[1 - cur], l2), GemmBatch(), ws));
+    cur = 1 - cur;
+    ++it;
+    MB_CHECK(ctx_sync_scalars(c));
+    converged = kn_converged(c->scal_host->norm, tol);   // (:198-201)
+  }
+  MB_CHECK(copy2d(c, Qbar, l, QG[cur], l2, m, l));   // (:205)
+  MB_CHECK(ctx_toc(c));
+  *iters = it;
+  return MCNLA_B200_OK;
+}
+
+// Bs := Qs' Qs with the reference's triangle convention (see launch_gramian_prepare).
+int gramian_bs(Context* c, const Dims& d, const double* Qs, double* Bs, double* Bc, int64_t ldbc, double* ws) {
+  MB_CHECK(dgemm(c, d.L, d.L, d.m, 1.0, cm(Qs, 1, d.L), crow(Qs, d.L), 0.0, drow(Bs, d.L), GemmBatch(), ws));
+  MB_CHECK(launch_gramian_prepare(c, d.L, d.l, Bs, Bc, ldbc));
+  return MCNLA_B200_OK;
+}
+
+// Qbar := Q0 F~ + Qs E~ = Qs (E~ + [F~; 0])
+int gramian_form_qbar(Context* c, const Dims& d, const double* Qs, const double* E, int64_t lde, const double* F,
+                      double* Ebar, double* Qbar, double* ws) {
+  const int l = d.l;
+  MB_CHECK(copy2d(c, Ebar, l, E, lde, d.L, l));
+  MB_CHECK(launch_axpby(c, l, l, 1.0, F, l, 1.0, Ebar, l));
+  MB_CHECK(dgemm(c, d.m, l, d.L, 1.0, crow(Qs, d.L), crow(Ebar, l), 0.0, drow(Qbar, l), GemmBatch(), ws));
+  return MCNLA_B200_OK;
+}
+
+// RowBlockGramianKolmogorovNagumoIntegrator
+// (row_block_gramian_kolmogorov_nagumo_integrator.hpp:79-229)
+int run_rb_gramian_kn(Context* c, const Dims& d, const double* Qs, int maxit, double tol, double* Qbar, int* iters) {
+  const int l = d.l;
+  const int64_t m = d.m, L = d.L;
+  const double inv_n = 1.0 / d.N;
+  const int64_t l3 = 3 * l, l2 = 2 * l;
+  const size_t wsb = gemm_ws(c, {{L, L, m, 1}, {L, l, L, 1}, {l, l2, L, 1}, {L, l, l2, 1}, {m, l, L, 1}});
+  Plan pl;
+  pl.add(size_t(L) * L); pl.add(size_t(L) * l3); pl.add(size_t(L) * l3); pl.add(size_t(l2) * l);
+  pl.add(size_t(l2) * l); pl.add(size_t(l2) * l); pl.add(size_t(l) * l); pl.add(size_t(l) * l);
+  pl.add(size_t(L) * l); pl.add(size_t(l) * l); pl.add(wsb / 8 + 1);
+  MB_CHECK(ctx_reserve(c, pl.bytes));
+  double* Bs = ctx_take<double>(c, size_t(L) * L);
+  double* EB[2] = {ctx_take<double>(c, size_t(L) * l3), ctx_take<double>(c, size_t(L) * l3)};
+  double* DD = ctx_take<double>(c, size_t(l2) * l);
+  double* FC = ctx_take<double>(c, size_t(l2) * l);
+  double* FCN = ctx_take<double>(c, size_t(l2) * l);
+  double* FF[2] = {ctx_take<double>(c, size_t(l) * l), ctx_take<double>(c, size_t(l) * l)};
+  double* Ebar = ctx_take<double>(c, size_t(L) * l);
+  double* vwork = ctx_take<double>(c, size_t(l) * l);
+  double* ws = take_ws(c, wsb);
+  MB_CHECK(check_arena(c));
+  MB_CHECK(ctx_tic(c));
+  // Bs := Qs' Qs; Bc := Bs(:, 0:l); F~ := I; E~ := 0   (:112-133)
+  MB_CHECK(gramian_bs(c, d, Qs, Bs, EB[0] + l, l3, ws));
+  MB_CHECK(launch_fill(c, L, l, 0.0, EB[0], l3));
+  MB_CHECK(launch_set_identity(c, l, FF[0], l));
+  MB_CHECK(ctx_toc(c));
+  int cur = 0, it = 0;
+  bool converged = false;
+  for (; it < maxit && !converged;) {
+    double* Ec = EB[cur];
+    double* Bc = EB[cur] + l;
+    double* Bgc = EB[cur] + l2;
+    // Bgc := 1/N Bs Bc   (:152)
+    MB_CHECK(dgemm(c, L, l, L, inv_n, crow(Bs, L), crow(Bc, l3), 0.0, drow(Bgc, l3), GemmBatch(), ws));
+    // [Dc | Dgc] := 1/N Bc' [Bc | Bgc]   (:155-158)
+    MB_CHECK(dgemm(c, l, l2, L, inv_n, cm(Bc, 1, l3), crow(Bc, l3), 0.0, drow(DD, l2), GemmBatch(), ws));
+    // Z, eig, C, inv(C), Fc; F~+ := F~c Fc   (:164-197)
+    MB_CHECK(launch_kn_step(c, l, nullptr, DD, inv_n, FC, FCN, FF[cur], FF[1 - cur], vwork));
+    // E~+ := E~c Fc + 1/N Bc inv(C) = [E~c Bc] [Fc; inv(C)/N]   (:194, :200)
+    MB_CHECK(dgemm(c, L, l, l2, 1.0, crow(Ec, l3), crow(FCN, l), 0.0, drow(EB[1 - cur], l3), GemmBatch(), ws));
+    // B+ := [Bc Bgc] [Fc; inv(C)]   (:203-204)
+    MB_CHECK(dgemm(c, L, l, l2, 1.0, crow(Bc, l3), crow(FC, l), 0.0, drow(EB[1 - cur] + l, l3), GemmBatch(), ws));
+    cur = 1 - cur;
+    ++it;
+    MB_CHECK(ctx_sync_scalars(c));
+    converged = kn_converged(c->scal_host->norm, tol);   // (:207-214)
+  }
+  MB_CHECK(ctx_toc(c));
+  // Qbar := Q0 F~ + Qs E~   (:225-226)
+  MB_CHECK(gramian_form_qbar(c, d, Qs, EB[cur], l3, FF[cur], Ebar, Qbar, ws));
+  MB_CHECK(ctx_toc(c));
+  *iters = it;
+  return MCNLA_B200_OK;
+}
+
+// Wen-Yin line search shared by both Wen-Yin integrators
+// (row_block_wen_yin_integrator.hpp:171-214).  bbc = [Bc | Bgc] (row stride
+// ldb); B+ is written to bp (row stride ldp).  Returns phit through *phit.
+int wy_line_search(Context* c, const Dims& d, const double* dd, const double* bbc, int64_t ldb, double* bp,
+                   int64_t ldp, double taug, double phi, double mu, double* F, double* FN, double* partials,
+                   double* ws, double* phit) {
+  const int l = d.l;
+  const double inv_n = 1.0 / d.N;
+  double tau = taug;
+  double pt = phi;
+  for (int trial = 0; trial < kTauMaxIter; ++trial, tau *= kBeta) {
+    MB_CHECK(launch_wy_trial(c, l, dd, tau, inv_n, F, FN));
+    MB_CHECK(dgemm(c, d.L, l, 2 * l, 1.0, crow(bbc, ldb), crow(F, l), 0.0, drow(bp, ldp), GemmBatch(), ws));
+    MB_CHECK(launch_sumsq(c, bp, d.L, l, ldp, 0.5 * inv_n, partials, &c->scal->phit));
+    MB_CHECK(ctx_sync_scalars(c));
+    if (c->scal_host->status) return c->scal_host->status;
+    pt = c->scal_host->phit;
+    if (pt >= phi + tau * kSigma * mu) break;
+  }
+  *phit = pt;
+  return MCNLA_B200_OK;
+}
+
+// RowBlockWenYinIntegrator (row_block_wen_yin_integrator.hpp:79-281)
+int run_rb_wy(Context* c, const Dims& d, const double* Qs, int maxit, double tol, double* Qbar, int* iters) {
+  const int l = d.l;
+  const int64_t m = d.m, L = d.L, l2 = 2 * l;
+  const double inv_n = 1.0 / d.N;
+  if (l > MCNLA_B200_MAX_DIM_SKETCH_WENYIN) return MCNLA_B200_ERR_UNSUPPORTED;
+  const size_t wsb = gemm_ws(c, {{L, l, m, 1}, {m, l, L, 1}, {l, l2, L, 1}, {m, l, l, 1}, {L, l, l2, 1}, {m, l, l2, 1}});
+  const int np = reduce_partials(c) * 3;
+  Plan pl;
+  for (int i = 0; i < 2; ++i) { pl.add(size_t(m) * l2); pl.add(size_t(m) * l); pl.add(size_t(L) * l2); }
+  pl.add(size_t(l) * l2); pl.add(size_t(l2) * l); pl.add(size_t(np)); pl.add(wsb / 8 + 1);
+  MB_CHECK(ctx_reserve(c, pl.bytes));
+  double* QG[2] = {ctx_take<double>(c, size_t(m) * l2), ctx_take<double>(c, size_t(m) * l2)};
+  double* X[2] = {ctx_take<double>(c, size_t(m) * l), ctx_take<double>(c, size_t(m) * l)};
+  double* BB[2] = {ctx_take<double>(c, size_t(L) * l2), ctx_take<double>(c, size_t(L) * l2)};
+  double* DD = ctx_take<double>(c, size_t(l) * l2);
+  double* F = ctx_take<double>(c, size_t(l2) * l);
+  double* partials = ctx_take<double>(c, size_t(np));
+  double* ws = take_ws(c, wsb);
+  MB_CHECK(check_arena(c));
+  MB_CHECK_CUDA(cudaMemsetAsync(c->scal, 0, sizeof(DevScalars), c->stream));
+  MB_CHECK(ctx_tic(c));
+  // Initializing (:112-143)
+  MB_CHECK(copy2d(c, QG[0], l2, Qs, L, m, l));                                                        // Qc := Q0
+  MB_CHECK(dgemm(c, L, l, m, 1.0, cm(Qs, 1, L), crow(QG[0], l2), 0.0, drow(BB[0], l2), GemmBatch(), ws));  // Bc
+  MB_CHECK(dgemm(c, m, l, L, inv_n, crow(Qs, L), crow(BB[0], l2), 0.0, drow(QG[0] + l, l2), GemmBatch(), ws));  // Gc
+  MB_CHECK(dgemm(c, L, l, m, 1.0, cm(Qs, 1, L), crow(QG[0] + l, l2), 0.0, drow(BB[0] + l, l2), GemmBatch(), ws));  // Bgc
+  MB_CHECK(dgemm(c, l, l2, L, inv_n, cm(BB[0], 1, l2), crow(BB[0], l2), 0.0, drow(DD, l2), GemmBatch(), ws));  // Dc|Dgc
+  // Xc := Gc - Qc Dc
+  MB_CHECK(copy2d(c, X[0], l, QG[0] + l, l2, m, l));
+  MB_CHECK(dgemm(c, m, l, l, -1.0, crow(QG[0], l2), crow(DD, l2), 1.0, drow(X[0], l), GemmBatch(), ws));
+  // phi := 1/2N ||Bc||_F^2; mu := tr(Dgc) - ||Dc||_F^2
+  MB_CHECK(launch_sumsq(c, BB[0], L, l, l2, 0.5 * inv_n, partials, &c->scal->dot[0]));
+  MB_CHECK(launch_wy_mu(c, l, DD, &c->scal->mu));
+  MB_CHECK(ctx_sync_scalars(c));
+  double taug = kTau0, zeta = 1.0, phi = c->scal_host->dot[0], mu = c->scal_host->mu;
+  MB_CHECK(ctx_toc(c));
+  int cur = 0, it = 0, fin = 0;
+  bool is_odd = false;
+  for (; it < maxit;) {
+    const int nx = 1 - cur;
+    is_odd = !is_odd;
+    double phit = phi;
+    // B+ := Bc Fc + Bgc Fgc with the accepted step   (:171-214)
+    MB_CHECK(wy_line_search(c, d, DD, BB[cur], l2, BB[nx], l2, taug, phi, mu, F, nullptr, partials, ws, &phit));
+    phi = (kEta * zeta * phi + phit) / (kEta * zeta + 1);   // (:217)
+    zeta = kEta * zeta + 1;                                  // (:218)
+    // Q+ := [Qc Gc] [Fc; Fgc]   (:221-222)
+    MB_CHECK(dgemm(c, m, l, l2, 1.0, crow(QG[cur], l2), crow(F, l), 0.0, drow(QG[nx], l2), GemmBatch(), ws));
+    // G+ := 1/N Qs B+; Bg+ := Qs' G+; [D+ | Dg+] := 1/N B+' [B+ | Bg+]   (:224-236)
+    MB_CHECK(dgemm(c, m, l, L, inv_n, crow(Qs, L), crow(BB[nx], l2), 0.0, drow(QG[nx] + l, l2), GemmBatch(), ws));
+    MB_CHECK(dgemm(c, L, l, m, 1.0, cm(Qs, 1, L), crow(QG[nx] + l, l2), 0.0, drow(BB[nx] + l, l2), GemmBatch(), ws));
+    MB_CHECK(dgemm(c, l, l2, L, inv_n, cm(BB[nx], 1, l2), crow(BB[nx], l2), 0.0, drow(DD, l2), GemmBatch(), ws));
+    // mu := tr(Dg+) - ||D+||_F^2   (:240)
+    MB_CHECK(launch_wy_mu(c, l, DD, &c->scal->mu));
+    MB_CHECK(ctx_sync_scalars(c));
+    mu = c->scal_host->mu;
+    if (mu < tol * tol) {   // (:249-250)
+      ++it;
+      fin = nx;
+      break;
+    }
+    // X+ := G+ - Q+ D+   (:253-254)
+    MB_CHECK(copy2d(c, X[nx], l, QG[nx] + l, l2, m, l));
+    MB_CHECK(dgemm(c, m, l, l, -1.0, crow(QG[nx], l2), crow(DD, l2), 1.0, drow(X[nx], l), GemmBatch(), ws));
+    // Delta1 := Qc - Q+, Delta2 := Xc - X+ and their inner products   (:261-274)
+    MB_CHECK(launch_wy_delta_dots(c, QG[cur], QG[nx], l2, X[cur], X[nx], l, m, l, partials, &c->scal->dot[0]));
+    MB_CHECK(ctx_sync_scalars(c));
+    const double d11 = c->scal_host->dot[0], d12 = c->scal_host->dot[1], d22 = c->scal_host->dot[2];
+    const double t1 = is_odd ? d11 : d12, t2 = is_odd ? d12 : d22;
+    taug = std::fabs(t1 / t2);   // (:278-280)
+    if (taug < kTauMin) taug = kTauMin;
+    if (taug > kTauMax) taug = kTauMax;
+    cur = nx;
+    fin = cur;
+    ++it;
+  }
+  MB_CHECK(copy2d(c, Qbar, l, QG[fin], l2, m, l));
+  MB_CHECK(ctx_toc(c));
+  *iters = it;
+  return MCNLA_B200_OK;
+}
+
+// RowBlockGramianWenYinIntegrator (row_block_gramian_wen_yin_integrator.hpp:86-331)
+int run_rb_gramian_wy(Context* c, const Dims& d, const double* Qs, int maxit, double tol, double* Qbar, int* iters) {
+  const int l = d.l;
+  const int64_t m = d.m, L = d.L, l2 = 2 * l, l3 = 3 * l;
+  const double inv_n = 1.0 / d.N;
+  if (l > MCNLA_B200_MAX_DIM_SKETCH_WENYIN) return MCNLA_B200_ERR_UNSUPPORTED;
+  const size_t wsb = gemm_ws(c, {{L, L, m, 1}, {L, l, L, 1}, {l, l2, L, 1}, {L, l, l2, 1}, {L, l, l, 1}, {l, l, l, 1},
+                                 {m, l, L, 1}});
+  const int np = reduce_partials(c) * 3;
+  Plan pl;
+  pl.add(size_t(L) * L);
+  for (int i = 0; i < 2; ++i) { pl.add(size_t(L) * l3); pl.add(size_t(l) * l2); pl.add(size_t(l) * l); }
+  pl.add(size_t(l2) * l); pl.add(size_t(l2) * l); pl.add(size_t(L) * l2); pl.add(size_t(L) * l);
+  pl.add(size_t(l) * l); pl.add(size_t(l) * l); pl.add(size_t(l) * l2); pl.add(size_t(L) * l);
+  pl.add(size_t(np)); pl.add(wsb / 8 + 1);
+  MB_CHECK(ctx_reserve(c, pl.bytes));
+  double* Bs = ctx_take<double>(c, size_t(L) * L);
+  double* EB[2] = {ctx_take<double>(c, size_t(L) * l3), ctx_take<double>(c, size_t(L) * l3)};
+  double* DD[2] = {ctx_take<double>(c, size_t(l) * l2), ctx_take<double>(c, size_t(l) * l2)};
+  double* FF[2] = {ctx_take<double>(c, size_t(l) * l), ctx_take<double>(c, size_t(l) * l)};
+  double* F = ctx_take<double>(c, size_t(l2) * l);
+  double* FN = ctx_take<double>(c, size_t(l2) * l);
+  double* U = ctx_take<double>(c, size_t(L) * l2);     // [U1 | U2]
+  double* BsU = ctx_take<double>(c, size_t(L) * l);
+  double* PHI1 = ctx_take<double>(c, size_t(l) * l);
+  double* PHI2 = ctx_take<double>(c, size_t(l) * l);
+  double* BCU = ctx_take<double>(c, size_t(l) * l2);   // [Bc'U1 | Bc'U2]
+  double* Ebar = ctx_take<double>(c, size_t(L) * l);
+  double* partials = ctx_take<double>(c, size_t(np));
+  double* ws = take_ws(c, wsb);
+  MB_CHECK(check_arena(c));
+  MB_CHECK_CUDA(cudaMemsetAsync(c->scal, 0, sizeof(DevScalars), c->stream));
+  MB_CHECK(ctx_tic(c));
+  // Initializing (:121-155)
+  MB_CHECK(gramian_bs(c, d, Qs, Bs, EB[0] + l, l3, ws));
+  MB_CHECK(dgemm(c, L, l, L, inv_n, crow(Bs, L), crow(EB[0] + l, l3), 0.0, drow(EB[0] + l2, l3), GemmBatch(), ws));
+  MB_CHECK(dgemm(c, l, l2, L, inv_n, cm(EB[0] + l, 1, l3), crow(EB[0] + l, l3), 0.0, drow(DD[0], l2), GemmBatch(), ws));
+  MB_CHECK(launch_set_identity(c, l, FF[0], l));
+  MB_CHECK(launch_fill(c, L, l, 0.0, EB[0], l3));
+  MB_CHECK(launch_sumsq(c, EB[0] + l, L, l, l3, 0.5 * inv_n, partials, &c->scal->dot[0]));
+  MB_CHECK(launch_wy_mu(c, l, DD[0], &c->scal->mu));
+  MB_CHECK(ctx_sync_scalars(c));
+  double taug = kTau0, zeta = 1.0, phi = c->scal_host->dot[0], mu = c->scal_host->mu;
+  MB_CHECK(ctx_toc(c));
+  int cur = 0, it = 0;
+  bool is_odd = false;
+  for (; it < maxit;) {
+    const int nx = 1 - cur;
+    double* Ec = EB[cur];
+    double* Bc = EB[cur] + l;
+    double* Bp = EB[nx] + l;
+    is_odd = !is_odd;
+    double phit = phi;
+    MB_CHECK(wy_line_search(c, d, DD[cur], Bc, l3, Bp, l3, taug, phi, mu, F, FN, partials, ws, &phit));
+    phi = (kEta * zeta * phi + phit) / (kEta * zeta + 1);   // (:225)
+    zeta = kEta * zeta + 1;
+    // U1 := 1/N Bc Fgc   (:229)
+    MB_CHECK(dgemm(c, L, l, l, inv_n, crow(Bc, l3), crow(F + size_t(l) * l, l), 0.0, drow(U, l2), GemmBatch(), ws));
+    // F~+ := F~c Fc   (:232)
+    MB_CHECK(dgemm(c, l, l, l, 1.0, crow(FF[cur], l), crow(F, l), 0.0, drow(FF[nx], l), GemmBatch(), ws));
+    // E~+ := E~c Fc + U1 = [E~c Bc] [Fc; Fgc/N]   (:235-236)
+    MB_CHECK(dgemm(c, L, l, l2, 1.0, crow(Ec, l3), crow(FN, l), 0.0, drow(EB[nx], l3), GemmBatch(), ws));
+    // Bg+ := 1/N Bs B+; [D+ | Dg+] := 1/N B+' [B+ | Bg+]   (:239-245)
+    MB_CHECK(dgemm(c, L, l, L, inv_n, crow(Bs, L), crow(Bp, l3), 0.0, drow(EB[nx] + l2, l3), GemmBatch(), ws));
+    MB_CHECK(dgemm(c, l, l2, L, inv_n, cm(Bp, 1, l3), crow(Bp, l3), 0.0, drow(DD[nx], l2), GemmBatch(), ws));
+    MB_CHECK(launch_wy_mu(c, l, DD[nx], &c->scal->mu));   // (:248)
+    MB_CHECK(ctx_sync_scalars(c));
+    mu = c->scal_host->mu;
+    cur = nx;
+    if (mu < tol * tol) {   // (:252)
+      ++it;
+      break;
+    }
+    // Phi2 := Dc - Fc D+; Phi1 := Fc - I   (:261-266)
+    MB_CHECK(launch_wy_gramian_phis(c, l, F, DD[1 - cur], l2, DD[cur], l2, PHI1, PHI2));
+    // U2 := 1/N (B+ - Bc) - U1 D+   (:269-271)
+    MB_CHECK(launch_axpby(c, L, l, inv_n, Bp, l3, 0.0, U + l, l2));
+    MB_CHECK(launch_axpby(c, L, l, -inv_n, Bc, l3, 1.0, U + l, l2));
+    MB_CHECK(dgemm(c, L, l, l, -1.0, crow(U, l2), crow(DD[cur], l2), 1.0, drow(U + l, l2), GemmBatch(), ws));
+    // [Bc'U1 | Bc'U2]   (:274-277)
+    MB_CHECK(dgemm(c, l, l2, L, 1.0, cm(Bc, 1, l3), crow(U, l2), 0.0, drow(BCU, l2), GemmBatch(), ws));
+    // Bs U1 (odd) or Bs U2 (even)   (:286, :298)
+    const double* Usel = is_odd ? U : U + l;
+    MB_CHECK(dgemm(c, L, l, L, 1.0, crow(Bs, L), crow(Usel, l2), 0.0, drow(BsU, l), GemmBatch(), ws));
+    MB_CHECK(launch_gwy_small_dots(c, l, PHI1, PHI2, BCU, &c->scal->dot[0]));
+    MB_CHECK(launch_dot(c, U, l2, BsU, l, L, l, partials, &c->scal->dot[8]));
+    MB_CHECK(launch_dot(c, U + l, l2, BsU, l, L, l, partials, &c->scal->dot[9]));
+    MB_CHECK(ctx_sync_scalars(c));
+    const double* s = c->scal_host->dot;
+    // s: 0 <P1,P1> 1 <P1,P2> 2 <P2,P2> 3 <P1,BU1> 4 <P1,BU2> 5 <P2,BU1> 6 <P2,BU2> 8 <U1,BsU> 9 <U2,BsU>
+    double t1, t2;
+    if (is_odd) {   // (:284-293)
+      t1 = s[0] + 2 * s[3] + s[8];
+      t2 = s[1] + s[4] + s[5] + s[9];
+    } else {        // (:294-306)
+      t1 = s[1] + s[4] + s[5] + s[8];
+      t2 = s[2] + 2 * s[6] + s[9];
+    }
+    taug = std::fabs(t1 / t2);   // (:309-311)
+    if (taug < kTauMin) taug = kTauMin;
+    if (taug > kTauMax) taug = kTauMax;
+    ++it;
+  }
+  MB_CHECK(ctx_toc(c));
+  // Qbar := Q0 F~ + Qs E~   (:327-328)
+  MB_CHECK(gramian_form_qbar(c, d, Qs, EB[cur], l3, FF[cur], Ebar, Qbar, ws));
+  MB_CHECK(ctx_toc(c));
+  *iters = it;
+  return MCNLA_B200_OK;
+}
+
+int run_integrate(Context* c, const Dims& d, int kind, const double* Qs, int maxit, double tol, double* Qbar,
+                  int* iters) {
+  if (!Qs || !Qbar || !iters) return MCNLA_B200_ERR_ARG;
+  if (maxit < 0 || !(tol >= 0.0)) return MCNLA_B200_ERR_ARG;
+  switch (kind) {
+    case MCNLA_B200_KOLMOGOROV_NAGUMO: return run_kn(c, d, Qs, maxit, tol, Qbar, iters);
+    case MCNLA_B200_ROW_BLOCK_KOLMOGOROV_NAGUMO: return run_rb_kn(c, d, Qs, maxit, tol, Qbar, iters);
+    case MCNLA_B200_ROW_BLOCK_GRAMIAN_KOLMOGOROV_NAGUMO: return run_rb_gramian_kn(c, d, Qs, maxit, tol, Qbar, iters);
+    case MCNLA_B200_ROW_BLOCK_WEN_YIN: return run_rb_wy(c, d, Qs, maxit, tol, Qbar, iters);
+    case MCNLA_B200_ROW_BLOCK_GRAMIAN_WEN_YIN: return run_rb_gramian_wy(c, d, Qs, maxit, tol, Qbar, iters);
+    default: return MCNLA_B200_ERR_ARG;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Formers
+// ---------------------------------------------------------------------------
+// SvdFormer<_, true> (svd_former.hpp:70-116).  gesvd(Vt) is replaced by an
+// accuracy-preserving equivalent: two Gram re-orthonormalizations of the rows
+// of Vt give Y2 (orthonormal rows spanning the same space), M := Vt Y2' is
+// formed by a GEMM, and M's SVD is taken by one-sided Jacobi:
+// Vt = M Y2 = W S (Y2' Z)'.
+int run_form_svd(Context* c, const Dims& d, const CMat& Am, const double* Qbar, double* S, double* U, double* V) {
+  const int l = d.l, k = d.k;
+  const int64_t m = d.m, n = d.n;
+  const size_t ll = size_t(l) * l;
+  const size_t wsb = gemm_ws(c, {{l, n, m, 1}, {l, l, n, 1}, {l, n, l, 1}, {m, k, l, 1}, {n, k, l, 1}});
+  Plan pl;
+  pl.add(size_t(l) * n); pl.add(size_t(l) * n); pl.add(size_t(l) * n);
+  for (int i = 0; i < 6; ++i) pl.add(ll);
+  pl.add(size_t(2) * l); pl.add(wsb / 8 + 1);
+  for (int i = 0; i < 4; ++i) pl.add(ll);   // on-chip solver spill copies (l > 112)
+  MB_CHECK(ctx_reserve(c, pl.bytes));
+  double* Vt = ctx_take<double>(c, size_t(l) * n);
+  double* Y1 = ctx_take<double>(c, size_t(l) * n);
+  double* Y2 = ctx_take<double>(c, size_t(l) * n);
+  double* G = ctx_take<double>(c, ll);
+  double* Ue = ctx_take<double>(c, ll);
+  double* P = ctx_take<double>(c, ll);
+  double* M = ctx_take<double>(c, ll);
+  double* Wm = ctx_take<double>(c, ll);
+  double* Zm = ctx_take<double>(c, ll);
+  double* w = ctx_take<double>(c, size_t(2) * l);
+  double* sig = w + l;
+  double* ws = take_ws(c, wsb);
+  MB_CHECK(check_arena(c));
+  MB_CHECK(ctx_tic(c));
+  // Vt := Q' A   (:99)
+  MB_CHECK(dgemm(c, l, n, m, 1.0, cm(Qbar, 1, l), Am, 0.0, drow(Vt, n), GemmBatch(), ws));
+  MB_CHECK(ctx_toc(c));
+  // svd(Vt)   (:106)
+  const double* Yin = Vt;
+  double* Yout[2] = {Y1, Y2};
+  for (int pass = 0; pass < 2; ++pass) {
+    MB_CHECK(dgemm(c, l, l, n, 1.0, crow(Yin, n), cm(Yin, 1, n), 0.0, drow(G, l), GemmBatch(), ws));
+    MB_CHECK(launch_syev(c, l, 1, G, l, 0, w, Ue, 1));
+    MB_CHECK(launch_rsqrt_rows_t(c, l, Ue, w, P));
+    MB_CHECK(dgemm(c, l, n, l, 1.0, crow(P, l), crow(Yin, n), 0.0, drow(Yout[pass], n), GemmBatch(), ws));
+    Yin = Yout[pass];
+  }
+  MB_CHECK(dgemm(c, l, l, n, 1.0, crow(Vt, n), cm(Y2, 1, n), 0.0, drow(M, l), GemmBatch(), ws));
+  MB_CHECK(launch_svd_small(c, l, M, Wm, sig, Zm));
+  MB_CHECK(ctx_toc(c));
+  // U := Q W(:, 0:k); V := (Y2' Z)(:, 0:k)   (:113, :142)
+  if (U) MB_CHECK(dgemm(c, m, k, l, 1.0, crow(Qbar, l), crow(Wm, l), 0.0, drow(U, k), GemmBatch(), ws));
+  if (V) MB_CHECK(dgemm(c, n, k, l, 1.0, cm(Y2, 1, n), crow(Zm, l), 0.0, drow(V, k), GemmBatch(), ws));
+  if (S) MB_CHECK_CUDA(cudaMemcpyAsync(S, sig, size_t(k) * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  MB_CHECK(ctx_toc(c));
+  return MCNLA_B200_OK;
+}
+
+// GramianFormer / RowBlockGramianFormer / ColBlockGramianFormer (with V)
+// (gramian_former.hpp:72-132; row_block_gramian_former.hpp:78-146;
+//  col_block_gramian_former.hpp:73-131): on one device the three agree.
+int run_form_gramian(Context* c, const Dims& d, const CMat& Am, const double* Qbar, double* S, double* U,
+                     double* V) {
+  const int l = d.l, k = d.k;
+  const int64_t m = d.m, n = d.n;
+  const size_t ll = size_t(l) * l;
+  const size_t wsb = gemm_ws(c, {{n, l, m, 1}, {l, l, n, 1}, {m, k, l, 1}, {n, k, l, 1}});
+  Plan pl;
+  pl.add(size_t(n) * l); pl.add(ll); pl.add(ll); pl.add(ll); pl.add(size_t(2) * l);
+  pl.add(wsb / 8 + 1);
+  for (int i = 0; i < 2; ++i) pl.add(ll);   // on-chip solver spill copy (l > 112)
+  MB_CHECK(ctx_reserve(c, pl.bytes));
+  double* Z = ctx_take<double>(c, size_t(n) * l);
+  double* W = ctx_take<double>(c, ll);
+  double* Ue = ctx_take<double>(c, ll);
+  double* Wk = ctx_take<double>(c, ll);
+  double* w = ctx_take<double>(c, size_t(2) * l);
+  double* s = w + l;
+  double* ws = take_ws(c, wsb);
+  MB_CHECK(check_arena(c));
+  MB_CHECK(ctx_tic(c));
+  // Z := A' Q   (gramian_former.hpp:101)
+  MB_CHECK(dgemm(c, n, l, m, 1.0, ctr(Am), crow(Qbar, l), 0.0, drow(Z, l), GemmBatch(), ws));
+  MB_CHECK(ctx_toc(c));
+  // W := Z' Z; eig(W) = W S W' (descending); S := sqrt(S)   (:108-115)
+  MB_CHECK(dgemm(c, l, l, n, 1.0, cm(Z, 1, l), crow(Z, l), 0.0, drow(W, l), GemmBatch(), ws));
+  MB_CHECK(launch_syev(c, l, 1, W, l, 0, w, Ue, 1));
+  MB_CHECK(launch_sqrt_vec(c, l, w, s));
+  MB_CHECK(ctx_toc(c));
+  // U := Q W(:, 0:k); V := Z W(:, 0:k) diag(1/S)   (:123-128)
+  if (U) MB_CHECK(dgemm(c, m, k, l, 1.0, crow(Qbar, l), crow(Ue, l), 0.0, drow(U, k), GemmBatch(), ws));
+  if (V) {
+    MB_CHECK(launch_scale_cols(c, l, k, Ue, l, s, 0, Wk, k));
+    MB_CHECK(dgemm(c, n, k, l, 1.0, crow(Z, l), crow(Wk, k), 0.0, drow(V, k), GemmBatch(), ws));
+  }
+  if (S) MB_CHECK_CUDA(cudaMemcpyAsync(S, s, size_t(k) * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  MB_CHECK(ctx_toc(c));
+  return MCNLA_B200_OK;
+}
+
+int run_form(Context* c, const Dims& d, int kind, const double* A, int layout, int64_t lda, const double* Qbar,
+             double* S, double* U, double* V) {
+  if (!A || !Qbar) return MCNLA_B200_ERR_ARG;
+  if (layout != MCNLA_B200_ROW_MAJOR && layout != MCNLA_B200_COL_MAJOR) return MCNLA_B200_ERR_ARG;
+  if (layout == MCNLA_B200_ROW_MAJOR ? lda < d.n : lda < d.m) return MCNLA_B200_ERR_SHAPE;
+  if (d.k > d.l) return MCNLA_B200_ERR_SHAPE;
+  const CMat Am = layout == MCNLA_B200_ROW_MAJOR ? crow(A, lda) : ccol(A, lda);
+  switch (kind) {
+    case MCNLA_B200_SVD_FORMER: return run_form_svd(c, d, Am, Qbar, S, U, V);
+    case MCNLA_B200_GRAMIAN_FORMER:
+    case MCNLA_B200_ROW_BLOCK_GRAMIAN_FORMER:
+    case MCNLA_B200_COL_BLOCK_GRAMIAN_FORMER: return run_form_gramian(c, d, Am, Qbar, S, U, V);
+    default: return MCNLA_B200_ERR_ARG;
+  }
+}
+
+int run_isvd(Context* c, const Dims& d, int integrator, int former, const double* A, int layout, int64_t lda,
+             const double* omega_in, uint64_t seed, int maxit, double tol, double* S, double* U, double* V,
+             int* iters, char* pbase) {
+  // pipeline buffers live in the pipeline arena (after whatever the caller put there)
+  auto take = [&](size_t count) {
+    double* p = reinterpret_cast<double*>(pbase);
+    pbase += arena_bytes_for(count, sizeof(double));
+    return p;
+  };
+  double* Q = take(size_t(d.m) * d.L);
+  double* Qbar = take(size_t(d.m) * d.l);
+  double* omega = take(size_t(d.n) * d.L);
+  if (!omega_in) {
+    MB_CHECK(launch_gaussian(c, seed, int64_t(d.n) * d.L, omega));
+  } else {
+    omega = const_cast<double*>(omega_in);   // read only: the sketch runs without power iterations
+  }
+  MB_CHECK(run_sketch(c, d, A, layout, lda, omega, 0, Q, false));
+  MB_CHECK(run_orthogonalize(c, d, Q));
+  MB_CHECK(run_integrate(c, d, integrator, Q, maxit, tol, Qbar, iters));
+  MB_CHECK(run_form(c, d, former, A, layout, lda, Qbar, S, U, V));
+  return MCNLA_B200_OK;
+}
+
+size_t pipeline_bytes(const Dims& d) {
+  return arena_bytes_for(size_t(d.m) * d.L, 8) + arena_bytes_for(size_t(d.m) * d.l, 8) +
+         arena_bytes_for(size_t(d.n) * d.L, 8);
+}
+
+// Workspace bytes each stage will ask for (for mcnla_b200_initialize).
+size_t stage_bytes_upper(Context* c, const Dims& d) {
+  const int64_t m = d.m, n = d.n, L = d.L, l = d.l;
+  size_t b = 0;
+  b = std::max(b, size_t(m) * L * 8 + 5 * size_t(l) * l * d.N * 8 + gemm_ws(c, {{l, l, m, d.N}, {m, l, l, d.N}}));
+  b = std::max(b, size_t(L) * L * 8 + 8 * size_t(L) * 3 * l * 8 + 4 * size_t(m) * 2 * l * 8 +
+                      gemm_ws(c, {{L, L, m, 1}, {L, l, m, 1}, {m, l, L, 1}, {l, 2 * l, L, 1}}));
+  b = std::max(b, 3 * size_t(l) * n * 8 + size_t(n) * l * 8 + gemm_ws(c, {{l, n, m, 1}, {n, l, m, 1}, {l, l, n, 1}}));
+  return b + (64 << 20);
+}
+
+}  // namespace
+}  // namespace mb
+
+using mb::Context;
+using mb::Dims;
+
+extern "C" {
+
+int mcnla_b200_initialize(mcnla_b200_ctx* ctx, const mcnla_b200_params* params, int integrator, int former) {
+  if (!ctx) return MCNLA_B200_ERR_ARG;
+  (void)integrator; (void)former;
+  Dims d;
+  MB_CHECK(mb::get_dims(params, d));
+  MB_CHECK_CUDA(cudaSetDevice(ctx->device));
+  MB_CHECK(mb::ctx_reserve(ctx, mb::stage_bytes_upper(ctx, d)));
+  return MCNLA_B200_OK;
+}
+
+int mcnla_b200_sketch(mcnla_b200_ctx* ctx, const mcnla_b200_params* params, const double* A, int a_layout,
+                      int64_t lda, double* omega, int exponent, double* Q) {
+  if (!ctx || !A || !omega || !Q) return MCNLA_B200_ERR_ARG;
+  Dims d;
+  MB_CHECK(mb::get_dims(params, d));
+  MB_CHECK_CUDA(cudaSetDevice(ctx->device));
+  return mb::run_sketch(ctx, d, A, a_layout, lda, omega, exponent, Q, false);
+}
+
+int mcnla_b200_gaussian(mcnla_b200_ctx* ctx, uint64_t seed, int64_t count, double* out) {
+  if (!ctx || (!out && count > 0) || count < 0) return MCNLA_B200_ERR_ARG;
+  MB_CHECK_CUDA(cudaSetDevice(ctx->device));
+  return mb::launch_gaussian(ctx, seed, count, out);
+}
+
+int mcnla_b200_orthogonalize(mcnla_b200_ctx* ctx, const mcnla_b200_params* params, double* Q) {
+  if (!ctx || !Q) return MCNLA_B200_ERR_ARG;
+  Dims d;
+  MB_CHECK(mb::get_dims(params, d));
+  MB_CHECK_CUDA(cudaSetDevice(ctx->device));
+  return mb::run_orthogonalize(ctx, d, Q);
+}
+
+int mcnla_b200_integrate(mcnla_b200_ctx* ctx, const mcnla_b200_params* params, int kind, const double* Q,
+                         int max_iteration, double tolerance, double* Qbar, int* iteration) {
+  if (!ctx) return MCNLA_B200_ERR_ARG;
+  Dims d;
+  MB_CHECK(mb::get_dims(params, d));
+  MB_CHECK_CUDA(cudaSetDevice(ctx->device));
+  return mb::run_integrate(ctx, d, kind, Q, max_iteration, tolerance, Qbar, iteration);
+}
+
+int mcnla_b200_form(mcnla_b200_ctx* ctx, const mcnla_b200_params* params, int kind, const double* A, int a_layout,
+                    int64_t lda, const double* Qbar, double* S, double* U, double* V) {
+  if (!ctx) return MCNLA_B200_ERR_ARG;
+  Dims d;
+  MB_CHECK(mb::get_dims(params, d));
+  MB_CHECK_CUDA(cudaSetDevice(ctx->device));
+  return mb::run_form(ctx, d, kind, A, a_layout, lda, Qbar, S, U, V);
+}
+
+int mcnla_b200_isvd(mcnla_b200_ctx* ctx, const mcnla_b200_params* params, int integrator, int former,
+                    const double* A, int a_layout, int64_t lda, const double* omega, uint64_t seed,
+                    int max_iteration, double tolerance, double* S, double* U, double* V, int* iteration) {
+  if (!ctx || !A || !iteration) return MCNLA_B200_ERR_ARG;
+  Dims d;
+  MB_CHECK(mb::get_dims(params, d));
+  MB_CHECK_CUDA(cudaSetDevice(ctx->device));
+  MB_CHECK(mb::ctx_reserve_pipeline(ctx, mb::pipeline_bytes(d)));
+  return mb::run_isvd(ctx, d, integrator, former, A, a_layout, lda, omega, seed, max_iteration, tolerance, S, U, V,
+                      iteration, static_cast<char*>(ctx->parena));
+}
+
+int mcnla_b200_isvd_host(mcnla_b200_ctx* ctx, const mcnla_b200_params* params, int integrator, int former,
+                         const double* A_host, int a_layout, const double* omega_host, int max_iteration,
+                         double tolerance, double* S_host, double* U_host, double* V_host, int* iteration) {
+  if (!ctx || !A_host || !omega_host || !iteration) return MCNLA_B200_ERR_ARG;
+  Dims d;
+  MB_CHECK(mb::get_dims(params, d));
+  MB_CHECK_CUDA(cudaSetDevice(ctx->device));
+  const size_t a_elems = size_t(d.m) * d.n;
+  const size_t io = mb::arena_bytes_for(a_elems, 8) + mb::arena_bytes_for(size_t(d.k), 8) +
+                    mb::arena_bytes_for(size_t(d.m) * d.k, 8) + mb::arena_bytes_for(size_t(d.n) * d.k, 8);
+  MB_CHECK(mb::ctx_reserve_pipeline(ctx, io + mb::pipeline_bytes(d)));
+  char* base = static_cast<char*>(ctx->parena);
+  double* A = reinterpret_cast<double*>(base);
+  base += mb::arena_bytes_for(a_elems, 8);
+  double* S = reinterpret_cast<double*>(base);
+  base += mb::arena_bytes_for(size_t(d.k), 8);
+  double* U = reinterpret_cast<double*>(base);
+  base += mb::arena_bytes_for(size_t(d.m) * d.k, 8);
+  double* V = reinterpret_cast<double*>(base);
+  base += mb::arena_bytes_for(size_t(d.n) * d.k, 8);
+  // omega goes straight into its pipeline slot
+  MB_CHECK_CUDA(cudaMemcpyAsync(A, A_host, a_elems * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  char* pbase = base;
+  double* omega_dev = reinterpret_cast<double*>(pbase + mb::arena_bytes_for(size_t(d.m) * d.L, 8) +
+                                                mb::arena_bytes_for(size_t(d.m) * d.l, 8));
+  MB_CHECK_CUDA(cudaMemcpyAsync(omega_dev, omega_host, size_t(d.n) * d.L * sizeof(double), cudaMemcpyHostToDevice,
+                                ctx->stream));
+  const int64_t lda = a_layout == MCNLA_B200_ROW_MAJOR ? d.n : d.m;
+  MB_CHECK(mb::run_isvd(ctx, d, integrator, former, A, a_layout, lda, omega_dev, 0, max_iteration, tolerance, S, U,
+                        V, iteration, pbase));
+  MB_CHECK_CUDA(cudaMemcpyAsync(S_host, S, size_t(d.k) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  if (U_host)
+    MB_CHECK_CUDA(cudaMemcpyAsync(U_host, U, size_t(d.m) * d.k * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  if (V_host)
+    MB_CHECK_CUDA(cudaMemcpyAsync(V_host, V, size_t(d.n) * d.k * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  MB_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
+  return MCNLA_B200_OK;
+}
+
+int mcnla_b200_dgemm(mcnla_b200_ctx* ctx, int64_t M, int64_t N, int64_t K, double alpha, const double* A,
+                     int64_t a_rs, int64_t a_cs, const double* B, int64_t b_rs, int64_t b_cs, double beta, double* C,
+                     int64_t c_rs, int64_t c_cs, int force_splits) {
+  if (!ctx || (M > 0 && N > 0 && (!C || (K > 0 && (!A || !B))))) return MCNLA_B200_ERR_ARG;
+  MB_CHECK_CUDA(cudaSetDevice(ctx->device));
+  // workspace for the split-K path (forced splits need their own size)
+  size_t wsb = mb::dgemm_workspace_bytes(ctx, M, N, K, 1);
+  if (force_splits > 0) wsb = std::max(wsb, size_t(force_splits) * M * N * sizeof(double));
+  MB_CHECK(mb::ctx_reserve(ctx, wsb + 512));
+  double* ws = nullptr;
+  if (wsb) {
+    ws = mb::ctx_take<double>(ctx, wsb / 8 + 1);
+    ctx->gws = ws;
+    ctx->gws_bytes = ws ? wsb + 8 : 0;
+  }
+  return mb::dgemm(ctx, M, N, K, alpha, mb::cm(A, a_rs, a_cs), mb::cm(B, b_rs, b_cs), beta, mb::dm(C, c_rs, c_cs),
+                   mb::GemmBatch(), ws, force_splits);
+}
+
+int mcnla_b200_inverse_batched(mcnla_b200_ctx* ctx, int n, int batch, double* A) {
+  if (!ctx || !A || n < 1 || batch < 1) return MCNLA_B200_ERR_ARG;
+  MB_CHECK_CUDA(cudaSetDevice(ctx->device));
+  MB_CHECK_CUDA(cudaMemsetAsync(ctx->scal, 0, sizeof(mb::DevScalars), ctx->stream));
+  MB_CHECK(mb::launch_inverse(ctx, n, batch, A));
+  MB_CHECK(mb::ctx_sync_scalars(ctx));
+  return ctx->scal_host->status ? ctx->scal_host->status : MCNLA_B200_OK;
+}
+
+int mcnla_b200_syev_batched(mcnla_b200_ctx* ctx, int n, int batch, const double* A, double* W, double* V,
+                            int order) {
+  if (!ctx || !A || !W || !V || n < 1 || batch < 1 || (order != 0 && order != 1)) return MCNLA_B200_ERR_ARG;
+  MB_CHECK_CUDA(cudaSetDevice(ctx->device));
+  MB_CHECK(mb::ctx_reserve(ctx, mb::arena_bytes_for(size_t(batch) * n * n, 8)));
+  return mb::launch_syev(ctx, n, batch, A, n, int64_t(n) * n, W, V, order);
+}
+
+}  // extern "C"
