@@ -92,8 +92,8 @@ typedef struct mcnla_b200_ctx mcnla_b200_ctx;
 /* ---- context -------------------------------------------------------------
  * Replaces mcnla::init()/gpuInit (include/mcnla/core/def.hpp:42-61,
  * include/mcnla/core_gpu/def.hpp:42-47): binds one device and one stream.
- * stream == NULL creates a private non-blocking stream; otherwise the given
- * cudaStream_t is used (and not destroyed).                                  */
+ * stream is a cudaStream_t; NULL means CUDA's default stream.  The context
+ * never destroys the stream it is given.                                     */
 MCNLA_B200_API int mcnla_b200_create(mcnla_b200_ctx** ctx, int device, void* stream);
 MCNLA_B200_API int mcnla_b200_destroy(mcnla_b200_ctx* ctx);
 MCNLA_B200_API int mcnla_b200_set_stream(mcnla_b200_ctx* ctx, void* stream);

@@ -132,14 +132,9 @@ int mcnla_b200_create(mcnla_b200_ctx** out, int device, void* stream) {
   if (e != cudaSuccess) { mb::set_last_cuda_error(e, "cudaGetDeviceProperties", __FILE__, __LINE__); return fail(MCNLA_B200_ERR_CUDA); }
   c->num_sms = prop.multiProcessorCount;
   c->smem_optin = prop.sharedMemPerBlockOptin;
-  if (stream) {
-    c->stream = static_cast<cudaStream_t>(stream);
-    c->own_stream = false;
-  } else {
-    e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
-    if (e != cudaSuccess) { mb::set_last_cuda_error(e, "cudaStreamCreate", __FILE__, __LINE__); return fail(MCNLA_B200_ERR_CUDA); }
-    c->own_stream = true;
-  }
+  // NULL is CUDA's (legacy) default stream, as in every CUDA API
+  c->stream = static_cast<cudaStream_t>(stream);
+  c->own_stream = false;
   e = cudaMalloc(&c->scal, sizeof(mb::DevScalars));
   if (e != cudaSuccess) { mb::set_last_cuda_error(e, "cudaMalloc scalars", __FILE__, __LINE__); return fail(MCNLA_B200_ERR_NOMEM); }
   e = cudaMallocHost(&c->scal_host, sizeof(mb::DevScalars));
@@ -154,7 +149,7 @@ int mcnla_b200_create(mcnla_b200_ctx** out, int device, void* stream) {
 int mcnla_b200_destroy(mcnla_b200_ctx* c) {
   if (!c) return MCNLA_B200_OK;
   cudaSetDevice(c->device);
-  if (c->stream) cudaStreamSynchronize(c->stream);
+  cudaStreamSynchronize(c->stream);
   for (auto ev : c->events) cudaEventDestroy(ev);
   if (c->arena) cudaFree(c->arena);
   if (c->parena) cudaFree(c->parena);
@@ -171,11 +166,8 @@ int mcnla_b200_set_stream(mcnla_b200_ctx* c, void* stream) {
     MB_CHECK_CUDA(cudaStreamSynchronize(c->stream));
     MB_CHECK_CUDA(cudaStreamDestroy(c->stream));
   }
-  if (stream) { c->stream = static_cast<cudaStream_t>(stream); c->own_stream = false; }
-  else {
-    MB_CHECK_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
-    c->own_stream = true;
-  }
+  c->stream = static_cast<cudaStream_t>(stream);
+  c->own_stream = false;
   return MCNLA_B200_OK;
 }
 
