@@ -50,7 +50,8 @@ struct DevScalars {
   double dot[16];     // scratch reductions
   int status;         // device-side error code (0 = ok)
   int sweeps;         // Jacobi sweeps used by the last small solve
-  int pad[2];
+  int stop_it;        // iteration at which an integrator converged (INT_MAX: not yet)
+  int pad;
 };
 
 // Per-device context: one stream, a growable workspace arena, timing events.
@@ -71,6 +72,11 @@ struct Context {
   // every split-K launch against its size)
   double* gws = nullptr;
   size_t gws_bytes = 0;
+  // iteration guard: while guard_stop is set, every kernel launched for
+  // iteration guard_it returns at once when *guard_stop < guard_it (the
+  // integrator converged earlier on the device).
+  const int* guard_stop = nullptr;
+  int guard_it = 0;
   DevScalars* scal = nullptr;       // device scalars
   DevScalars* scal_host = nullptr;  // pinned mirror
   // stage part timers (CUDA events), filled by the last stage call

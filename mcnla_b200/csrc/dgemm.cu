@@ -25,6 +25,8 @@ struct KArgs {
   double* ws;
   int splits;
   int64_t kps;
+  const int* guard_stop;   // skip the launch when *guard_stop < guard_it
+  int guard_it;
 };
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes) {
@@ -60,66 +62,72 @@ struct Cfg {
   static constexpr size_t SMEM = size_t(STAGES) * STAGE_ELEMS * sizeof(double);
 };
 
-template <class C>
-__device__ __forceinline__ void load_stage(double* sA, double* sB, const KArgs& g, const double* A,
-                                           const double* B, int64_t m0, int64_t n0, int64_t k0, int64_t kend,
-                                           int tid) {
-  constexpr int V = C::VEC;
-  if constexpr (C::AK) {  // rows of A along M, K contiguous
-    constexpr int CPR = BK / V, TOTAL = C::BM * CPR;
+// Per-thread copy plan of one operand tile.  The chunks a thread copies are
+// the same for every k-tile, so their global addresses and row validity are
+// computed once; each k-tile only adds k0 * (k stride) and re-checks the K end.
+//   KROWS: the tile's rows run along M (or N) and K is contiguous;
+//   otherwise the rows run along K and M (or N) is contiguous.
+template <int ROWS_MN, bool KCONTIG, int V, int THREADS, int LD>
+struct TileLoader {
+  static constexpr int CPR = KCONTIG ? BK / V : ROWS_MN / V;        // chunks per smem row
+  static constexpr int TOTAL = KCONTIG ? ROWS_MN * CPR : BK * CPR;
+  static constexpr int PER = (TOTAL + THREADS - 1) / THREADS;
+  const double* src[PER];
+  int mn_valid[PER];   // KCONTIG: row in range; else valid elements along M/N (0..V)
+  int kk[PER];         // k offset of the chunk inside the tile
+  int dst[PER];        // element offset in the smem tile
+  int64_t kstride;     // element stride of k in global memory
+
+  __device__ __forceinline__ void init(const double* base, int64_t mn0, int64_t mn_extent, int64_t ld_mn,
+                                       int64_t ld_k, int tid) {
+    kstride = ld_k;
 #pragma unroll
-    for (int c = tid; c < TOTAL; c += C::THREADS) {
-      const int r = c / CPR, kc = (c % CPR) * V;
-      const int64_t gm = m0 + r, gk = k0 + kc;
-      int valid = 0;
-      if (gm < g.M) { int64_t v = kend - gk; valid = v <= 0 ? 0 : (v >= V ? V : int(v)); }
-      const double* src = valid ? A + gm * g.a_rs + gk : A;
-      double* dst = sA + r * C::LDA + kc;
-      if constexpr (V == 2) cp_async16(dst, src, valid * 8); else cp_async8(dst, src, valid * 8);
-    }
-  } else {  // rows of A along K, M contiguous
-    constexpr int CPR = C::BM / V, TOTAL = BK * CPR;
-#pragma unroll
-    for (int c = tid; c < TOTAL; c += C::THREADS) {
-      const int kr = c / CPR, mc = (c % CPR) * V;
-      const int64_t gk = k0 + kr, gm = m0 + mc;
-      int valid = 0;
-      if (gk < kend) { int64_t v = g.M - gm; valid = v <= 0 ? 0 : (v >= V ? V : int(v)); }
-      const double* src = valid ? A + gk * g.a_cs + gm : A;
-      double* dst = sA + kr * C::LDA + mc;
-      if constexpr (V == 2) cp_async16(dst, src, valid * 8); else cp_async8(dst, src, valid * 8);
-    }
-  }
-  if constexpr (C::BKM) {  // rows of B along N, K contiguous
-    constexpr int CPR = BK / V, TOTAL = C::BN * CPR;
-#pragma unroll
-    for (int c = tid; c < TOTAL; c += C::THREADS) {
-      const int r = c / CPR, kc = (c % CPR) * V;
-      const int64_t gn = n0 + r, gk = k0 + kc;
-      int valid = 0;
-      if (gn < g.N) { int64_t v = kend - gk; valid = v <= 0 ? 0 : (v >= V ? V : int(v)); }
-      const double* src = valid ? B + gn * g.b_cs + gk : B;
-      double* dst = sB + r * C::LDB + kc;
-      if constexpr (V == 2) cp_async16(dst, src, valid * 8); else cp_async8(dst, src, valid * 8);
-    }
-  } else {  // rows of B along K, N contiguous
-    constexpr int CPR = C::BN / V, TOTAL = BK * CPR;
-#pragma unroll
-    for (int c = tid; c < TOTAL; c += C::THREADS) {
-      const int kr = c / CPR, nc = (c % CPR) * V;
-      const int64_t gk = k0 + kr, gn = n0 + nc;
-      int valid = 0;
-      if (gk < kend) { int64_t v = g.N - gn; valid = v <= 0 ? 0 : (v >= V ? V : int(v)); }
-      const double* src = valid ? B + gk * g.b_rs + gn : B;
-      double* dst = sB + kr * C::LDB + nc;
-      if constexpr (V == 2) cp_async16(dst, src, valid * 8); else cp_async8(dst, src, valid * 8);
+    for (int i = 0; i < PER; ++i) {
+      const int c = tid + i * THREADS;
+      if (c >= TOTAL) {   // no chunk for this slot
+        src[i] = base; mn_valid[i] = 0; kk[i] = 0; dst[i] = -1;
+        continue;
+      }
+      if (KCONTIG) {
+        const int r = c / CPR, kc = (c % CPR) * V;
+        const int64_t gmn = mn0 + r;
+        mn_valid[i] = (gmn < mn_extent) ? 1 : 0;
+        src[i] = base + (mn_valid[i] ? gmn * ld_mn : 0) + kc;
+        kk[i] = kc;
+        dst[i] = r * LD + kc;
+      } else {
+        const int kr = c / CPR, mc = (c % CPR) * V;
+        const int64_t gmn = mn0 + mc;
+        const int64_t v = mn_extent - gmn;
+        mn_valid[i] = v <= 0 ? 0 : (v >= V ? V : int(v));
+        src[i] = base + (mn_valid[i] ? gmn : 0) + kr * ld_k;
+        kk[i] = kr;
+        dst[i] = kr * LD + mc;
+      }
     }
   }
-}
+
+  __device__ __forceinline__ void load(double* s, int64_t k0, int64_t kend) const {
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+      if (PER * THREADS > TOTAL && dst[i] < 0) continue;
+      int valid;
+      if (KCONTIG) {
+        const int64_t v = kend - (k0 + kk[i]);
+        valid = mn_valid[i] ? (v <= 0 ? 0 : (v >= V ? V : int(v))) : 0;
+      } else {
+        valid = (k0 + kk[i] < kend) ? mn_valid[i] : 0;
+      }
+      const double* g = valid ? src[i] + (KCONTIG ? k0 : k0 * kstride) : src[i];
+      if (V == 2) cp_async16(s + dst[i], g, valid * 8); else cp_async8(s + dst[i], g, valid * 8);
+    }
+  }
+};
 
 template <class C>
 __global__ void __launch_bounds__(C::THREADS) dgemm_kernel(KArgs g) {
   extern __shared__ __align__(16) double smem[];
+  if (g.guard_stop && *g.guard_stop < g.guard_it) return;
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
   const int wm = warp / C::WARPS_N, wn = warp % C::WARPS_N;
@@ -141,11 +149,19 @@ __global__ void __launch_bounds__(C::THREADS) dgemm_kernel(KArgs g) {
 #pragma unroll
     for (int j = 0; j < C::NT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
+  // A tile: BM rows along M (K contiguous) or BK rows along K (M contiguous);
+  // B tile: BN rows along N (K contiguous) or BK rows along K (N contiguous).
+  TileLoader<C::BM, C::AK, C::VEC, C::THREADS, C::LDA> la;
+  TileLoader<C::BN, C::BKM, C::VEC, C::THREADS, C::LDB> lb;
+  la.init(A, m0, g.M, C::AK ? g.a_rs : 1, C::AK ? 1 : g.a_cs, tid);
+  lb.init(B, n0, g.N, C::BKM ? g.b_cs : 1, C::BKM ? 1 : g.b_rs, tid);
+
 #pragma unroll
   for (int s = 0; s < C::STAGES - 1; ++s) {
     if (s < KT) {
       double* st = smem + s * C::STAGE_ELEMS;
-      load_stage<C>(st, st + C::A_ELEMS, g, A, B, m0, n0, kbeg + int64_t(s) * BK, kend, tid);
+      la.load(st, kbeg + int64_t(s) * BK, kend);
+      lb.load(st + C::A_ELEMS, kbeg + int64_t(s) * BK, kend);
     }
     cp_commit();
   }
@@ -157,7 +173,8 @@ __global__ void __launch_bounds__(C::THREADS) dgemm_kernel(KArgs g) {
       const int nt = kt + C::STAGES - 1;
       if (nt < KT) {
         double* st = smem + (nt % C::STAGES) * C::STAGE_ELEMS;
-        load_stage<C>(st, st + C::A_ELEMS, g, A, B, m0, n0, kbeg + int64_t(nt) * BK, kend, tid);
+        la.load(st, kbeg + int64_t(nt) * BK, kend);
+        lb.load(st + C::A_ELEMS, kbeg + int64_t(nt) * BK, kend);
       }
       cp_commit();
     }
@@ -212,7 +229,9 @@ __global__ void __launch_bounds__(C::THREADS) dgemm_kernel(KArgs g) {
 }
 
 __global__ void splitk_reduce_kernel(const double* ws, int splits, int batch, int64_t M, int64_t N, double alpha,
-                                     double beta, double* C, int64_t c_rs, int64_t c_cs, int64_t c_bs) {
+                                     double beta, double* C, int64_t c_rs, int64_t c_cs, int64_t c_bs,
+                                     const int* guard_stop, int guard_it) {
+  if (guard_stop && *guard_stop < guard_it) return;
   const int64_t MN = M * N;
   const int64_t total = MN * batch;
   for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total;
@@ -245,12 +264,13 @@ int launch(Context* ctx, const KArgs& g, int batch) {
 }
 
 // Tile shape families, picked by the output shape.
-enum Shape { S128x128 = 0, S128x64 = 1, S64x64 = 2, S128x32 = 3, S64x32 = 4 };
+enum Shape { S128x128 = 0, S128x64 = 1, S64x64 = 2, S128x32 = 3, S64x32 = 4, S128x128w16 = 5 };
 
 template <bool AK, bool BKM, int VEC>
 int dispatch_shape(Context* ctx, const KArgs& g, int batch, Shape s) {
   switch (s) {
     case S128x128: return launch<Cfg<128, 128, 64, 32, AK, BKM, VEC, 4>>(ctx, g, batch);
+    case S128x128w16: return launch<Cfg<128, 128, 32, 32, AK, BKM, VEC, 4>>(ctx, g, batch);
     case S128x64: return launch<Cfg<128, 64, 32, 32, AK, BKM, VEC, 4>>(ctx, g, batch);
     case S64x64: return launch<Cfg<64, 64, 32, 32, AK, BKM, VEC, 4>>(ctx, g, batch);
     case S128x32: return launch<Cfg<128, 32, 32, 16, AK, BKM, VEC, 4>>(ctx, g, batch);
@@ -269,7 +289,7 @@ Plan make_plan(const Context* ctx, int64_t M, int64_t N, int64_t K, int batch, i
   Plan p;
   if (N <= 32) { p.shape = M <= 64 ? S64x32 : S128x32; p.bn = 32; }
   else if (N <= 64) { p.shape = M <= 64 ? S64x64 : S128x64; p.bn = 64; }
-  else { p.shape = M <= 64 ? S64x64 : S128x128; p.bn = M <= 64 ? 64 : 128; }
+  else { p.shape = M <= 64 ? S64x64 : S128x128w16; p.bn = M <= 64 ? 64 : 128; }
   p.bm = (p.shape == S64x64 || p.shape == S64x32) ? 64 : 128;
   const int64_t tiles = cdiv(M, p.bm) * cdiv(N, p.bn) * batch;
   int splits = 1;
@@ -317,6 +337,8 @@ int dgemm(Context* ctx, int64_t M, int64_t N, int64_t K, double alpha, CMat A, C
   g.C = Cm.p; g.c_rs = Cm.rs; g.c_cs = Cm.cs; g.c_bs = batch.c;
   g.splits = p.splits; g.kps = p.kps;
   g.ws = nullptr;
+  g.guard_stop = ctx->guard_stop;
+  g.guard_it = ctx->guard_it;
   if (p.splits > 1) {
     const size_t need = size_t(p.splits) * batch.count * M * N * sizeof(double);
     if (!ws || ws != ctx->gws || need > ctx->gws_bytes) return MCNLA_B200_ERR_WORKSPACE;
@@ -337,7 +359,8 @@ int dgemm(Context* ctx, int64_t M, int64_t N, int64_t K, double alpha, CMat A, C
     const int threads = 256;
     const int blocks = int(std::min<int64_t>(cdiv(total, threads), int64_t(ctx->num_sms) * 8));
     splitk_reduce_kernel<<<blocks, threads, 0, ctx->stream>>>(ws, p.splits, batch.count, M, N, alpha, beta, Cm.p,
-                                                             Cm.rs, Cm.cs, batch.c);
+                                                             Cm.rs, Cm.cs, batch.c, ctx->guard_stop,
+                                                             ctx->guard_it);
     ctx->kernels_launched++;
     MB_CHECK_CUDA(cudaGetLastError());
   }

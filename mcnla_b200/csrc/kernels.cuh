@@ -25,8 +25,12 @@ int launch_scale_cols_rsqrt(Context* c, int n, int batch, const double* V, const
 //       ffn  = ff * Fc                 (optional, ff/ffn l x l)
 // scal->norm := || s - 1 ||_2, s = sqrt(1/2 + sqrt(1/4 - eig(Z))).
 // vwork: l*l doubles of global scratch used when V does not fit on chip.
+// When the context's iteration guard is set, the step is skipped for an
+// iteration past convergence, and scal->stop_it is set to the guard
+// iteration when ||s - 1||_2 < tol fails to hold as "norm >= tol" (a NaN norm
+// converges, like the reference's !(nrm2 >= tol)).
 int launch_kn_step(Context* c, int l, const double* z, const double* dd, double inv_n, double* out, double* outn,
-                   const double* ff, double* ffn, double* vwork);
+                   const double* ff, double* ffn, double* vwork, double tol);
 
 // Wen-Yin line-search trial (one CTA): from dd = [Dc | Dgc] and tau builds the
 // 2l x 2l C, inverts it and writes F = [Fc; Fgc] (2l x l) and optionally

@@ -116,8 +116,10 @@ __global__ void k_scale_cols_rsqrt(int n, int batch, const double* V, const doub
 __global__ void __launch_bounds__(kSmallThreads) k_kn_step(int l, const double* z_in, const double* dd,
                                                            double inv_n, double* out, double* outn,
                                                            const double* ff, double* ffn, double* vwork,
-                                                           int v_smem, DevScalars* scal) {
+                                                           int v_smem, DevScalars* scal, double tol,
+                                                           const int* guard_stop, int guard_it) {
   extern __shared__ __align__(16) char smem_raw[];
+  if (guard_stop && *guard_stop < guard_it) return;
   SmemCarve sc(smem_raw);
   const int ld = l + 1;
   double* a = sc.take<double>(size_t(l) * ld);
@@ -199,8 +201,10 @@ __global__ void __launch_bounds__(kSmallThreads) k_kn_step(int l, const double* 
     }
   }
   if (tid == 0) {
-    scal->norm = sqrt(norm2);
+    const double norm = sqrt(norm2);
+    scal->norm = norm;
     scal->sweeps = sweeps;
+    if (guard_stop && !(norm >= tol)) scal->stop_it = guard_it;
   }
 }
 
@@ -614,14 +618,14 @@ int launch_scale_cols_rsqrt(Context* c, int n, int batch, const double* V, const
 }
 
 int launch_kn_step(Context* c, int l, const double* z, const double* dd, double inv_n, double* out, double* outn,
-                   const double* ff, double* ffn, double* vwork) {
+                   const double* ff, double* ffn, double* vwork, double tol) {
   if (l < 1 || l > MCNLA_B200_MAX_DIM_SKETCH) return MCNLA_B200_ERR_UNSUPPORTED;
   const bool v_smem = small_smem_syev(l, true) + l * 8 + 64 <= c->smem_optin;
   const size_t smem = small_smem_syev(l, v_smem) + l * 8 + 64;
   if (smem > c->smem_optin) return MCNLA_B200_ERR_UNSUPPORTED;
   MB_CHECK(set_smem(reinterpret_cast<const void*>(k_kn_step), smem));
   k_kn_step<<<1, kSmallThreads, smem, c->stream>>>(l, z, dd, inv_n, out, outn, ff, ffn, vwork, v_smem ? 1 : 0,
-                                                    c->scal);
+                                                    c->scal, tol, c->guard_stop, c->guard_it);
   c->kernels_launched++;
   MB_CHECK_CUDA(cudaGetLastError());
   return MCNLA_B200_OK;

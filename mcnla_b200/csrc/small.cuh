@@ -78,9 +78,14 @@ __device__ inline int cta_jacobi_eig(double* a, int lda, double* v, int ldv, int
   const int P = (n + 1) & ~1;
   const int npairs = P / 2;
   const double fro2 = cta_frob2(a, lda, n, js.red);
-  // Off-diagonal entries below this are treated as zero (absolute floor for
-  // exactly singular inputs); the relative test below drives convergence.
-  const double abs_floor = 1e-40 + 1e-34 * fro2;
+  // An off-diagonal entry is left alone when it is below eps * sqrt(|app aqq|)
+  // (relative test) or below eps * ||A||_F (absolute floor: LAPACK's
+  // eigensolvers are normwise accurate to that level, and below it rounding
+  // in the rotations regenerates off-diagonal noise faster than a sweep
+  // removes it).
+  const double eps = 2.220446049250313e-16;
+  const double abs_floor = eps * eps * fro2;
+  const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
   int sweep = 0;
   for (; sweep < max_sweeps; ++sweep) {
     int rotated = 0;
@@ -96,7 +101,7 @@ __device__ inline int cta_jacobi_eig(double* a, int lda, double* v, int ldv, int
           apq = a[p * lda + q];
           app = a[p * lda + p];
           aqq = a[q * lda + q];
-          const double thr = 2.220446049250313e-16 * sqrt(fabs(app) * fabs(aqq));
+          const double thr = eps * sqrt(fabs(app) * fabs(aqq));
           if (fabs(apq) > thr && apq * apq > abs_floor) {
             const double theta = (aqq - app) / (2.0 * apq);
             const double at = fabs(theta);
@@ -115,38 +120,42 @@ __device__ inline int cta_jacobi_eig(double* a, int lda, double* v, int ldv, int
       const int cnt = *js.count;
       if (cnt == 0) { __syncthreads(); continue; }
       rotated += cnt;
-      // 2. rows: a <- J' a
-      for (int e = tid; e < npairs * n; e += nt) {
-        const int k = e / n, j = e % n;
-        if (js.s[k] == 0.0) continue;
+      // 2. rows: a <- J' a   (a warp per pair, lanes along the row)
+      for (int k = warp; k < npairs; k += nwarps) {
+        const double s = js.s[k];
+        if (s == 0.0) continue;
+        const double c = js.c[k];
         const int p = js.p[k], q = js.q[k];
-        const double c = js.c[k], s = js.s[k];
-        const double x = a[p * lda + j], y = a[q * lda + j];
-        a[p * lda + j] = c * x - s * y;
-        a[q * lda + j] = s * x + c * y;
+        for (int j = lane; j < n; j += 32) {
+          const double x = a[p * lda + j], y = a[q * lda + j];
+          a[p * lda + j] = c * x - s * y;
+          a[q * lda + j] = s * x + c * y;
+        }
       }
       __syncthreads();
       // 3. columns: a <- a J and v <- v J.  The 2x2 block of each pair is
       //    written exactly: J' B J = diag(app - t apq, aqq + t apq).
-      for (int e = tid; e < npairs * n; e += nt) {
-        const int k = e / n, i = e % n;
-        if (js.s[k] == 0.0) continue;
+      for (int k = warp; k < npairs; k += nwarps) {
+        const double s = js.s[k];
+        if (s == 0.0) continue;
+        const double c = js.c[k];
         const int p = js.p[k], q = js.q[k];
-        const double c = js.c[k], s = js.s[k];
-        if (i == p) {
-          a[p * lda + p] = js.app[k] - js.t[k] * js.apq[k];
-          a[p * lda + q] = 0.0;
-        } else if (i == q) {
-          a[q * lda + q] = js.aqq[k] + js.t[k] * js.apq[k];
-          a[q * lda + p] = 0.0;
-        } else {
-          const double x = a[i * lda + p], y = a[i * lda + q];
-          a[i * lda + p] = c * x - s * y;
-          a[i * lda + q] = s * x + c * y;
+        for (int i = lane; i < n; i += 32) {
+          if (i == p) {
+            a[p * lda + p] = js.app[k] - js.t[k] * js.apq[k];
+            a[p * lda + q] = 0.0;
+          } else if (i == q) {
+            a[q * lda + q] = js.aqq[k] + js.t[k] * js.apq[k];
+            a[q * lda + p] = 0.0;
+          } else {
+            const double x = a[i * lda + p], y = a[i * lda + q];
+            a[i * lda + p] = c * x - s * y;
+            a[i * lda + q] = s * x + c * y;
+          }
+          const double vx = v[i * ldv + p], vy = v[i * ldv + q];
+          v[i * ldv + p] = c * vx - s * vy;
+          v[i * ldv + q] = s * vx + c * vy;
         }
-        const double vx = v[i * ldv + p], vy = v[i * ldv + q];
-        v[i * ldv + p] = c * vx - s * vy;
-        v[i * ldv + q] = s * vx + c * vy;
       }
       __syncthreads();
     }

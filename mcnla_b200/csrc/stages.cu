@@ -136,7 +136,34 @@ int run_orthogonalize(Context* c, const Dims& d, double* Q) {
 // ---------------------------------------------------------------------------
 // Integrators
 // ---------------------------------------------------------------------------
-bool kn_converged(double norm, double tol) { return !(norm >= tol); }
+// Kolmogorov-Nagumo iteration driver.  The reference's loop
+//   for (it = 0; it < maxit && !converged; ++it) { body; converged = !(norm >= tol); }
+// runs here without a host round trip per iteration: iterations are launched
+// in chunks, the KN step records on the device the first iteration whose
+// norm converged (scal->stop_it), and every kernel launched for a later
+// iteration returns at once.  The host reads stop_it once per chunk.
+// Returns the number of executed bodies (the reference's iteration()).
+template <class Body>
+int kn_loop(Context* c, int maxit, Body body, int* iters) {
+  MB_CHECK_CUDA(cudaMemsetAsync(&c->scal->stop_it, 0x7f, sizeof(int), c->stream));   // "not yet"
+  struct Reset { Context* c; ~Reset() { c->guard_stop = nullptr; c->guard_it = 0; } } reset{c};
+  c->guard_stop = &c->scal->stop_it;
+  const int chunk = 8;
+  int launched = 0, done = -1;
+  while (launched < maxit) {
+    const int end = std::min(maxit, launched + chunk);
+    for (int it = launched; it < end; ++it) {
+      c->guard_it = it;
+      MB_CHECK(body(it));
+    }
+    launched = end;
+    MB_CHECK(ctx_sync_scalars(c));
+    const int stop = c->scal_host->stop_it;
+    if (stop < launched) { done = stop + 1; break; }
+  }
+  *iters = done < 0 ? launched : done;
+  return MCNLA_B200_OK;
+}
 
 // KolmogorovNagumoIntegrator (kolmogorov_nagumo_integrator.hpp:76-185)
 int run_kn(Context* c, const Dims& d, const double* Qs, int maxit, double tol, double* Qbar, int* iters) {
@@ -161,9 +188,9 @@ int run_kn(Context* c, const Dims& d, const double* Qs, int maxit, double tol, d
   // Qc := Q0   (:105)
   MB_CHECK(copy2d(c, QX[0], lq, Qs, L, m, l));
   MB_CHECK(ctx_toc(c));
-  int cur = 0, it = 0;
-  bool converged = false;
-  for (; it < maxit && !converged;) {
+  int it = 0;
+  MB_CHECK(kn_loop(c, maxit, [&](int i) -> int {
+    const int cur = i & 1;
     double* Qc = QX[cur];
     double* X = QX[cur] + l;
     // B := Qs' Qc   (:117)
@@ -175,15 +202,13 @@ int run_kn(Context* c, const Dims& d, const double* Qs, int maxit, double tol, d
     MB_CHECK(dgemm(c, m, l, l, -inv_n, crow(Qc, lq), crow(D, l), 1.0, drow(X, lq), GemmBatch(), ws));
     // Z := X' X   (:143)
     MB_CHECK(dgemm(c, l, l, m, 1.0, cm(X, 1, lq), crow(X, lq), 0.0, drow(Z, l), GemmBatch(), ws));
-    // eig(Z); C, inv(C)   (:146-164)
-    MB_CHECK(launch_kn_step(c, l, Z, nullptr, inv_n, CC, nullptr, nullptr, nullptr, vwork));
+    // eig(Z); C, inv(C); convergence test   (:146-164, :174-181)
+    MB_CHECK(launch_kn_step(c, l, Z, nullptr, inv_n, CC, nullptr, nullptr, nullptr, vwork, tol));
     // Qc := Qc C + X inv(C) = [Qc X] [C; inv(C)]   (:170-171)
     MB_CHECK(dgemm(c, m, l, 2 * l, 1.0, crow(QX[cur], lq), crow(CC, l), 0.0, drow(QX[1 - cur], lq), GemmBatch(), ws));
-    cur = 1 - cur;
-    ++it;
-    MB_CHECK(ctx_sync_scalars(c));
-    converged = kn_converged(c->scal_host->norm, tol);   // (:174-181)
-  }
+    return MCNLA_B200_OK;
+  }, &it));
+  const int cur = it & 1;
   MB_CHECK(copy2d(c, Qbar, l, QX[cur], lq, m, l));
   MB_CHECK(ctx_toc(c));
   *iters = it;
@@ -213,25 +238,23 @@ int run_rb_kn(Context* c, const Dims& d, const double* Qs, int maxit, double tol
   MB_CHECK(copy2d(c, QG[0], l2, Qs, L, m, l));
   MB_CHECK(dgemm(c, L, l, m, 1.0, cm(Qs, 1, L), crow(QG[0], l2), 0.0, drow(BB[0], l2), GemmBatch(), ws));
   MB_CHECK(ctx_toc(c));
-  int cur = 0, it = 0;
-  bool converged = false;
-  for (; it < maxit && !converged;) {
+  int it = 0;
+  MB_CHECK(kn_loop(c, maxit, [&](int i) -> int {
+    const int cur = i & 1;
     // Gc := 1/N Qs Bc   (:138)
     MB_CHECK(dgemm(c, m, l, L, inv_n, crow(Qs, L), crow(BB[cur], l2), 0.0, drow(QG[cur] + l, l2), GemmBatch(), ws));
     // Bgc := Qs' Gc   (:141)
     MB_CHECK(dgemm(c, L, l, m, 1.0, cm(Qs, 1, L), crow(QG[cur] + l, l2), 0.0, drow(BB[cur] + l, l2), GemmBatch(), ws));
     // [Dc | Dgc] := 1/N Bc' [Bc | Bgc]   (:147-150)
     MB_CHECK(dgemm(c, l, l2, L, inv_n, cm(BB[cur], 1, l2), crow(BB[cur], l2), 0.0, drow(DD, l2), GemmBatch(), ws));
-    // Z := Dgc - Dc^2; eig; C, inv(C); Fc := C - Dc inv(C)   (:156-186)
-    MB_CHECK(launch_kn_step(c, l, nullptr, DD, inv_n, FC, nullptr, nullptr, nullptr, vwork));
+    // Z := Dgc - Dc^2; eig; C, inv(C); Fc := C - Dc inv(C); convergence test   (:156-201)
+    MB_CHECK(launch_kn_step(c, l, nullptr, DD, inv_n, FC, nullptr, nullptr, nullptr, vwork, tol));
     // Q+ := [Qc Gc] [Fc; inv(C)];  B+ := [Bc Bgc] [Fc; inv(C)]   (:189-194)
     MB_CHECK(dgemm(c, m, l, l2, 1.0, crow(QG[cur], l2), crow(FC, l), 0.0, drow(QG[1 - cur], l2), GemmBatch(), ws));
     MB_CHECK(dgemm(c, L, l, l2, 1.0, crow(BB[cur], l2), crow(FC, l), 0.0, drow(BB[1 - cur], l2), GemmBatch(), ws));
-    cur = 1 - cur;
-    ++it;
-    MB_CHECK(ctx_sync_scalars(c));
-    converged = kn_converged(c->scal_host->norm, tol);   // (:198-201)
-  }
+    return MCNLA_B200_OK;
+  }, &it));
+  const int cur = it & 1;
   MB_CHECK(copy2d(c, Qbar, l, QG[cur], l2, m, l));   // (:205)
   MB_CHECK(ctx_toc(c));
   *iters = it;
@@ -284,9 +307,9 @@ int run_rb_gramian_kn(Context* c, const Dims& d, const double* Qs, int maxit, do
   MB_CHECK(launch_fill(c, L, l, 0.0, EB[0], l3));
   MB_CHECK(launch_set_identity(c, l, FF[0], l));
   MB_CHECK(ctx_toc(c));
-  int cur = 0, it = 0;
-  bool converged = false;
-  for (; it < maxit && !converged;) {
+  int it = 0;
+  MB_CHECK(kn_loop(c, maxit, [&](int i) -> int {
+    const int cur = i & 1;
     double* Ec = EB[cur];
     double* Bc = EB[cur] + l;
     double* Bgc = EB[cur] + l2;
@@ -294,17 +317,15 @@ int run_rb_gramian_kn(Context* c, const Dims& d, const double* Qs, int maxit, do
     MB_CHECK(dgemm(c, L, l, L, inv_n, crow(Bs, L), crow(Bc, l3), 0.0, drow(Bgc, l3), GemmBatch(), ws));
     // [Dc | Dgc] := 1/N Bc' [Bc | Bgc]   (:155-158)
     MB_CHECK(dgemm(c, l, l2, L, inv_n, cm(Bc, 1, l3), crow(Bc, l3), 0.0, drow(DD, l2), GemmBatch(), ws));
-    // Z, eig, C, inv(C), Fc; F~+ := F~c Fc   (:164-197)
-    MB_CHECK(launch_kn_step(c, l, nullptr, DD, inv_n, FC, FCN, FF[cur], FF[1 - cur], vwork));
+    // Z, eig, C, inv(C), Fc; F~+ := F~c Fc; convergence test   (:164-214)
+    MB_CHECK(launch_kn_step(c, l, nullptr, DD, inv_n, FC, FCN, FF[cur], FF[1 - cur], vwork, tol));
     // E~+ := E~c Fc + 1/N Bc inv(C) = [E~c Bc] [Fc; inv(C)/N]   (:194, :200)
     MB_CHECK(dgemm(c, L, l, l2, 1.0, crow(Ec, l3), crow(FCN, l), 0.0, drow(EB[1 - cur], l3), GemmBatch(), ws));
     // B+ := [Bc Bgc] [Fc; inv(C)]   (:203-204)
     MB_CHECK(dgemm(c, L, l, l2, 1.0, crow(Bc, l3), crow(FC, l), 0.0, drow(EB[1 - cur] + l, l3), GemmBatch(), ws));
-    cur = 1 - cur;
-    ++it;
-    MB_CHECK(ctx_sync_scalars(c));
-    converged = kn_converged(c->scal_host->norm, tol);   // (:207-214)
-  }
+    return MCNLA_B200_OK;
+  }, &it));
+  const int cur = it & 1;
   MB_CHECK(ctx_toc(c));
   // Qbar := Q0 F~ + Qs E~   (:225-226)
   MB_CHECK(gramian_form_qbar(c, d, Qs, EB[cur], l3, FF[cur], Ebar, Qbar, ws));

@@ -260,6 +260,18 @@ def test_pipeline_config1_shape(cuda, integrator, former):
     assert np.abs(O.align_signs(v, ref["v"]) - ref["v"]).max() < TOL
 
 
+def rounding_sensitivity(a, omega, k, p, N, integ, tol, ref):
+    """How far the reference algorithm itself moves sigma when A is perturbed
+    at the rounding level (1e-16 relative): the floor of any two FP64
+    implementations' agreement.  The row-block Gramian Wen-Yin integrator
+    amplifies rounding by about 1e7 (its Qbar = Q0 F~ + Qs E~ cancels), the
+    others stay near 1e-15."""
+    rng = np.random.default_rng(1)
+    a1 = a * (1 + 1e-16 * rng.standard_normal(a.shape))
+    r1 = O.isvd(a1, omega, k, p, N, integrator=integ, former="svd", tol=tol)
+    return float(np.max(np.abs(r1["s"] - ref["s"]) / ref["s"]))
+
+
 @pytest.mark.parametrize("m,n,k,p,N", [(97, 61, 3, 2, 1), (257, 129, 7, 5, 3), (640, 300, 30, 2, 4),
                                        (50, 2000, 8, 8, 2)])
 def test_pipeline_ragged_shapes(cuda, m, n, k, p, N):
@@ -268,11 +280,12 @@ def test_pipeline_ragged_shapes(cuda, m, n, k, p, N):
     a = synthetic.lowrank_np(m, n, 1.0 / np.arange(1, min(m, n) + 1), seed=m)
     omega = rng.standard_normal((n, (k + p) * N))
     for integ in ("kn", "rb_gramian_wy"):
+        ref = O.isvd(a, omega, k, p, N, integrator=integ, former="svd", tol=1e-4)
+        tol_s = max(TOL, 20 * rounding_sensitivity(a, omega, k, p, N, integ, 1e-4, ref))
         for colmajor in (False, True):
             s, u, v, it = _pipeline(cuda, a, omega, k, p, N, integ, "svd", 1e-4, colmajor)
-            ref = O.isvd(a, omega, k, p, N, integrator=integ, former="svd", tol=1e-4)
             assert it == ref["iterations"]
-            np.testing.assert_allclose(s, ref["s"], rtol=TOL)
+            np.testing.assert_allclose(s, ref["s"], rtol=tol_s)
 
 
 def test_host_entry_point_matches_device(cuda):
