@@ -272,6 +272,21 @@ def run_b200(args, world, rank, local):
     former(a, qbar)
     stages = {"sketch_s": sk.time(), "sketch_gemm_s": sketch_s, "orthogonalize_s": orth.time(),
               "integrate_s": integ.time(), "integrate_iterations": integ.iteration(), "form_s": former.time()}
+    # every integrator on the same orthonormal sketches (tol and maxit of the workload)
+    variants = {}
+    if world == 1 and not args.quick:
+        for name, cls in (("kn", isvd.KolmogorovNagumoIntegrator),
+                          ("rb_kn", isvd.RowBlockKolmogorovNagumoIntegrator),
+                          ("rb_gramian_kn", isvd.RowBlockGramianKolmogorovNagumoIntegrator),
+                          ("rb_wy", isvd.RowBlockWenYinIntegrator),
+                          ("rb_gramian_wy", isvd.RowBlockGramianWenYinIntegrator)):
+            if "wy" in name and l > _lib.MAX_DIM_SKETCH_WENYIN:
+                continue
+            it_ = cls(prm, args.maxit, args.tol)
+            it_.initialize()
+            it_(q, qbar)
+            variants[name] = {"s": round(it_.time(), 5), "iterations": it_.iteration(),
+                              "s_per_iteration": round(it_.time() / max(1, it_.iteration()), 7)}
     peak64 = fp64_peak_tflops()
     flops = 2.0 * m * n * L
     achieved = flops / sketch_s / 1e12
@@ -323,7 +338,7 @@ def run_b200(args, world, rank, local):
         "a_read_gbs": round(2 * m * n * 8 * world * args.steps / total / 1e9, 2),
         "p50_ms": round(step_ms[len(step_ms) // 2], 3),
         "p99_ms": round(step_ms[min(len(step_ms) - 1, int(0.99 * len(step_ms)))], 3),
-        "iterations": iters[-1], "stages": stages, "roofline": roofline, "e2e": e2e,
+        "iterations": iters[-1], "stages": stages, "integrators": variants, "roofline": roofline, "e2e": e2e,
         "gpu_launches": int(launches), "clocks": clk,
     }
     return result

@@ -103,6 +103,16 @@ MCNLA_B200_API const char* mcnla_b200_last_error(void);
 /* Number of kernels this context has launched (for launch accounting). */
 MCNLA_B200_API int64_t mcnla_b200_kernels_launched(const mcnla_b200_ctx* ctx);
 
+/* Kolmogorov-Nagumo step method.  The reference forms C = f(Z) and inv(C)
+ * from an eigendecomposition of Z (row_block_kolmogorov_nagumo_integrator.hpp:159-180).
+ * MCNLA_B200_KN_AUTO (default) evaluates the same matrix functions by coupled
+ * Newton-Schulz iterations on the FP64 MMA when l <= 80 and falls back to the
+ * eigendecomposition when they do not converge; MCNLA_B200_KN_EIGEN always
+ * uses the eigendecomposition (parallel Jacobi).                             */
+#define MCNLA_B200_KN_AUTO  0
+#define MCNLA_B200_KN_EIGEN 1
+MCNLA_B200_API int mcnla_b200_set_kn_method(mcnla_b200_ctx* ctx, int method);
+
 /* Stage timers: seconds per part of the last stage call, the reference's
  * StageWrapper::times() (include/mcnla/isvd/core/stage_wrapper.hpp:128-135),
  * measured with CUDA events.  Synchronizes the stream.  Returns the number of

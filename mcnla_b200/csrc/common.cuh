@@ -77,6 +77,9 @@ struct Context {
   // integrator converged earlier on the device).
   const int* guard_stop = nullptr;
   int guard_it = 0;
+  // KN step: 0 = matrix functions by Newton-Schulz when l <= 80 (eigen
+  // fallback), 1 = always the eigendecomposition (Jacobi) path
+  int kn_mode = 0;
   DevScalars* scal = nullptr;       // device scalars
   DevScalars* scal_host = nullptr;  // pinned mirror
   // stage part timers (CUDA events), filled by the last stage call

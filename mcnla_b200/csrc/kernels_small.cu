@@ -8,6 +8,7 @@ namespace {
 
 constexpr int kSmallThreads = 512;
 constexpr int kMaxSweeps = 40;
+constexpr int kKnNsMaxDim = 80;   // the matrix-function KN step keeps four padded l x l matrices on chip
 
 // Shared-memory carve-up shared by the one-CTA solvers.
 struct SmemCarve {
@@ -204,6 +205,254 @@ __global__ void __launch_bounds__(kSmallThreads) k_kn_step(int l, const double* 
     const double norm = sqrt(norm2);
     scal->norm = norm;
     scal->sweeps = sweeps;
+    if (guard_stop && !(norm >= tol)) scal->stop_it = guard_it;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Kolmogorov-Nagumo step by matrix functions (l <= 80)
+//
+// The step needs C = f(Z) and inv(C) for f(x) = sqrt(1/2 + sqrt(1/4 - x)),
+// which the reference forms from an eigendecomposition of Z
+// (row_block_kolmogorov_nagumo_integrator.hpp:159-180).  Here they come from
+// two coupled Newton-Schulz iterations (Higham, Functions of Matrices, 2008,
+// eq. 6.35; inversion-free, built from matrix products only):
+//   S = (I - 4Z)^(1/2)            -> sqrt(1/4 - Z) = S/2
+//   C = ((I + S)/2)^(1/2), inv(C) = ((I + S)/2)^(-1/2)
+// The products run on the FP64 MMA inside one CTA.  Jacobi on the
+// clustered spectrum Z has near convergence (dozens of near-zero
+// eigenvalues) needs 15-20 sweeps; the iteration above needs a handful of
+// products.  When an iteration fails (non-finite values or no convergence,
+// e.g. an eigenvalue of Z above 1/4 where the reference produces NaN), the
+// kernel falls back to the eigendecomposition path of k_kn_step.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void small_dmma(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+// C := A * op(B) for lp x lp matrices in shared memory (lp a multiple of 16,
+// row stride ld, zero padding outside the active block).  Each warp owns
+// 16 x 16 output blocks (four independent 8 x 8 MMA accumulators).  C must not
+// alias A or B.  Ends with a block barrier.
+template <bool TB>
+__device__ void cta_mm16(double* C, const double* A, const double* B, int lp, int ld) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int g = lane >> 2, t4 = lane & 3;
+  const int nb = lp >> 4;
+  for (int blk = warp; blk < nb * nb; blk += nw) {
+    const int bi = (blk / nb) * 16, bj = (blk % nb) * 16;
+    double c[2][2][2] = {{{0.0, 0.0}, {0.0, 0.0}}, {{0.0, 0.0}, {0.0, 0.0}}};
+    for (int k = 0; k < lp; k += 4) {
+      const double a0 = A[(bi + g) * ld + k + t4];
+      const double a1 = A[(bi + 8 + g) * ld + k + t4];
+      const double b0 = TB ? B[(bj + g) * ld + k + t4] : B[(k + t4) * ld + bj + g];
+      const double b1 = TB ? B[(bj + 8 + g) * ld + k + t4] : B[(k + t4) * ld + bj + 8 + g];
+      small_dmma(c[0][0][0], c[0][0][1], a0, b0);
+      small_dmma(c[0][1][0], c[0][1][1], a0, b1);
+      small_dmma(c[1][0][0], c[1][0][1], a1, b0);
+      small_dmma(c[1][1][0], c[1][1][1], a1, b1);
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        double* cp = C + (bi + i * 8 + g) * ld + bj + j * 8 + 2 * t4;
+        cp[0] = c[i][j][0];
+        cp[1] = c[i][j][1];
+      }
+  }
+  __syncthreads();
+}
+
+// Coupled Newton-Schulz for M^(1/2) and M^(-1/2): on entry *Y holds M; on
+// success *Y = M^(1/2), *Zm = M^(-1/2).  Buffers are rotated through the four
+// pointers.  Returns the iterations used, or -1 (non-finite or no convergence).
+__device__ int cta_ns_sqrt(double*& Y, double*& Zm, double*& T, double*& W, int l, int lp, int ld, double* red,
+                           int maxit) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int e = tid; e < lp * lp; e += nt) {
+    const int i = e / lp, j = e % lp;
+    Zm[i * ld + j] = (i == j && i < l) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  bool polish = false;
+  for (int it = 0; it < maxit; ++it) {
+    cta_mm16<false>(W, Zm, Y, lp, ld);                      // P = Zm Y
+    double part = 0.0;
+    for (int e = tid; e < lp * lp; e += nt) {
+      const int i = e / lp, j = e % lp;
+      const double pij = W[i * ld + j];
+      const double d = ((i == j && i < l) ? 1.0 : 0.0) - pij;
+      part += d * d;
+      T[i * ld + j] = (i < l && j < l) ? 0.5 * (((i == j) ? 3.0 : 0.0) - pij) : 0.0;   // T = (3I - P)/2
+    }
+    const double r2 = small::cta_sum(part, red);
+    if (!(r2 < 1e300)) return -1;                           // non-finite
+    if (polish) return it;
+    if (r2 < 1e-18) polish = true;                          // one more step reaches rounding level
+    cta_mm16<false>(W, Y, T, lp, ld);                       // Y+ = Y T
+    double* oldY = Y;
+    Y = W;
+    cta_mm16<false>(oldY, T, Zm, lp, ld);                   // Z+ = T Zm
+    W = Zm;
+    Zm = oldY;
+  }
+  return -1;
+}
+
+__global__ void __launch_bounds__(kSmallThreads) k_kn_step_ns(int l, const double* z_in, const double* dd,
+                                                              double inv_n, double* out, double* outn,
+                                                              const double* ff, double* ffn, double* vwork,
+                                                              DevScalars* scal, double tol, const int* guard_stop,
+                                                              int guard_it) {
+  extern __shared__ __align__(16) char smem_raw[];
+  if (guard_stop && *guard_stop < guard_it) return;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int lp = (l + 15) & ~15, ld = lp + 4;
+  const size_t mat = size_t(lp) * ld;
+  double* buf = reinterpret_cast<double*>(smem_raw);
+  double* B0 = buf;
+  double* B1 = buf + mat;
+  double* B2 = buf + 2 * mat;
+  double* B3 = buf + 3 * mat;
+  double* red = buf + 4 * mat;          // 64 doubles
+  double* sv = red + 64;                // 96 doubles (eigen fallback)
+  const int ldd = 2 * l;
+  // ---- Z (upper triangle mirrored, as a symmetric eigensolver reads it) into B0
+  if (dd == nullptr) {
+    for (int e = tid; e < lp * lp; e += nt) {
+      const int i = e / lp, j = e % lp;
+      B0[i * ld + j] = (i < l && j < l) ? z_in[min(i, j) * l + max(i, j)] : 0.0;
+    }
+    __syncthreads();
+  } else {
+    // Z := Dgc - Dc Dc'   (row_block_kolmogorov_nagumo_integrator.hpp:150-156)
+    for (int e = tid; e < lp * lp; e += nt) {
+      const int i = e / lp, j = e % lp;
+      B1[i * ld + j] = (i < l && j < l) ? dd[i * ldd + j] : 0.0;
+    }
+    __syncthreads();
+    cta_mm16<true>(B2, B1, B1, lp, ld);
+    for (int e = tid; e < lp * lp; e += nt) {
+      const int i = e / lp, j = e % lp;
+      const int a = min(i, j), b = max(i, j);
+      B0[i * ld + j] = (i < l && j < l) ? dd[a * ldd + l + b] - B2[a * ld + b] : 0.0;
+    }
+    __syncthreads();
+  }
+  // ---- M1 = I - 4Z; S = M1^(1/2)
+  for (int e = tid; e < lp * lp; e += nt) {
+    const int i = e / lp, j = e % lp;
+    const double z = B0[i * ld + j];
+    B0[i * ld + j] = (i < l && j < l) ? ((i == j) ? 1.0 : 0.0) - 4.0 * z : 0.0;
+  }
+  __syncthreads();
+  double *Y = B0, *Zm = B1, *T = B2, *W = B3;
+  int it1 = cta_ns_sqrt(Y, Zm, T, W, l, lp, ld, red, 60);
+  int it2 = -1;
+  if (it1 >= 0) {
+    // M2 = (I + S)/2 into Zm's buffer, then C = M2^(1/2), inv(C) = M2^(-1/2)
+    for (int e = tid; e < lp * lp; e += nt) {
+      const int i = e / lp, j = e % lp;
+      Zm[i * ld + j] = (i < l && j < l) ? 0.5 * (((i == j) ? 1.0 : 0.0) + Y[i * ld + j]) : 0.0;
+    }
+    __syncthreads();
+    double* tmp = Y;
+    Y = Zm;
+    Zm = tmp;
+    it2 = cta_ns_sqrt(Y, Zm, T, W, l, lp, ld, red, 60);
+  }
+  if (it1 < 0 || it2 < 0) {
+    // eigendecomposition fallback (the reference's path, NaN semantics included)
+    if (tid == 0) scal->sweeps = -1;
+    // recompute Z into B0 (as above) and run the Jacobi step on it
+    if (dd == nullptr) {
+      for (int e = tid; e < l * l; e += nt) B0[(e / l) * (l + 1) + (e % l)] = z_in[e];
+    } else {
+      for (int e = tid; e < l * l; e += nt) {
+        const int i = e / l, j = e % l;
+        double s = 0.0;
+        for (int k = 0; k < l; ++k) s = fma(dd[i * ldd + k], dd[j * ldd + k], s);
+        B0[i * (l + 1) + j] = dd[i * ldd + l + j] - s;
+      }
+    }
+    __syncthreads();
+    // the Jacobi matrices sit in B0 | B1 (l (l+1) <= lp (lp+4)), its scratch after sv
+    SmemCarve sc(reinterpret_cast<char*>(sv + 96));
+    small::JacobiScratch js = carve_jacobi(sc, l);
+    double* v = B1;
+    small::cta_jacobi_eig(B0, l + 1, v, l + 1, l, true, js, kMaxSweeps);
+    for (int i = tid; i < l; i += nt) sv[i] = sqrt(sqrt(0.5 + sqrt(0.25 - B0[i * (l + 1) + i])));
+    __syncthreads();
+    // C and inv(C) into B2 / B3 in the padded layout
+    for (int e = tid; e < lp * lp; e += nt) {
+      const int i = e / lp, j = e % lp;
+      double cc = 0.0, ci = 0.0;
+      if (i < l && j < l) {
+        for (int k = 0; k < l; ++k) {
+          const double x = v[i * (l + 1) + k], y = v[j * (l + 1) + k];
+          cc = fma(x * sv[k], y * sv[k], cc);
+          ci = fma(x / sv[k], y / sv[k], ci);
+        }
+      }
+      B2[i * ld + j] = cc;
+      B3[i * ld + j] = ci;
+    }
+    __syncthreads();
+    Y = B2;
+    Zm = B3;
+    T = B0;
+    W = B1;
+  }
+  // ---- C in *Y, inv(C) in *Zm;  ||e - 1||_2 = ||C - I||_F
+  double part = 0.0;
+  for (int e = tid; e < l * l; e += nt) {
+    const int i = e / l, j = e % l;
+    const double d = Y[i * ld + j] - ((i == j) ? 1.0 : 0.0);
+    part += d * d;
+    out[size_t(l) * l + e] = Zm[i * ld + j];                  // rows [l, 2l): inv(C)
+  }
+  const double norm2 = small::cta_sum(part, red);
+  if (dd == nullptr) {
+    for (int e = tid; e < l * l; e += nt) out[e] = Y[(e / l) * ld + (e % l)];   // rows [0, l): C
+  } else {
+    // Fc := C - Dc inv(C)   (row_block_kolmogorov_nagumo_integrator.hpp:186)
+    for (int e = tid; e < lp * lp; e += nt) {
+      const int i = e / lp, j = e % lp;
+      T[i * ld + j] = (i < l && j < l) ? dd[i * ldd + j] : 0.0;
+    }
+    __syncthreads();
+    cta_mm16<false>(W, T, Zm, lp, ld);
+    for (int e = tid; e < lp * lp; e += nt) {
+      const int i = e / lp, j = e % lp;
+      const double fc = (i < l && j < l) ? Y[i * ld + j] - W[i * ld + j] : 0.0;
+      W[i * ld + j] = fc;
+      if (i < l && j < l) {
+        out[i * l + j] = fc;
+        if (outn) {
+          outn[i * l + j] = fc;
+          outn[size_t(l) * l + i * l + j] = Zm[i * ld + j] * inv_n;
+        }
+      }
+    }
+    __syncthreads();
+    if (ff && ffn) {
+      // F~+ := F~c Fc  (row_block_gramian_kolmogorov_nagumo_integrator.hpp:197)
+      for (int e = tid; e < lp * lp; e += nt) {
+        const int i = e / lp, j = e % lp;
+        T[i * ld + j] = (i < l && j < l) ? ff[i * l + j] : 0.0;
+      }
+      __syncthreads();
+      cta_mm16<false>(Y, T, W, lp, ld);
+      for (int e = tid; e < l * l; e += nt) ffn[e] = Y[(e / l) * ld + (e % l)];
+    }
+  }
+  if (tid == 0) {
+    const double norm = sqrt(norm2);
+    scal->norm = norm;
+    if (it1 >= 0 && it2 >= 0) scal->sweeps = it1 * 100 + it2;
     if (guard_stop && !(norm >= tol)) scal->stop_it = guard_it;
   }
 }
@@ -620,6 +869,19 @@ int launch_scale_cols_rsqrt(Context* c, int n, int batch, const double* V, const
 int launch_kn_step(Context* c, int l, const double* z, const double* dd, double inv_n, double* out, double* outn,
                    const double* ff, double* ffn, double* vwork, double tol) {
   if (l < 1 || l > MCNLA_B200_MAX_DIM_SKETCH) return MCNLA_B200_ERR_UNSUPPORTED;
+  if (l <= kKnNsMaxDim && c->kn_mode == 0) {
+    const int lp = (l + 15) & ~15;
+    const size_t smem = 4 * size_t(lp) * (lp + 4) * sizeof(double) + (64 + 96) * sizeof(double) +
+                        jacobi_scratch_bytes(l) + 64;
+    if (smem <= c->smem_optin) {
+      MB_CHECK(set_smem(reinterpret_cast<const void*>(k_kn_step_ns), smem));
+      k_kn_step_ns<<<1, kSmallThreads, smem, c->stream>>>(l, z, dd, inv_n, out, outn, ff, ffn, vwork, c->scal, tol,
+                                                          c->guard_stop, c->guard_it);
+      c->kernels_launched++;
+      MB_CHECK_CUDA(cudaGetLastError());
+      return MCNLA_B200_OK;
+    }
+  }
   const bool v_smem = small_smem_syev(l, true) + l * 8 + 64 <= c->smem_optin;
   const size_t smem = small_smem_syev(l, v_smem) + l * 8 + 64;
   if (smem > c->smem_optin) return MCNLA_B200_ERR_UNSUPPORTED;

@@ -73,6 +73,10 @@ class Context:
     def kernels_launched(self):
         return int(self.lib.mcnla_b200_kernels_launched(self.handle))
 
+    def set_kn_method(self, method):
+        """_lib.KN_AUTO (matrix functions, eigen fallback) or _lib.KN_EIGEN."""
+        _lib.check(self.lib.mcnla_b200_set_kn_method(self.handle, method), "set_kn_method")
+
     def close(self):
         if getattr(self, "handle", None):
             self.lib.mcnla_b200_destroy(self.handle)

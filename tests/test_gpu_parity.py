@@ -172,6 +172,30 @@ def test_kn_golden(cuda, golden, cls_name, oracle_name):
     assert np.abs(qb - qo).max() < TOL
 
 
+@pytest.mark.parametrize("cls_name", ["KolmogorovNagumoIntegrator", "RowBlockKolmogorovNagumoIntegrator",
+                                      "RowBlockGramianKolmogorovNagumoIntegrator"])
+def test_kn_step_methods_agree(cuda, golden, cls_name):
+    """The matrix-function KN step and the eigendecomposition step give the
+    same integrated basis and iteration count on the golden fixture."""
+    from mcnla_b200 import isvd, _lib
+    m, l, N = golden["m"], golden["l"], golden["N"]
+    prm = params(m, l, l, 0, N)
+    out = []
+    ctx = isvd.context()
+    try:
+        for method in (_lib.KN_AUTO, _lib.KN_EIGEN):
+            ctx.set_kn_method(method)
+            integ = getattr(isvd, cls_name)(prm, 256, 1e-4)
+            integ.initialize()
+            qbar = prm.createMatrixQbar()
+            integ(dev(golden["qs"], cuda), qbar)
+            out.append((integ.iteration(), host(qbar)))
+    finally:
+        ctx.set_kn_method(_lib.KN_AUTO)
+    assert out[0][0] == out[1][0] == 81
+    assert np.abs(out[0][1] - out[1][1]).max() < TOL
+
+
 @pytest.mark.parametrize("cls_name,oracle_name", [
     ("RowBlockWenYinIntegrator", "rb_wy"),
     ("RowBlockGramianWenYinIntegrator", "rb_gramian_wy"),
