@@ -206,6 +206,26 @@ MCNLA_B200_API int mcnla_b200_syev_batched(mcnla_b200_ctx* ctx, int n, int batch
  * n <= 2 * MCNLA_B200_MAX_DIM_SKETCH_WENYIN.                                 */
 MCNLA_B200_API int mcnla_b200_inverse_batched(mcnla_b200_ctx* ctx, int n, int batch, double* A);
 
+/* FP64 GEMM that allocates nothing (no counterpart in the reference; an
+ * addition of this library).  For callers that cannot call cudaMalloc: a
+ * plugin whose host framework owns the device memory pool, or a
+ * latency-critical loop that cannot take the implicit synchronization of an
+ * allocation.  Same operation and strides as mcnla_b200_dgemm, but it needs no
+ * context: it runs on `stream` (NULL: the default stream) on the current
+ * device, and keeps the split-K partial sums in a 16 MiB device array that
+ * the library defines (held on every GPU that loads the library until the
+ * process exits).  The first call on each device looks that array's address
+ * up (cudaGetSymbolAddress); make that first call before any stream capture.
+ * Shapes whose partial sums need more than MCNLA_B200_NOALLOC_SCRATCH_BYTES
+ * are rejected with MCNLA_B200_ERR_SHAPE (mcnla_b200_last_error names the
+ * size).  All calls on a device share the array: calls that overlap on the
+ * GPU (other streams, other host threads) race; serialize them.            */
+#define MCNLA_B200_NOALLOC_SCRATCH_BYTES (16u << 20)
+MCNLA_B200_API int mcnla_b200_dgemm_noalloc(void* stream, int64_t M, int64_t N, int64_t K, double alpha,
+                                            const double* A, int64_t a_rs, int64_t a_cs, const double* B,
+                                            int64_t b_rs, int64_t b_cs, double beta, double* C, int64_t c_rs,
+                                            int64_t c_cs);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif

@@ -79,6 +79,8 @@ SIGNATURES = {
     "mcnla_b200_dgemm": (_INT, [_P, _I64, _I64, _I64, _D, _P, _I64, _I64, _P, _I64, _I64, _D, _P, _I64, _I64, _INT]),
     "mcnla_b200_syev_batched": (_INT, [_P, _INT, _INT, _P, _P, _P, _INT]),
     "mcnla_b200_inverse_batched": (_INT, [_P, _INT, _INT, _P]),
+    "mcnla_b200_dgemm_noalloc": (_INT, [_P, _I64, _I64, _I64, _D, _P, _I64, _I64, _P, _I64, _I64, _D, _P, _I64,
+                                        _I64]),
 }
 
 
