@@ -12,7 +12,8 @@ LIB_PATH = os.path.join(HERE, "libmcnla_b200.so")
 HEADER_PATH = os.path.join(os.path.dirname(HERE), "include", "mcnla_b200.h")
 
 OK = 0
-ERR_SHAPE, ERR_LAYOUT, ERR_WORKSPACE, ERR_CUDA, ERR_NOMEM, ERR_ARG, ERR_UNSUPPORTED, ERR_SINGULAR = range(1, 9)
+ERR_SHAPE, ERR_LAYOUT, ERR_WORKSPACE, ERR_CUDA, ERR_NOMEM, ERR_ARG, ERR_UNSUPPORTED, ERR_SINGULAR, \
+    ERR_DEVICE_TIMEOUT = range(1, 10)
 
 ROW_MAJOR, COL_MAJOR = 0, 1
 
@@ -79,6 +80,12 @@ SIGNATURES = {
     "mcnla_b200_dgemm": (_INT, [_P, _I64, _I64, _I64, _D, _P, _I64, _I64, _P, _I64, _I64, _D, _P, _I64, _I64, _INT]),
     "mcnla_b200_syev_batched": (_INT, [_P, _INT, _INT, _P, _P, _P, _INT]),
     "mcnla_b200_inverse_batched": (_INT, [_P, _INT, _INT, _P]),
+    "mcnla_b200_split_bf16": (_INT, [_P, _P, _INT, _I64, _I64, _I64, _P, _P, _I64]),
+    "mcnla_b200_gaussian_bf16": (_INT, [_P, ctypes.c_uint64, _I64, _I64, _P, _I64, _P]),
+    "mcnla_b200_gemm_bf16": (_INT, [_P, _I64, _I64, _I64, _P, _P, _I64, _P, _I64, _P, _I64, _INT]),
+    "mcnla_b200_sketch_bf16": (_INT, [_P, ctypes.POINTER(Params), _P, _P, _I64, _P, _I64, _P]),
+    "mcnla_b200_isvd_mixed": (_INT, [_P, ctypes.POINTER(Params), _INT, _INT, _P, _INT, _I64, _P, _P, _I64,
+                                     ctypes.c_uint64, _INT, _D, _P, _P, _P, ctypes.POINTER(_INT)]),
     "mcnla_b200_dgemm_noalloc": (_INT, [_P, _I64, _I64, _I64, _D, _P, _I64, _I64, _P, _I64, _I64, _D, _P, _I64,
                                         _I64]),
 }

@@ -1,0 +1,27 @@
+// BF16 tensor-core products and the conversions feeding them (the
+// mixed-precision sketch).
+#pragma once
+#include "common.cuh"
+
+namespace mb {
+
+// D (M x N) = (A_hi + A_lo) * B', all BF16 K-major (row pitch in elements,
+// multiple of 8), FP32 accumulation on tcgen05; D is FP64 (out_fp64) or FP32
+// row-major with leading dimension ldd.  a_lo may be null (one part).
+// Device-side wait timeouts are reported in c->scal->status.
+int bf16_gemm(Context* c, int64_t M, int64_t N, int64_t K, const uint16_t* a_hi, const uint16_t* a_lo, int64_t lda,
+              const uint16_t* b, int64_t ldb, void* D, int64_t ldd, bool out_fp64);
+
+// hi := bf16(A), lo := bf16(A - hi) (lo may be null), written row-major (K
+// contiguous) with pitch ldo, from row-major (layout 0) or column-major
+// (layout 1) FP64 A.
+int launch_split_bf16(Context* c, const double* A, int layout, int64_t lda, int64_t m, int64_t n, uint16_t* hi,
+                      uint16_t* lo, int64_t ldo);
+
+// Omega' in BF16 (L x n, pitch ldo) from the same Philox stream as the FP64
+// generator (element (i, j) of the n x L Omega is sample i L + j), rounded to
+// BF16; omega (n x L FP64, optional) receives the same rounded values.
+int launch_gaussian_bf16(Context* c, uint64_t seed, int64_t n, int64_t L, uint16_t* omega_t, int64_t ldo,
+                         double* omega);
+
+}  // namespace mb

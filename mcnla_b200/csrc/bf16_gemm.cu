@@ -1,0 +1,312 @@
+// BF16 tensor-core GEMM on the 5th-generation tensor cores (tcgen05) for the
+// mixed-precision sketch:
+//
+//   D (M x N, FP64 or FP32, row-major) = sum_p A_p (M x K, BF16, K-major) * B (N x K, BF16, K-major)'
+//
+// with p over one or two parts of A (A = A_hi + A_lo, both BF16: 16 bits of
+// mantissa in total) and FP32 accumulation in tensor memory.
+//
+// One CTA computes a 128 x 256 tile of D: warp 0 (one lane) streams 128 x 64
+// and 256 x 64 BF16 tiles of A and B into a 4-stage shared-memory ring with
+// TMA (128-byte swizzle), warp 1 (one lane) issues tcgen05.mma (M=128, N=256,
+// K=16, four per stage) into a 256-column TMEM accumulator and releases each
+// stage with tcgen05.commit, and warps 4-7 read the accumulator back with
+// tcgen05.ld (one TMEM lane = one row per thread) and store D.  Every
+// mbarrier wait is bounded: when one runs out the kernel records the fact in
+// a device status word, lets the work already in flight drain (also with
+// bounded waits) and frees its TMEM before returning.
+#include "common.cuh"
+#include "bf16.cuh"
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_bf16.h>
+
+#include <mutex>
+
+namespace mb {
+namespace {
+
+constexpr int BM = 128, BN = 256, BK = 64, STAGES = 4;
+constexpr int A_TILE_BYTES = BM * BK * 2;                 // 16 KB
+constexpr int B_TILE_BYTES = BN * BK * 2;                 // 32 KB
+constexpr int STAGE_BYTES = A_TILE_BYTES + B_TILE_BYTES;  // 48 KB
+constexpr uint32_t TMEM_COLS = 256;
+constexpr int THREADS = 256;
+constexpr size_t SMEM_BYTES = size_t(STAGES) * STAGE_BYTES + 1024;   // + alignment slack
+constexpr long long kWaitCycles = 4000000000LL;           // ~2 s at 2 GHz: a bounded wait
+
+// instruction descriptor, kind::f16: D f32, A bf16, B bf16, both K-major, M=128, N=256
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(BN >> 3) << 17) |
+                            (uint32_t(BM >> 4) << 24);
+
+struct Args {
+  int M, N;
+  int KT;          // k-tiles per part of A
+  int parts;       // 1 (A_hi) or 2 (A_hi + A_lo)
+  void* D;
+  int64_t ldd;
+  int* status;     // device status word: set to MCNLA_B200_ERR_DEVICE_TIMEOUT on a run-out wait
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+// Waits for the phase of `bar` with the given parity to complete; false when
+// the wait ran out (about two seconds).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t addr = smem_u32(bar);
+  const long long t0 = clock64();
+  while (true) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (clock64() - t0 > kWaitCycles) return false;
+  }
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
+      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+
+// Shared-memory matrix descriptor of a K-major tile written by TMA with the
+// 128-byte swizzle: rows of 128 bytes, 8-row groups 1024 bytes apart.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= uint64_t((saddr & 0x3FFFFu) >> 4);        // start address, bits [0, 14)
+  d |= uint64_t(1) << 16;                         // leading byte offset (unused for swizzled K-major)
+  d |= uint64_t(1024 >> 4) << 32;                 // stride byte offset: 8 rows x 128 B
+  d |= uint64_t(1) << 46;                         // descriptor version (sm_100)
+  d |= uint64_t(2) << 61;                         // layout: 128-byte swizzle
+  return d;
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+      ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+template <class OutT>
+__global__ void __launch_bounds__(THREADS, 1) bf16_gemm_kernel(const __grid_constant__ CUtensorMap tm_a_hi,
+                                                               const __grid_constant__ CUtensorMap tm_a_lo,
+                                                               const __grid_constant__ CUtensorMap tm_b, Args g) {
+  extern __shared__ uint8_t smem_dyn[];
+  __shared__ __align__(8) uint64_t full_bar[STAGES];
+  __shared__ __align__(8) uint64_t empty_bar[STAGES];
+  __shared__ __align__(8) uint64_t accum_bar;
+  __shared__ uint32_t tmem_base_s;
+
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_dyn) + 1023) & ~uintptr_t(1023));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int n0 = blockIdx.x * BN, m0 = blockIdx.y * BM;
+  const int total_kt = g.KT * g.parts;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_s)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (threadIdx.x == 32) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    mbar_init(&accum_bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = tmem_base_s;
+
+  if (warp == 0 && lane == 0) {
+    // ---- producer: TMA into the ring
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tm_a_hi)) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tm_b)) : "memory");
+    int issued = 0;
+    bool ok = true;
+    for (int kt = 0; kt < total_kt; ++kt) {
+      const int s = kt % STAGES;
+      if (kt >= STAGES && !mbar_wait(&empty_bar[s], ((kt / STAGES) & 1) ^ 1)) { ok = false; break; }
+      uint8_t* sa = smem + s * STAGE_BYTES;
+      uint8_t* sb = sa + A_TILE_BYTES;
+      const int part = kt / g.KT, kk = kt % g.KT;
+      mbar_expect_tx(&full_bar[s], STAGE_BYTES);
+      tma_load_2d(sa, part ? &tm_a_lo : &tm_a_hi, &full_bar[s], kk * BK, m0);
+      tma_load_2d(sb, &tm_b, &full_bar[s], kk * BK, n0);
+      ++issued;
+    }
+    if (!ok) {
+      atomicExch(g.status, MCNLA_B200_ERR_DEVICE_TIMEOUT);
+      // let the copies in flight land before the CTA's shared memory goes away
+      for (int kt = issued > STAGES ? issued - STAGES : 0; kt < issued; ++kt)
+        mbar_wait(&full_bar[kt % STAGES], (kt / STAGES) & 1);
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---- MMA issuer
+    for (int kt = 0; kt < total_kt; ++kt) {
+      const int s = kt % STAGES;
+      if (!mbar_wait(&full_bar[s], (kt / STAGES) & 1)) { atomicExch(g.status, MCNLA_B200_ERR_DEVICE_TIMEOUT); break; }
+      fence_after();
+      const uint32_t sa = smem_u32(smem + s * STAGE_BYTES);
+      const uint32_t sb = sa + A_TILE_BYTES;
+#pragma unroll
+      for (int k = 0; k < BK / 16; ++k)   // 16 BF16 = 32 bytes along K per MMA
+        umma_bf16(tmem, sw128_desc(sa + k * 32), sw128_desc(sb + k * 32), (kt | k) != 0);
+      umma_commit(&empty_bar[s]);        // the stage is free once these MMAs have read it
+    }
+    umma_commit(&accum_bar);             // all MMAs issued so far are complete
+  } else if (warp >= 4) {
+    // ---- epilogue: TMEM -> registers -> global
+    const int ew = warp - 4;             // TMEM lanes [32 ew, 32 ew + 32)
+    const bool ok = mbar_wait(&accum_bar, 0);
+    fence_after();
+    if (!ok) {
+      if (lane == 0) atomicExch(g.status, MCNLA_B200_ERR_DEVICE_TIMEOUT);
+    } else {
+      const int row = m0 + ew * 32 + lane;
+      OutT* drow = static_cast<OutT*>(g.D) + int64_t(row) * g.ldd;
+#pragma unroll 1
+      for (int c = 0; c < BN / 32; ++c) {
+        uint32_t r[32];
+        tmem_ld32(tmem + (uint32_t(ew * 32) << 16) + uint32_t(c * 32), r);
+        const int col = n0 + c * 32;
+        if (row < g.M) {
+          if (col + 32 <= g.N) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) drow[col + j] = OutT(__uint_as_float(r[j]));
+          } else {
+            for (int j = 0; j < 32 && col + j < g.N; ++j) drow[col + j] = OutT(__uint_as_float(r[j]));
+          }
+        }
+      }
+    }
+  }
+  fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+  }
+}
+
+// ---- host: tensor maps through the driver entry point (no libcuda link)
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+std::mutex g_encode_mutex;
+
+int encode_fn(PFN_cuTensorMapEncodeTiled_v12000* out) {
+  std::lock_guard<std::mutex> lock(g_encode_mutex);
+  if (!g_encode) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    MB_CHECK_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+    if (q != cudaDriverEntryPointSuccess || !fn) {
+      set_last_message("cuTensorMapEncodeTiled is not available from the driver");
+      return MCNLA_B200_ERR_CUDA;
+    }
+    g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  *out = g_encode;
+  return MCNLA_B200_OK;
+}
+
+// 2-D BF16 K-major tensor: rows x cols (cols = K, contiguous), row pitch ld elements.
+int make_map(CUtensorMap* map, const void* base, int64_t rows, int64_t cols, int64_t ld, int box_rows) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc;
+  MB_CHECK(encode_fn(&enc));
+  cuuint64_t dims[2] = {cuuint64_t(cols), cuuint64_t(rows)};
+  cuuint64_t strides[1] = {cuuint64_t(ld) * 2};
+  cuuint32_t box[2] = {cuuint32_t(BK), cuuint32_t(box_rows)};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_last_message("cuTensorMapEncodeTiled failed with CUresult " + std::to_string(int(r)));
+    return MCNLA_B200_ERR_CUDA;
+  }
+  return MCNLA_B200_OK;
+}
+
+}  // namespace
+
+int bf16_gemm(Context* c, int64_t M, int64_t N, int64_t K, const uint16_t* a_hi, const uint16_t* a_lo, int64_t lda,
+              const uint16_t* b, int64_t ldb, void* D, int64_t ldd, bool out_fp64) {
+  if (M <= 0 || N <= 0 || K <= 0) return MCNLA_B200_ERR_SHAPE;
+  if (M > (int64_t(1) << 31) - 1 || N > (int64_t(1) << 31) - 1) return MCNLA_B200_ERR_SHAPE;
+  // TMA: 16-byte aligned bases and row pitches
+  auto al16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+  if (!al16(a_hi) || (a_lo && !al16(a_lo)) || !al16(b) || (lda * 2) % 16 || (ldb * 2) % 16)
+    return MCNLA_B200_ERR_LAYOUT;
+  if (lda < K || ldb < K) return MCNLA_B200_ERR_SHAPE;
+  CUtensorMap ta_hi, ta_lo, tb;
+  MB_CHECK(make_map(&ta_hi, a_hi, M, K, lda, BM));
+  MB_CHECK(make_map(&ta_lo, a_lo ? a_lo : a_hi, M, K, lda, BM));
+  MB_CHECK(make_map(&tb, b, N, K, ldb, BN));
+  Args g;
+  g.M = int(M);
+  g.N = int(N);
+  g.KT = int(cdiv(K, BK));
+  g.parts = a_lo ? 2 : 1;
+  g.D = D;
+  g.ldd = ldd;
+  g.status = &c->scal->status;
+  dim3 grid(unsigned(cdiv(N, BN)), unsigned(cdiv(M, BM)));
+  if (grid.y > 65535) return MCNLA_B200_ERR_SHAPE;
+  if (out_fp64) {
+    MB_CHECK_CUDA(cudaFuncSetAttribute(bf16_gemm_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(SMEM_BYTES)));
+    bf16_gemm_kernel<double><<<grid, THREADS, SMEM_BYTES, c->stream>>>(ta_hi, ta_lo, tb, g);
+  } else {
+    MB_CHECK_CUDA(cudaFuncSetAttribute(bf16_gemm_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(SMEM_BYTES)));
+    bf16_gemm_kernel<float><<<grid, THREADS, SMEM_BYTES, c->stream>>>(ta_hi, ta_lo, tb, g);
+  }
+  c->kernels_launched++;
+  MB_CHECK_CUDA(cudaGetLastError());
+  return MCNLA_B200_OK;
+}
+
+}  // namespace mb

@@ -11,6 +11,7 @@
 #include "common.cuh"
 #include "dgemm.cuh"
 #include "kernels.cuh"
+#include "bf16.cuh"
 #include <algorithm>
 #include <array>
 #include <cmath>
@@ -704,6 +705,39 @@ int run_isvd(Context* c, const Dims& d, int integrator, int former, const double
   return MCNLA_B200_OK;
 }
 
+// Mixed solve: Omega drawn in BF16, sketch on tcgen05, FP64 afterwards.
+int run_isvd_mixed(Context* c, const Dims& d, int integrator, int former, const double* A, int layout, int64_t lda,
+                   const uint16_t* a_hi, const uint16_t* a_lo, int64_t lda16, uint64_t seed, int maxit, double tol,
+                   double* S, double* U, double* V, int* iters, char* pbase) {
+  auto take = [&](size_t bytes) {
+    char* p = pbase;
+    pbase += (bytes + 511) & ~size_t(511);
+    return p;
+  };
+  const int64_t ldo = (d.n + 7) & ~int64_t(7);
+  double* Q = reinterpret_cast<double*>(take(size_t(d.m) * d.L * 8));
+  double* Qbar = reinterpret_cast<double*>(take(size_t(d.m) * d.l * 8));
+  uint16_t* omega_t = reinterpret_cast<uint16_t*>(take(size_t(d.L) * ldo * 2));
+  MB_CHECK_CUDA(cudaMemsetAsync(c->scal, 0, sizeof(DevScalars), c->stream));
+  MB_CHECK(ctx_tic(c));
+  MB_CHECK(launch_gaussian_bf16(c, seed, d.n, d.L, omega_t, ldo, nullptr));
+  MB_CHECK(ctx_toc(c));
+  MB_CHECK(bf16_gemm(c, d.m, d.L, d.n, a_hi, a_lo, lda16, omega_t, ldo, Q, d.L, true));
+  MB_CHECK(ctx_toc(c));
+  MB_CHECK(run_orthogonalize(c, d, Q));
+  MB_CHECK(run_integrate(c, d, integrator, Q, maxit, tol, Qbar, iters));
+  MB_CHECK(run_form(c, d, former, A, layout, lda, Qbar, S, U, V));
+  MB_CHECK(ctx_sync_scalars(c));
+  if (c->scal_host->status) return c->scal_host->status;
+  return MCNLA_B200_OK;
+}
+
+size_t pipeline_bytes_mixed(const Dims& d) {
+  const int64_t ldo = (d.n + 7) & ~int64_t(7);
+  auto r = [](size_t b) { return (b + 511) & ~size_t(511); };
+  return r(size_t(d.m) * d.L * 8) + r(size_t(d.m) * d.l * 8) + r(size_t(d.L) * ldo * 2);
+}
+
 size_t pipeline_bytes(const Dims& d) {
   return arena_bytes_for(size_t(d.m) * d.L, 8) + arena_bytes_for(size_t(d.m) * d.l, 8) +
          arena_bytes_for(size_t(d.n) * d.L, 8);
@@ -856,6 +890,61 @@ int mcnla_b200_inverse_batched(mcnla_b200_ctx* ctx, int n, int batch, double* A)
   MB_CHECK(mb::launch_inverse(ctx, n, batch, A));
   MB_CHECK(mb::ctx_sync_scalars(ctx));
   return ctx->scal_host->status ? ctx->scal_host->status : MCNLA_B200_OK;
+}
+
+int mcnla_b200_split_bf16(mcnla_b200_ctx* ctx, const double* A, int a_layout, int64_t lda, int64_t m, int64_t n,
+                          uint16_t* hi, uint16_t* lo, int64_t ldo) {
+  if (!ctx || !A || !hi || m < 0 || n < 0) return MCNLA_B200_ERR_ARG;
+  if (a_layout != MCNLA_B200_ROW_MAJOR && a_layout != MCNLA_B200_COL_MAJOR) return MCNLA_B200_ERR_ARG;
+  if (ldo < n || (a_layout == MCNLA_B200_ROW_MAJOR ? lda < n : lda < m)) return MCNLA_B200_ERR_SHAPE;
+  MB_CHECK_CUDA(cudaSetDevice(ctx->device));
+  return mb::launch_split_bf16(ctx, A, a_layout, lda, m, n, hi, lo, ldo);
+}
+
+int mcnla_b200_gaussian_bf16(mcnla_b200_ctx* ctx, uint64_t seed, int64_t n, int64_t L, uint16_t* omega_t,
+                             int64_t ldo, double* omega) {
+  if (!ctx || !omega_t || n < 0 || L < 0 || ldo < n) return MCNLA_B200_ERR_ARG;
+  MB_CHECK_CUDA(cudaSetDevice(ctx->device));
+  return mb::launch_gaussian_bf16(ctx, seed, n, L, omega_t, ldo, omega);
+}
+
+int mcnla_b200_gemm_bf16(mcnla_b200_ctx* ctx, int64_t M, int64_t N, int64_t K, const uint16_t* a_hi,
+                         const uint16_t* a_lo, int64_t lda, const uint16_t* b, int64_t ldb, void* D, int64_t ldd,
+                         int out_fp64) {
+  if (!ctx || !a_hi || !b || !D || ldd < N) return MCNLA_B200_ERR_ARG;
+  MB_CHECK_CUDA(cudaSetDevice(ctx->device));
+  MB_CHECK_CUDA(cudaMemsetAsync(ctx->scal, 0, sizeof(mb::DevScalars), ctx->stream));
+  MB_CHECK(mb::bf16_gemm(ctx, M, N, K, a_hi, a_lo, lda, b, ldb, D, ldd, out_fp64 != 0));
+  MB_CHECK(mb::ctx_sync_scalars(ctx));
+  return ctx->scal_host->status ? ctx->scal_host->status : MCNLA_B200_OK;
+}
+
+int mcnla_b200_sketch_bf16(mcnla_b200_ctx* ctx, const mcnla_b200_params* params, const uint16_t* a_hi,
+                           const uint16_t* a_lo, int64_t lda16, const uint16_t* omega_t, int64_t ldo, double* Q) {
+  if (!ctx || !a_hi || !omega_t || !Q) return MCNLA_B200_ERR_ARG;
+  Dims d;
+  MB_CHECK(mb::get_dims(params, d));
+  MB_CHECK_CUDA(cudaSetDevice(ctx->device));
+  MB_CHECK_CUDA(cudaMemsetAsync(ctx->scal, 0, sizeof(mb::DevScalars), ctx->stream));
+  MB_CHECK(mb::ctx_tic(ctx));
+  MB_CHECK(mb::ctx_toc(ctx));
+  MB_CHECK(mb::bf16_gemm(ctx, d.m, d.L, d.n, a_hi, a_lo, lda16, omega_t, ldo, Q, d.L, true));
+  MB_CHECK(mb::ctx_toc(ctx));
+  MB_CHECK(mb::ctx_sync_scalars(ctx));
+  return ctx->scal_host->status ? ctx->scal_host->status : MCNLA_B200_OK;
+}
+
+int mcnla_b200_isvd_mixed(mcnla_b200_ctx* ctx, const mcnla_b200_params* params, int integrator, int former,
+                          const double* A, int a_layout, int64_t lda, const uint16_t* a_hi, const uint16_t* a_lo,
+                          int64_t lda16, uint64_t seed, int max_iteration, double tolerance, double* S, double* U,
+                          double* V, int* iteration) {
+  if (!ctx || !A || !a_hi || !iteration) return MCNLA_B200_ERR_ARG;
+  Dims d;
+  MB_CHECK(mb::get_dims(params, d));
+  MB_CHECK_CUDA(cudaSetDevice(ctx->device));
+  MB_CHECK(mb::ctx_reserve_pipeline(ctx, mb::pipeline_bytes_mixed(d)));
+  return mb::run_isvd_mixed(ctx, d, integrator, former, A, a_layout, lda, a_hi, a_lo, lda16, seed, max_iteration,
+                            tolerance, S, U, V, iteration, static_cast<char*>(ctx->parena));
 }
 
 int mcnla_b200_syev_batched(mcnla_b200_ctx* ctx, int n, int batch, const double* A, double* W, double* V,

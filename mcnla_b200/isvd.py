@@ -34,7 +34,7 @@ __all__ = [
     "KolmogorovNagumoIntegrator", "RowBlockKolmogorovNagumoIntegrator", "RowBlockGramianKolmogorovNagumoIntegrator",
     "RowBlockWenYinIntegrator", "RowBlockGramianWenYinIntegrator",
     "SvdFormer", "GramianFormer", "RowBlockGramianFormer", "ColBlockGramianFormer",
-    "solve", "solve_host",
+    "solve", "solve_host", "split_bf16", "gaussian_bf16", "gemm_bf16", "solve_mixed",
 ]
 
 
@@ -612,4 +612,73 @@ def solve_host(a_host, omega_host, k, p, N, integrator="kn", former="svd", maxit
                                             _ptr(a_host), _lib.COL_MAJOR if colmajor else _lib.ROW_MAJOR,
                                             _ptr(omega_host), maxit, tol, _ptr(s), _ptr(u), _ptr(v),
                                             ctypes.byref(it)), "isvd_host")
+    return s, u, v, it.value
+
+
+# ----------------------------------------------------------------------------------------------
+# Mixed precision: BF16 tensor-core sketch (tcgen05), FP64 elsewhere
+# ----------------------------------------------------------------------------------------------
+def _bf16_buffer(rows, cols, dev):
+    """rows x cols BF16 with a row pitch that is a multiple of 8 elements (16 bytes)."""
+    ld = (cols + 7) // 8 * 8
+    buf = torch.zeros(rows, ld, dtype=torch.bfloat16, device=dev)
+    return buf[:, :cols], ld
+
+
+def split_bf16(a, with_lo=True):
+    """A = A_hi + A_lo in BF16 (row-major views with 16-byte pitch).  Returns (hi, lo, pitch)."""
+    _check_dev(a, "A")
+    layout, lda = _layout(a)
+    m, n = a.shape
+    hi, ld = _bf16_buffer(m, n, a.device)
+    lo = _bf16_buffer(m, n, a.device)[0] if with_lo else None
+    ctx = context(a.device)
+    _lib.check(ctx.lib.mcnla_b200_split_bf16(ctx.bind(), _ptr(a), layout, lda, m, n, _ptr(hi), _ptr(lo), ld),
+               "split_bf16")
+    return hi, lo, ld
+
+
+def gaussian_bf16(n, L, seed, device=None, with_fp64=False):
+    """Omega' (L x n BF16, pitch multiple of 8) and optionally the same values as an n x L FP64 Omega."""
+    dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+    omega_t, ld = _bf16_buffer(L, n, dev)
+    omega = torch.empty(n, L, dtype=torch.float64, device=dev) if with_fp64 else None
+    ctx = context(dev)
+    _lib.check(ctx.lib.mcnla_b200_gaussian_bf16(ctx.bind(), ctypes.c_uint64(seed), n, L, _ptr(omega_t), ld,
+                                                _ptr(omega)), "gaussian_bf16")
+    return omega_t, ld, omega
+
+
+def gemm_bf16(a_hi, a_lo, lda, b, ldb, out_dtype=torch.float64):
+    """D = (A_hi + A_lo) B' on tcgen05 (BF16 in, FP32 accumulation)."""
+    M, K = a_hi.shape
+    N = b.shape[0]
+    d = torch.empty(M, N, dtype=out_dtype, device=a_hi.device)
+    ctx = context(a_hi.device)
+    _lib.check(ctx.lib.mcnla_b200_gemm_bf16(ctx.bind(), M, N, K, _ptr(a_hi), _ptr(a_lo), lda, _ptr(b), ldb, _ptr(d),
+                                            N, 1 if out_dtype == torch.float64 else 0), "gemm_bf16")
+    return d
+
+
+def solve_mixed(a, k, p, N, seed=0, integrator="kn", former="svd", maxit=256, tol=1e-4, split=None, with_v=True,
+                with_lo=True):
+    """Whole iSVD with the BF16 tensor-core sketch (Omega drawn in BF16 from seed) and FP64
+    orthogonalizer / integrator / former.  `split` = (hi, lo, pitch) reuses a resident BF16 copy.
+    Returns (S, U, V, iterations)."""
+    m, n = a.shape
+    _check_dev(a, "A")
+    layout, lda = _layout(a)
+    if split is None:
+        split = split_bf16(a, with_lo)
+    hi, lo, ld16 = split
+    prm = _lib.Params(m, n, k, p, N)
+    dev = a.device
+    s = torch.empty(k, dtype=torch.float64, device=dev)
+    u = torch.empty(m, k, dtype=torch.float64, device=dev)
+    v = torch.empty(n, k, dtype=torch.float64, device=dev) if with_v else None
+    ctx = context(dev)
+    it = ctypes.c_int()
+    _lib.check(ctx.lib.mcnla_b200_isvd_mixed(ctx.bind(), ctypes.byref(prm), INTEGRATORS[integrator], FORMERS[former],
+                                             _ptr(a), layout, lda, _ptr(hi), _ptr(lo), ld16, ctypes.c_uint64(seed),
+                                             maxit, tol, _ptr(s), _ptr(u), _ptr(v), ctypes.byref(it)), "isvd_mixed")
     return s, u, v, it.value

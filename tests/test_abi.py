@@ -39,7 +39,7 @@ def test_binding_declares_every_symbol():
 def test_status_strings():
     lib = _lib.load()
     assert lib.mcnla_b200_status_string(0) == b"ok"
-    for st in range(1, 9):
+    for st in range(1, 10):
         assert lib.mcnla_b200_status_string(st) != b"unknown status"
     assert lib.mcnla_b200_status_string(99) == b"unknown status"
 
