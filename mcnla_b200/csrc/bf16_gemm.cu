@@ -202,7 +202,8 @@ __global__ void __launch_bounds__(THREADS, 1) bf16_gemm_kernel(const __grid_cons
   } else if (warp >= 4) {
     // ---- epilogue: TMEM -> registers -> global
     const int ew = warp - 4;             // TMEM lanes [32 ew, 32 ew + 32)
-    const bool ok = mbar_wait(&accum_bar, 0);
+    // warp-uniform outcome: the TMEM loads below are .sync.aligned
+    const bool ok = __all_sync(0xffffffffu, mbar_wait(&accum_bar, 0));
     fence_after();
     if (!ok) {
       if (lane == 0) atomicExch(g.status, MCNLA_B200_ERR_DEVICE_TIMEOUT);
@@ -228,6 +229,7 @@ __global__ void __launch_bounds__(THREADS, 1) bf16_gemm_kernel(const __grid_cons
   fence_before();
   __syncthreads();
   if (warp == 0) {
+    __syncwarp();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
   }
 }
