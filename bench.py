@@ -58,6 +58,7 @@ def parse():
     ap.add_argument("--colmajor", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--cpu-rows", type=int, default=0, help="row sample of the CPU baseline (0: auto)")
     ap.add_argument("--quick", action="store_true", help="small shape for a smoke run")
     args = ap.parse_args()
@@ -170,6 +171,14 @@ class ClockSampler:
 # ------------------------------------------------------------------------------------------------
 # this build
 # ------------------------------------------------------------------------------------------------
+def _measured_peak(key):
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)[key])
+    except Exception:
+        return {"bf16_tflops": 1590.0, "hbm_gbs": 6650.0}.get(key)
+
+
 def fp64_peak_tflops():
     """cuBLAS DGEMM throughput on this GPU (the FP64 roofline denominator; no FP64
     figure is in the measured-peaks file).  Best of 5 at 8192^3, after warm-up."""
@@ -293,6 +302,66 @@ def run_b200(args, world, rank, local):
     traffic = None
     if SKETCH_TRAFFIC_PER_ROW is not None:
         traffic = SKETCH_TRAFFIC_PER_ROW * m
+    # ---- mixed precision: BF16 (hi + lo) tcgen05 sketch, FP64 elsewhere; A kept resident as BF16 parts
+    mixed = None
+    if not args.no_mixed:
+        torch.cuda.synchronize()
+        e_s0, e_s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e_s0.record(stream)
+        split = isvd.split_bf16(a, True)
+        e_s1.record(stream)
+        torch.cuda.synchronize()
+        split_s = e_s0.elapsed_time(e_s1) / 1e3
+
+        def mixed_solve(seed):
+            return isvd.solve_mixed(a, k, p, N, seed=seed, integrator=args.integrator, former=args.former,
+                                    maxit=args.maxit, tol=args.tol, split=split)
+        for w in range(max(args.warmup, 1)):
+            mixed_solve(w)
+        torch.cuda.synchronize()
+        barrier(world)
+        m0e, m1e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        m0e.record(stream)
+        for step in range(args.steps):
+            sm_, um_, vm_, itm_ = mixed_solve(100 + step)
+        m1e.record(stream)
+        torch.cuda.synchronize()
+        t_mixed = max_over_ranks(m0e.elapsed_time(m1e) / 1e3, world)
+        # sketch kernel alone (tcgen05 BF16 x 2 parts) for its roofline
+        om_t, ldo, om64 = isvd.gaussian_bf16(n, L, 77, dev, with_fp64=True)
+        prm_c = _lib.Params(m, n, k, p, N)
+        qb = torch.empty(m, L, dtype=torch.float64, device=dev)
+        sk_t = []
+        for _ in range(3):
+            _lib.check(ctx.lib.mcnla_b200_sketch_bf16(ctx.bind(), ctypes.byref(prm_c), isvd._ptr(split[0]),
+                                                      isvd._ptr(split[1]), split[2], isvd._ptr(om_t), ldo,
+                                                      isvd._ptr(qb)), "sketch_bf16")
+            sk_t.append(ctx.last_times()[1])
+        sk_bf16 = sum(sk_t) / len(sk_t)
+        # accuracy of the mixed solve against the FP64 solve on the same A and Omega
+        s64, u64, v64, it64 = isvd.solve(a, k, p, N, omega=om64, integrator=args.integrator, former=args.former,
+                                         maxit=args.maxit, tol=args.tol)
+        smx, umx, vmx, itmx = isvd.solve_mixed(a, k, p, N, seed=77, integrator=args.integrator,
+                                               former=args.former, maxit=args.maxit, tol=args.tol, split=split)
+        rel = ((smx - s64).abs() / s64).max().item()
+        ang = float(torch.arccos(torch.clamp(torch.linalg.svdvals(u64.t() @ umx).min(), -1, 1)).item())
+        orth = float(torch.linalg.norm(umx.t() @ umx - torch.eye(k, dtype=torch.float64, device=dev)).item())
+        bf16_peak = _measured_peak("bf16_tflops")
+        ach = 2.0 * 2.0 * m * n * L / sk_bf16 / 1e12
+        mixed = {"value": round(world * args.steps / t_mixed, 5), "unit": "iSVD/s",
+                 "ms_per_step": round(t_mixed / args.steps * 1e3, 3),
+                 "speedup_vs_fp64": round((world * args.steps / t_mixed) / value, 3),
+                 "sketch": "A = A_hi + A_lo (BF16), Omega BF16, tcgen05 FP32 accumulation, FP64 out",
+                 "split_s": round(split_s, 5), "sketch_gemm_s": round(sk_bf16, 5),
+                 "sketch_roofline": {"bound": "tensor", "achieved": round(ach, 2),
+                                     "peak": bf16_peak, "unit": "TFLOP/s",
+                                     "frac": round(ach / bf16_peak, 4) if bf16_peak else None,
+                                     "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst) of measured",
+                                     "algorithmic": "2 parts x 2 m n N l flops"},
+                 "accuracy_vs_fp64_same_A_Omega": {"sigma_rel_err": rel, "max_principal_angle_U": ang,
+                                                   "UtU_minus_I_fro": orth, "iterations": [itmx, it64]}}
+        del split, qb, om_t, om64
+
     roofline = {"bound": "tensor", "kernel": "dgemm_kernel (sketch Y = A Omega, FP64 DMMA)",
                 "achieved": round(achieved, 3), "peak": round(peak64, 3), "unit": "TFLOP/s",
                 "frac": round(achieved / peak64, 4), "traffic": traffic,
@@ -338,7 +407,8 @@ def run_b200(args, world, rank, local):
         "a_read_gbs": round(2 * m * n * 8 * world * args.steps / total / 1e9, 2),
         "p50_ms": round(step_ms[len(step_ms) // 2], 3),
         "p99_ms": round(step_ms[min(len(step_ms) - 1, int(0.99 * len(step_ms)))], 3),
-        "iterations": iters[-1], "stages": stages, "integrators": variants, "roofline": roofline, "e2e": e2e,
+        "iterations": iters[-1], "stages": stages, "integrators": variants, "mixed": mixed, "roofline": roofline,
+        "e2e": e2e,
         "gpu_launches": int(launches), "clocks": clk,
     }
     return result
