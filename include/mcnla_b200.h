@@ -219,6 +219,58 @@ MCNLA_B200_API int mcnla_b200_isvd_mixed(mcnla_b200_ctx* ctx, const mcnla_b200_p
                                          const uint16_t* a_lo, int64_t lda16, uint64_t seed, int max_iteration,
                                          double tolerance, double* S, double* U, double* V, int* iteration);
 
+/* ---- batched and served solves ----------------------------------------------
+ * Many independent solves of uneven sizes share the GPU: a pool of workers,
+ * each with its own stream and workspaces, takes problems from a FIFO queue
+ * and runs them concurrently, so small problems fill the SMs together.  A
+ * problem is admitted when a worker is free and the estimated device bytes of
+ * the problems in flight stay within the budget (A itself is the caller's and
+ * is not counted).  Every solve is deterministic, so a problem gives the same
+ * result alone and in a mix.  (The reference runs one problem per MPI job;
+ * this has no counterpart there.)                                            */
+#define MCNLA_B200_PRECISION_FP64  0   /* FP64 sketch (plain path) */
+#define MCNLA_B200_PRECISION_MIXED 1   /* BF16 hi+lo tcgen05 sketch, FP64 elsewhere */
+
+typedef struct mcnla_b200_problem {
+  mcnla_b200_params params;
+  const double* A;        /* device, FP64; or NULL when A32 is given */
+  const float* A32;       /* device, FP32 (converted on the worker's stream) */
+  int a_layout;
+  int64_t lda;
+  uint64_t seed;          /* Omega is drawn on the device from this seed */
+  int integrator, former, max_iteration;
+  double tolerance;
+  int precision;          /* MCNLA_B200_PRECISION_* */
+  double* S;              /* device outputs: k, m x k, n x k (U, V may be NULL) */
+  double* U;
+  double* V;
+  int iteration;          /* out */
+  int status;             /* out */
+  double seconds;         /* out: device time of the solve */
+} mcnla_b200_problem;
+
+typedef struct mcnla_b200_server mcnla_b200_server;
+
+/* Device bytes a problem needs while in flight (workspaces and sketches).   */
+MCNLA_B200_API int64_t mcnla_b200_problem_bytes(const mcnla_b200_problem* problem);
+MCNLA_B200_API int mcnla_b200_server_create(mcnla_b200_server** server, int device, int workers,
+                                            int64_t budget_bytes);
+/* Queues a copy of *problem; returns at once with a ticket.                  */
+MCNLA_B200_API int mcnla_b200_server_submit(mcnla_b200_server* server, const mcnla_b200_problem* problem,
+                                            int64_t* ticket);
+/* Blocks until the ticket's problem is done and copies it (with iteration,
+ * status and seconds filled) to *out.  Each ticket can be waited on once.   */
+MCNLA_B200_API int mcnla_b200_server_wait(mcnla_b200_server* server, int64_t ticket, mcnla_b200_problem* out);
+/* Bytes admitted right now and the most ever admitted at once.              */
+MCNLA_B200_API int mcnla_b200_server_stats(mcnla_b200_server* server, int64_t* in_flight_bytes, int64_t* peak_bytes,
+                                           int64_t* completed);
+/* Finishes the queued work, stops the workers and frees everything.        */
+MCNLA_B200_API int mcnla_b200_server_destroy(mcnla_b200_server* server);
+/* All problems through a temporary server; returns the first non-zero status
+ * (each problem's own status is in problems[i].status).                      */
+MCNLA_B200_API int mcnla_b200_isvd_batched(int device, mcnla_b200_problem* problems, int count, int workers,
+                                           int64_t budget_bytes);
+
 /* ---- building blocks (exposed for tests) ----------------------------------
  * FP64 GEMM C := alpha*A*B + beta*C on strided device matrices (element (i,j)
  * of X at X[i*x_rs + j*x_cs]); the reference's la::mm

@@ -40,6 +40,18 @@ class Params(ctypes.Structure):
                 ("over_rank", ctypes.c_int64), ("num_sketch", ctypes.c_int64)]
 
 
+PRECISION_FP64, PRECISION_MIXED = 0, 1
+
+
+class Problem(ctypes.Structure):
+    """mirror of ``mcnla_b200_problem``"""
+    _fields_ = [("params", Params), ("A", ctypes.c_void_p), ("A32", ctypes.c_void_p), ("a_layout", ctypes.c_int),
+                ("lda", ctypes.c_int64), ("seed", ctypes.c_uint64), ("integrator", ctypes.c_int),
+                ("former", ctypes.c_int), ("max_iteration", ctypes.c_int), ("tolerance", ctypes.c_double),
+                ("precision", ctypes.c_int), ("S", ctypes.c_void_p), ("U", ctypes.c_void_p), ("V", ctypes.c_void_p),
+                ("iteration", ctypes.c_int), ("status", ctypes.c_int), ("seconds", ctypes.c_double)]
+
+
 class McnlaError(RuntimeError):
     def __init__(self, status, what, detail=""):
         self.status = status
@@ -86,6 +98,13 @@ SIGNATURES = {
     "mcnla_b200_sketch_bf16": (_INT, [_P, ctypes.POINTER(Params), _P, _P, _I64, _P, _I64, _P]),
     "mcnla_b200_isvd_mixed": (_INT, [_P, ctypes.POINTER(Params), _INT, _INT, _P, _INT, _I64, _P, _P, _I64,
                                      ctypes.c_uint64, _INT, _D, _P, _P, _P, ctypes.POINTER(_INT)]),
+    "mcnla_b200_problem_bytes": (_I64, [ctypes.POINTER(Problem)]),
+    "mcnla_b200_server_create": (_INT, [ctypes.POINTER(_P), _INT, _INT, _I64]),
+    "mcnla_b200_server_submit": (_INT, [_P, ctypes.POINTER(Problem), ctypes.POINTER(_I64)]),
+    "mcnla_b200_server_wait": (_INT, [_P, _I64, ctypes.POINTER(Problem)]),
+    "mcnla_b200_server_stats": (_INT, [_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64), ctypes.POINTER(_I64)]),
+    "mcnla_b200_server_destroy": (_INT, [_P]),
+    "mcnla_b200_isvd_batched": (_INT, [_INT, ctypes.POINTER(Problem), _INT, _INT, _I64]),
     "mcnla_b200_dgemm_noalloc": (_INT, [_P, _I64, _I64, _I64, _D, _P, _I64, _I64, _P, _I64, _I64, _D, _P, _I64,
                                         _I64]),
 }

@@ -1,0 +1,273 @@
+// Batched and served solves: a pool of host workers, each owning a context
+// (its own stream and workspaces), takes problems from a FIFO queue and runs
+// whole solves concurrently on the device.  Admission: the queue head is
+// started when a worker is free and the estimated bytes of the problems in
+// flight, plus its own, stay within the budget (a problem larger than the
+// budget runs alone).  Results do not depend on what else is in flight:
+// every kernel reduces in a fixed order.
+#include "common.cuh"
+
+#include <algorithm>
+#include <atomic>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+namespace mb {
+namespace {
+
+__global__ void k_f32_to_f64(const float* src, int64_t rows, int64_t cols, int64_t lds, double* dst, int64_t ldd) {
+  const int64_t total = rows * cols;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t r = e / cols, c = e % cols;
+    dst[r * ldd + c] = double(src[r * lds + c]);
+  }
+}
+
+struct Job {
+  mcnla_b200_problem p;
+  int64_t bytes = 0;
+  bool done = false;
+};
+
+int64_t round8(int64_t x) { return (x + 7) & ~int64_t(7); }
+
+}  // namespace
+
+int64_t problem_bytes(const mcnla_b200_problem& p) {
+  const int64_t m = p.params.nrow, n = p.params.ncol, l = p.params.rank + p.params.over_rank;
+  const int64_t L = l * p.params.num_sketch;
+  int64_t bytes = (m * L + m * l + n * L) * 8;                                  // Q, Qbar, Omega
+  int64_t stage = m * L * 8 + 5 * l * l * p.params.num_sketch * 8;              // orthogonalizer
+  stage = std::max(stage, L * L * 8 + 8 * L * 3 * l * 8 + 4 * m * 2 * l * 8);   // integrators
+  stage = std::max(stage, 4 * l * n * 8 + n * l * 8);                           // formers
+  bytes += stage + (int64_t(64) << 20);                                         // + split-K partials, small terms
+  if (!p.A && p.A32) bytes += m * n * 8;                                        // FP64 copy of an FP32 A
+  if (p.precision == MCNLA_B200_PRECISION_MIXED) bytes += 2 * m * round8(n) * 2 + L * round8(n) * 2;
+  return bytes;
+}
+
+}  // namespace mb
+
+struct mcnla_b200_server {
+  int device = 0;
+  int64_t budget = 0;
+  std::vector<std::thread> threads;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<int64_t> queue;
+  std::unordered_map<int64_t, mb::Job> jobs;
+  int64_t next_ticket = 1, in_flight = 0, peak = 0, completed = 0;
+  int running = 0;
+  bool stop = false;
+  std::atomic<int> init_failures{0};
+
+  void worker();
+  int run(mcnla_b200_ctx* ctx, mcnla_b200_problem& p, double*& a64, size_t& a64_bytes, uint16_t*& split,
+          size_t& split_bytes);
+};
+
+int mcnla_b200_server::run(mcnla_b200_ctx* ctx, mcnla_b200_problem& p, double*& a64, size_t& a64_bytes,
+                           uint16_t*& split, size_t& split_bytes) {
+  const int64_t m = p.params.nrow, n = p.params.ncol;
+  if (m <= 0 || n <= 0) return MCNLA_B200_ERR_SHAPE;
+  const double* A = p.A;
+  int layout = p.a_layout;
+  int64_t lda = p.lda;
+  if (!A) {
+    if (!p.A32) return MCNLA_B200_ERR_ARG;
+    const size_t need = size_t(m) * n * sizeof(double);
+    if (need > a64_bytes) {
+      if (a64) MB_CHECK_CUDA(cudaFreeAsync(a64, ctx->stream));
+      a64 = nullptr;
+      a64_bytes = 0;
+      MB_CHECK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&a64), need, ctx->stream));
+      a64_bytes = need;
+    }
+    const int64_t rows = layout == MCNLA_B200_ROW_MAJOR ? m : n, cols = layout == MCNLA_B200_ROW_MAJOR ? n : m;
+    const int blocks = int(std::min<int64_t>(mb::cdiv(rows * cols, 256), int64_t(ctx->num_sms) * 16));
+    mb::k_f32_to_f64<<<blocks, 256, 0, ctx->stream>>>(p.A32, rows, cols, lda, a64, cols);
+    MB_CHECK_CUDA(cudaGetLastError());
+    A = a64;
+    lda = cols;
+  }
+  if (p.precision == MCNLA_B200_PRECISION_MIXED) {
+    const int64_t ldo = (n + 7) & ~int64_t(7);
+    const size_t need = 2 * size_t(m) * ldo * sizeof(uint16_t);
+    if (need > split_bytes) {
+      if (split) MB_CHECK_CUDA(cudaFreeAsync(split, ctx->stream));
+      split = nullptr;
+      split_bytes = 0;
+      MB_CHECK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&split), need, ctx->stream));
+      split_bytes = need;
+    }
+    uint16_t* hi = split;
+    uint16_t* lo = split + size_t(m) * ldo;
+    MB_CHECK(mcnla_b200_split_bf16(ctx, A, layout, lda, m, n, hi, lo, ldo));
+    return mcnla_b200_isvd_mixed(ctx, &p.params, p.integrator, p.former, A, layout, lda, hi, lo, ldo, p.seed,
+                                 p.max_iteration, p.tolerance, p.S, p.U, p.V, &p.iteration);
+  }
+  return mcnla_b200_isvd(ctx, &p.params, p.integrator, p.former, A, layout, lda, nullptr, p.seed, p.max_iteration,
+                         p.tolerance, p.S, p.U, p.V, &p.iteration);
+}
+
+void mcnla_b200_server::worker() {
+  cudaSetDevice(device);
+  cudaStream_t stream = nullptr;
+  mcnla_b200_ctx* ctx = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  bool ok = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) == cudaSuccess &&
+            mcnla_b200_create(&ctx, device, stream) == MCNLA_B200_OK && cudaEventCreate(&e0) == cudaSuccess &&
+            cudaEventCreate(&e1) == cudaSuccess;
+  if (!ok) init_failures++;
+  double* a64 = nullptr;
+  size_t a64_bytes = 0;
+  uint16_t* split = nullptr;
+  size_t split_bytes = 0;
+  while (true) {
+    int64_t ticket = 0;
+    mcnla_b200_problem p;
+    int64_t bytes = 0;
+    {
+      std::unique_lock<std::mutex> lock(mu);
+      cv_work.wait(lock, [&] {
+        if (queue.empty()) return stop;
+        const int64_t b = jobs[queue.front()].bytes;
+        return running == 0 || in_flight + b <= budget;
+      });
+      if (queue.empty()) break;
+      ticket = queue.front();
+      queue.pop_front();
+      p = jobs[ticket].p;
+      bytes = jobs[ticket].bytes;
+      in_flight += bytes;
+      running++;
+      peak = std::max(peak, in_flight);
+    }
+    int st = MCNLA_B200_ERR_CUDA;
+    float ms = 0.f;
+    if (ok) {
+      cudaEventRecord(e0, stream);
+      st = run(ctx, p, a64, a64_bytes, split, split_bytes);
+      cudaEventRecord(e1, stream);
+      if (cudaStreamSynchronize(stream) != cudaSuccess && st == MCNLA_B200_OK) st = MCNLA_B200_ERR_CUDA;
+      cudaEventElapsedTime(&ms, e0, e1);
+    }
+    p.status = st;
+    p.seconds = ms * 1e-3;
+    {
+      std::lock_guard<std::mutex> lock(mu);
+      mb::Job& j = jobs[ticket];
+      j.p = p;
+      j.done = true;
+      in_flight -= bytes;
+      running--;
+      completed++;
+    }
+    cv_done.notify_all();
+    cv_work.notify_all();
+  }
+  if (a64) cudaFreeAsync(a64, stream);
+  if (split) cudaFreeAsync(split, stream);
+  if (stream) cudaStreamSynchronize(stream);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (ctx) mcnla_b200_destroy(ctx);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+extern "C" {
+
+int64_t mcnla_b200_problem_bytes(const mcnla_b200_problem* p) { return p ? mb::problem_bytes(*p) : -1; }
+
+int mcnla_b200_server_create(mcnla_b200_server** out, int device, int workers, int64_t budget_bytes) {
+  if (!out || workers < 1 || workers > 256 || budget_bytes <= 0) return MCNLA_B200_ERR_ARG;
+  *out = nullptr;
+  MB_CHECK_CUDA(cudaSetDevice(device));
+  auto* s = new mcnla_b200_server();
+  s->device = device;
+  s->budget = budget_bytes;
+  for (int i = 0; i < workers; ++i) s->threads.emplace_back([s] { s->worker(); });
+  *out = s;
+  return MCNLA_B200_OK;
+}
+
+int mcnla_b200_server_submit(mcnla_b200_server* s, const mcnla_b200_problem* problem, int64_t* ticket) {
+  if (!s || !problem || !ticket) return MCNLA_B200_ERR_ARG;
+  {
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (s->stop) return MCNLA_B200_ERR_ARG;
+    const int64_t t = s->next_ticket++;
+    mb::Job j;
+    j.p = *problem;
+    j.p.iteration = 0;
+    j.p.status = -1;
+    j.p.seconds = 0;
+    j.bytes = mb::problem_bytes(*problem);
+    s->jobs.emplace(t, j);
+    s->queue.push_back(t);
+    *ticket = t;
+  }
+  s->cv_work.notify_all();
+  return MCNLA_B200_OK;
+}
+
+int mcnla_b200_server_wait(mcnla_b200_server* s, int64_t ticket, mcnla_b200_problem* out) {
+  if (!s) return MCNLA_B200_ERR_ARG;
+  std::unique_lock<std::mutex> lock(s->mu);
+  auto it = s->jobs.find(ticket);
+  if (it == s->jobs.end()) return MCNLA_B200_ERR_ARG;
+  s->cv_done.wait(lock, [&] { return s->jobs[ticket].done; });
+  if (out) *out = s->jobs[ticket].p;
+  const int st = s->jobs[ticket].p.status;
+  s->jobs.erase(ticket);
+  return st;
+}
+
+int mcnla_b200_server_stats(mcnla_b200_server* s, int64_t* in_flight, int64_t* peak, int64_t* completed) {
+  if (!s) return MCNLA_B200_ERR_ARG;
+  std::lock_guard<std::mutex> lock(s->mu);
+  if (in_flight) *in_flight = s->in_flight;
+  if (peak) *peak = s->peak;
+  if (completed) *completed = s->completed;
+  return s->init_failures.load() ? MCNLA_B200_ERR_CUDA : MCNLA_B200_OK;
+}
+
+int mcnla_b200_server_destroy(mcnla_b200_server* s) {
+  if (!s) return MCNLA_B200_OK;
+  {
+    std::lock_guard<std::mutex> lock(s->mu);
+    s->stop = true;
+  }
+  s->cv_work.notify_all();
+  for (auto& t : s->threads) t.join();
+  delete s;
+  return MCNLA_B200_OK;
+}
+
+int mcnla_b200_isvd_batched(int device, mcnla_b200_problem* problems, int count, int workers, int64_t budget_bytes) {
+  if (count < 0 || (count > 0 && !problems)) return MCNLA_B200_ERR_ARG;
+  mcnla_b200_server* s = nullptr;
+  MB_CHECK(mcnla_b200_server_create(&s, device, workers, budget_bytes));
+  std::vector<int64_t> tickets(static_cast<size_t>(count));
+  int first = MCNLA_B200_OK;
+  for (int i = 0; i < count; ++i) {
+    const int st = mcnla_b200_server_submit(s, &problems[i], &tickets[size_t(i)]);
+    if (st != MCNLA_B200_OK) { first = st; tickets[size_t(i)] = 0; }
+  }
+  for (int i = 0; i < count; ++i) {
+    if (!tickets[size_t(i)]) continue;
+    const int st = mcnla_b200_server_wait(s, tickets[size_t(i)], &problems[i]);
+    if (st != MCNLA_B200_OK && first == MCNLA_B200_OK) first = st;
+  }
+  int64_t inflight = 0, peak = 0, done = 0;
+  const int sst = mcnla_b200_server_stats(s, &inflight, &peak, &done);
+  mcnla_b200_server_destroy(s);
+  if (first == MCNLA_B200_OK && sst != MCNLA_B200_OK) first = sst;
+  return first;
+}
+
+}  // extern "C"

@@ -35,6 +35,7 @@ __all__ = [
     "RowBlockWenYinIntegrator", "RowBlockGramianWenYinIntegrator",
     "SvdFormer", "GramianFormer", "RowBlockGramianFormer", "ColBlockGramianFormer",
     "solve", "solve_host", "split_bf16", "gaussian_bf16", "gemm_bf16", "solve_mixed",
+    "Request", "Server", "solve_batched",
 ]
 
 
@@ -682,3 +683,107 @@ def solve_mixed(a, k, p, N, seed=0, integrator="kn", former="svd", maxit=256, to
                                              _ptr(a), layout, lda, _ptr(hi), _ptr(lo), ld16, ctypes.c_uint64(seed),
                                              maxit, tol, _ptr(s), _ptr(u), _ptr(v), ctypes.byref(it)), "isvd_mixed")
     return s, u, v, it.value
+
+
+# ----------------------------------------------------------------------------------------------
+# Batched and served solves (mcnla_b200_server_*)
+# ----------------------------------------------------------------------------------------------
+class Request:
+    """One solve for the server: A (CUDA float64 or float32, row- or column-major) and its
+    parameters; the outputs S, U, V are allocated here on A's device."""
+
+    def __init__(self, a, k, p, N, seed=0, integrator="kn", former="svd", maxit=256, tol=1e-4, mixed=False,
+                 with_v=True):
+        if not isinstance(a, torch.Tensor) or not a.is_cuda or a.dtype not in (torch.float64, torch.float32):
+            raise TypeError("A must be a CUDA float64 or float32 tensor")
+        layout, lda = _layout(a)
+        m, n = a.shape
+        dev = a.device
+        self.a = a
+        self.s = torch.empty(k, dtype=torch.float64, device=dev)
+        self.u = torch.empty(m, k, dtype=torch.float64, device=dev)
+        self.v = torch.empty(n, k, dtype=torch.float64, device=dev) if with_v else None
+        pr = _lib.Problem()
+        pr.params = _lib.Params(m, n, k, p, N)
+        pr.A = a.data_ptr() if a.dtype == torch.float64 else None
+        pr.A32 = a.data_ptr() if a.dtype == torch.float32 else None
+        pr.a_layout = layout
+        pr.lda = lda
+        pr.seed = seed
+        pr.integrator = INTEGRATORS[integrator]
+        pr.former = FORMERS[former]
+        pr.max_iteration = maxit
+        pr.tolerance = tol
+        pr.precision = _lib.PRECISION_MIXED if mixed else _lib.PRECISION_FP64
+        pr.S = self.s.data_ptr()
+        pr.U = self.u.data_ptr()
+        pr.V = self.v.data_ptr() if self.v is not None else None
+        self.problem = pr
+        self.ticket = None
+        self.result = None
+
+    def bytes(self):
+        return int(_lib.load().mcnla_b200_problem_bytes(ctypes.byref(self.problem)))
+
+
+class Server:
+    """A pool of `workers` concurrent solvers on one device with an HBM admission budget."""
+
+    def __init__(self, workers=4, budget_bytes=150 << 30, device=None):
+        self.lib = _lib.load()
+        dev = torch.cuda.current_device() if device is None else torch.device(device).index
+        torch.cuda.synchronize(dev)
+        h = ctypes.c_void_p()
+        _lib.check(self.lib.mcnla_b200_server_create(ctypes.byref(h), dev, workers, budget_bytes), "server_create")
+        self.handle = h
+
+    def submit(self, req):
+        t = ctypes.c_int64()
+        _lib.check(self.lib.mcnla_b200_server_submit(self.handle, ctypes.byref(req.problem), ctypes.byref(t)),
+                   "server_submit")
+        req.ticket = t.value
+        return req
+
+    def wait(self, req):
+        out = _lib.Problem()
+        st = self.lib.mcnla_b200_server_wait(self.handle, req.ticket, ctypes.byref(out))
+        req.result = out
+        _lib.check(st, "server_wait")
+        return req
+
+    def stats(self):
+        a, b, c = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        _lib.check(self.lib.mcnla_b200_server_stats(self.handle, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)),
+                   "server_stats")
+        return {"in_flight_bytes": a.value, "peak_bytes": b.value, "completed": c.value}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.mcnla_b200_server_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def solve_batched(requests, workers=4, budget_bytes=150 << 30):
+    """All requests through one temporary pool (mcnla_b200_isvd_batched)."""
+    if not requests:
+        return requests
+    torch.cuda.synchronize()
+    arr = (_lib.Problem * len(requests))(*[r.problem for r in requests])
+    dev = requests[0].a.device.index
+    st = _lib.load().mcnla_b200_isvd_batched(dev, arr, len(requests), workers, budget_bytes)
+    for r, out in zip(requests, arr):
+        r.result = out
+    _lib.check(st, "isvd_batched")
+    return requests

@@ -59,7 +59,7 @@ def test_gaussian_bf16_matches_fp64_stream(cuda):
     # BF16-representable and within half a BF16 ulp of the FP64 stream
     # (round to nearest from FP64; torch's own cast may round twice via FP32)
     assert torch.equal(om.to(torch.bfloat16).double(), om)
-    assert bool(torch.all((om - ref).abs() <= 2.0 ** -9 * ref.abs()))
+    assert bool(torch.all((om - ref).abs() <= 2.0 ** -8 * ref.abs()))   # half a BF16 ulp: <= 2^-8 relative
     assert torch.equal(om_t.double(), om.t())
 
 
