@@ -61,9 +61,17 @@ def parse():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--cpu-rows", type=int, default=0, help="row sample of the CPU baseline (0: auto)")
     ap.add_argument("--quick", action="store_true", help="small shape for a smoke run")
+    ap.add_argument("--no-serving", action="store_true", help="skip the batched / served leg")
+    ap.add_argument("--only-serving", action="store_true", help="run the batched / served leg alone")
+    ap.add_argument("--batch-count", type=int, default=1024, help="matrices in the uneven batch")
+    ap.add_argument("--serve-workers", type=int, default=8, help="concurrent solves of the server")
+    ap.add_argument("--serve-pool", type=int, default=256, help="distinct resident matrices the requests use")
+    ap.add_argument("--serve-rates", default="200,1000,5000", help="Poisson arrival rates, requests/s")
+    ap.add_argument("--serve-seconds", type=float, default=0.5, help="arrival window per rate (>= 400 requests)")
     args = ap.parse_args()
     if args.quick:
         args.m, args.n, args.k, args.p, args.N, args.rank_r = 8192, 4096, 16, 8, 16, 64
+        args.batch_count, args.serve_pool, args.serve_seconds = 64, 32, 0.1
     return args
 
 
@@ -415,6 +423,170 @@ def run_b200(args, world, rank, local):
 
 
 # ------------------------------------------------------------------------------------------------
+# batched and served solves: uneven FP32 matrices through mcnla_b200_server_*
+# ------------------------------------------------------------------------------------------------
+def _pct(xs, q):
+    xs = sorted(xs)
+    return xs[min(len(xs) - 1, int(q * len(xs)))] if xs else None
+
+
+def run_serving(args, dev):
+    """Uneven batch (1024 FP32 matrices, m ~ U[512,16384], n ~ U[256,4096], k in {8,16,32,64},
+    p = k/2, N = 8, sigma_j = j^-alpha, KN tol 1e-5, SVD former) through the server:
+    per-request plain FP64 (one worker), batched FP64 and batched mixed precision (W
+    workers), then Poisson arrivals at each rate with 5 % large requests (65536 x 8192,
+    k = 128, p = 32, N = 16), mixed precision, 150 GB admission cap.  A stays resident in
+    HBM as FP32; wall-clock times on the host with the device synchronized on both sides
+    (the solves run on the workers' own streams)."""
+    import numpy as np
+    import torch
+    from mcnla_b200 import isvd, synthetic
+
+    W = args.serve_workers
+    budget = 150 << 30
+    shapes = synthetic.batch_shapes(args.batch_count, seed=4)
+    pool = [synthetic.lowrank_torch(sh["m"], sh["n"], sh["sigma"], seed=sh["seed"], device=dev, dtype=torch.float32)
+            for sh in shapes]
+    torch.cuda.synchronize()
+
+    def request(i, mixed, a=None, sh=None):
+        sh = shapes[i] if sh is None else sh
+        return isvd.Request(pool[i] if a is None else a, sh["k"], sh["p"], sh["N"], seed=sh["seed"],
+                            integrator="kn", former="svd", maxit=256, tol=1e-5, mixed=mixed)
+
+    order = sorted(range(len(shapes)), key=lambda i: -shapes[i]["m"] * shapes[i]["n"] * shapes[i]["k"])
+
+    def timed_batch(workers, mixed):
+        reqs = [request(i, mixed) for i in range(len(shapes))]
+        with isvd.Server(workers=workers, budget_bytes=budget, device=dev) as srv:
+            warm = [request(i, mixed) for i in order[:2 * workers]]        # grow every worker's buffers
+            for r in warm:
+                srv.submit(r)
+            for r in warm:
+                srv.wait(r)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for r in reqs:
+                srv.submit(r)
+            for r in reqs:
+                srv.wait(r)
+            torch.cuda.synchronize()
+            t = time.perf_counter() - t0
+            st = srv.stats()
+        bad = sum(1 for r in reqs if r.result.status != 0)
+        its = [r.result.iteration for r in reqs]
+        svc = [r.result.seconds for r in reqs]
+        a_bytes = sum(shapes[i]["m"] * shapes[i]["n"] * 4 for i in range(len(shapes)))
+        return reqs, {"workers": workers, "solves_per_s": round(len(reqs) / t, 2), "seconds": round(t, 4),
+                      "a_read_gbs": round(2 * a_bytes / t / 1e9, 2), "failed": bad,
+                      "iterations_mean": round(float(np.mean(its)), 2), "iterations_max": int(max(its)),
+                      "service_p50_ms": round(_pct(svc, 0.5) * 1e3, 3),
+                      "service_p99_ms": round(_pct(svc, 0.99) * 1e3, 3),
+                      "peak_admitted_gb": round(st["peak_bytes"] / 1e9, 3)}
+
+    _, serial64 = timed_batch(1, False)
+    _, batched64 = timed_batch(W, False)
+    mixed_reqs, batched_mx = timed_batch(W, True)
+
+    # accuracy of the mixed results against FP64 solves on the same A and Omega (BF16 Omega
+    # drawn from the same seed, FP64 copy), and against FP64 dgesvd singular values of A
+    acc = {"sigma_rel_err": 0.0, "max_principal_angle_U": 0.0, "UtU_minus_I_fro": 0.0, "sampled": 0,
+           "sigma_rel_err_vs_dgesvd": 0.0, "sampled_dgesvd": 0}
+    for i in range(min(16, len(shapes))):
+        sh, r = shapes[i], mixed_reqs[i]
+        k, L = sh["k"], (sh["k"] + sh["p"]) * sh["N"]
+        a64 = pool[i].double()
+        _, _, om64 = isvd.gaussian_bf16(sh["n"], L, sh["seed"], dev, with_fp64=True)
+        s64, u64, _, _ = isvd.solve(a64, k, sh["p"], sh["N"], omega=om64, integrator="kn", former="svd",
+                                    maxit=256, tol=1e-5)
+        acc["sigma_rel_err"] = max(acc["sigma_rel_err"], ((r.s - s64).abs() / s64).max().item())
+        cosmin = torch.linalg.svdvals(u64.t() @ r.u).min().clamp(-1, 1)
+        acc["max_principal_angle_U"] = max(acc["max_principal_angle_U"], float(torch.arccos(cosmin).item()))
+        eye = torch.eye(k, dtype=torch.float64, device=dev)
+        acc["UtU_minus_I_fro"] = max(acc["UtU_minus_I_fro"], float(torch.linalg.norm(r.u.t() @ r.u - eye).item()))
+        acc["sampled"] += 1
+        if sh["m"] * sh["n"] <= (1 << 23) and acc["sampled_dgesvd"] < 4:
+            sv = torch.linalg.svdvals(a64, driver="gesvd")[:k]
+            acc["sigma_rel_err_vs_dgesvd"] = max(acc["sigma_rel_err_vs_dgesvd"], ((r.s - sv).abs() / sv).max().item())
+            acc["sampled_dgesvd"] += 1
+        del a64, om64
+    del mixed_reqs
+
+    # ---- served: Poisson arrivals, mixed precision, 5 % large requests
+    keep = max(1, min(args.serve_pool, len(pool)))
+    del pool[keep:]
+    torch.cuda.empty_cache()
+    lsh = [synthetic.large_shape(seed=s) for s in (1, 2)]
+    large = [synthetic.lowrank_torch(x["m"], x["n"], x["sigma"], seed=x["seed"], device=dev, dtype=torch.float32)
+             for x in lsh]
+    torch.cuda.synchronize()
+    # per-request plain FP64 service time of the large request, for the mix's FP64 reference rate
+    t_large = []
+    for _ in range(2):
+        r = request(0, False, a=large[0], sh=lsh[0])
+        with isvd.Server(workers=1, budget_bytes=budget, device=dev) as srv:
+            srv.submit(r)
+            srv.wait(r)
+        t_large.append(r.result.seconds)
+    t_small = serial64["seconds"] / len(shapes)
+    fp64_mix_rate = 1.0 / (0.95 * t_small + 0.05 * t_large[-1])
+    served = []
+    rates = [float(x) for x in args.serve_rates.split(",") if x]
+    with isvd.Server(workers=W, budget_bytes=budget, device=dev) as srv:
+        warm = [request(0, True, a=large[j], sh=lsh[j]) for j in range(2)] + \
+               [request(i, True) for i in range(min(keep, 2 * W))]
+        for r in warm:
+            srv.submit(r)
+        for r in warm:
+            srv.wait(r)
+        for rate in rates:
+            rng = np.random.default_rng(int(rate))
+            count = max(400, int(rate * args.serve_seconds)) if not args.quick else 64
+            arrivals = np.cumsum(rng.exponential(1.0 / rate, count))
+            is_large = rng.random(count) < 0.05
+            pick = rng.integers(0, keep, count)
+            reqs = [request(0, True, a=large[j % 2], sh=lsh[j % 2]) if is_large[j] else request(int(pick[j]), True)
+                    for j in range(count)]
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for r, ta in zip(reqs, arrivals):
+                while time.perf_counter() - t0 < ta:
+                    pass
+                srv.submit(r)
+            for r in reqs:
+                srv.wait(r)
+            torch.cuda.synchronize()
+            t = time.perf_counter() - t0
+            lat = [r.result.latency for r in reqs]
+            lat_small = [r.result.latency for r, big in zip(reqs, is_large) if not big]
+            served.append({"rate_per_s": rate, "requests": count, "large": int(is_large.sum()),
+                           "solves_per_s": round(count / t, 2), "seconds": round(t, 4),
+                           "p50_ms": round(_pct(lat, 0.5) * 1e3, 3), "p99_ms": round(_pct(lat, 0.99) * 1e3, 3),
+                           "p50_ms_small": round(_pct(lat_small, 0.5) * 1e3, 3),
+                           "p99_ms_small": round(_pct(lat_small, 0.99) * 1e3, 3),
+                           "failed": sum(1 for r in reqs if r.result.status != 0)})
+            del reqs
+        st = srv.stats()
+    del large, pool
+    torch.cuda.empty_cache()
+    return {
+        "workload": "%d uneven FP32 matrices (m~U[512,16384], n~U[256,4096], k in {8,16,32,64}, p=k/2, N=8, "
+                    "sigma_j=j^-alpha, alpha~U[0.5,2], spectrum cut at 256), KN tol 1e-5, SVD former"
+                    % len(shapes),
+        "timing": "host wall clock, device synchronized on both sides; solves on the workers' own streams",
+        "per_request_fp64": serial64, "batched_fp64": batched64, "batched_mixed": batched_mx,
+        "mixed_speedup_vs_per_request_fp64": round(batched_mx["solves_per_s"] / serial64["solves_per_s"], 3),
+        "mixed_speedup_vs_batched_fp64": round(batched_mx["solves_per_s"] / batched64["solves_per_s"], 3),
+        "accuracy_mixed_vs_fp64_same_A_Omega": acc,
+        "served": {"precision": "mixed", "workers": W, "admission_cap_gb": budget / 1e9,
+                   "large": "5%% of requests: 65536 x 8192 FP32, k=128 p=32 N=16 (%s)" % "two resident matrices",
+                   "resident_pool": keep, "fp64_per_request_solves_per_s_same_mix": round(fp64_mix_rate, 2),
+                   "fp64_large_request_s": round(t_large[-1], 4), "rates": served,
+                   "peak_admitted_gb": round(st["peak_bytes"] / 1e9, 3)},
+    }
+
+
+# ------------------------------------------------------------------------------------------------
 # CPU: the reference's own stages on a bounded row sample
 # ------------------------------------------------------------------------------------------------
 def cpu_sample(args, rows=None):
@@ -496,8 +668,16 @@ def main():
     world, rank, local = dist_init(args)
     if args.impl == "reference":
         res = run_reference(args, world, rank)
+    elif args.only_serving:
+        import torch
+        torch.cuda.set_device(local)
+        res = {"metric": METRIC, "serving": run_serving(args, torch.device("cuda", local))}
     else:
         res = run_b200(args, world, rank, local)
+        if world == 1 and not args.no_serving:
+            import torch
+            torch.cuda.empty_cache()
+            res["serving"] = run_serving(args, torch.device("cuda", local))
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             est, info = cpu_sample(args)
             res["cpu_baseline"] = {"value": round(1.0 / est, 6), "unit": "iSVD/s", "cores": info["cores"],

@@ -106,12 +106,15 @@ MCNLA_B200_API int64_t mcnla_b200_kernels_launched(const mcnla_b200_ctx* ctx);
 
 /* Kolmogorov-Nagumo step method.  The reference forms C = f(Z) and inv(C)
  * from an eigendecomposition of Z (row_block_kolmogorov_nagumo_integrator.hpp:159-180).
- * MCNLA_B200_KN_AUTO (default) evaluates the same matrix functions by coupled
- * Newton-Schulz iterations on the FP64 MMA when l <= 80 and falls back to the
- * eigendecomposition when they do not converge; MCNLA_B200_KN_EIGEN always
- * uses the eigendecomposition (parallel Jacobi).                             */
+ * MCNLA_B200_KN_AUTO (default) evaluates the same matrix functions as power
+ * series in Z on the FP64 MMA of ceil(l/8) CTAs when 4 ||Z||_F <= 1/2 (all
+ * but the first iterations), else by coupled Newton-Schulz iterations
+ * (l <= 80) or the eigendecomposition.  MCNLA_B200_KN_NEWTON_SCHULZ skips the
+ * series; MCNLA_B200_KN_EIGEN always uses the eigendecomposition (parallel
+ * Jacobi).                                                                   */
 #define MCNLA_B200_KN_AUTO  0
 #define MCNLA_B200_KN_EIGEN 1
+#define MCNLA_B200_KN_NEWTON_SCHULZ 2
 MCNLA_B200_API int mcnla_b200_set_kn_method(mcnla_b200_ctx* ctx, int method);
 
 /* Stage timers: seconds per part of the last stage call, the reference's
@@ -247,6 +250,7 @@ typedef struct mcnla_b200_problem {
   int iteration;          /* out */
   int status;             /* out */
   double seconds;         /* out: device time of the solve */
+  double latency;         /* out: host seconds from submit to completion (server) */
 } mcnla_b200_problem;
 
 typedef struct mcnla_b200_server mcnla_b200_server;
@@ -259,7 +263,8 @@ MCNLA_B200_API int mcnla_b200_server_create(mcnla_b200_server** server, int devi
 MCNLA_B200_API int mcnla_b200_server_submit(mcnla_b200_server* server, const mcnla_b200_problem* problem,
                                             int64_t* ticket);
 /* Blocks until the ticket's problem is done and copies it (with iteration,
- * status and seconds filled) to *out.  Each ticket can be waited on once.   */
+ * status, seconds and latency filled) to *out.  Each ticket can be waited on
+ * once.                                                                      */
 MCNLA_B200_API int mcnla_b200_server_wait(mcnla_b200_server* server, int64_t ticket, mcnla_b200_problem* out);
 /* Bytes admitted right now and the most ever admitted at once.              */
 MCNLA_B200_API int mcnla_b200_server_stats(mcnla_b200_server* server, int64_t* in_flight_bytes, int64_t* peak_bytes,

@@ -28,7 +28,7 @@ GRAMIAN_FORMER = 1
 ROW_BLOCK_GRAMIAN_FORMER = 2
 COL_BLOCK_GRAMIAN_FORMER = 3
 
-KN_AUTO, KN_EIGEN = 0, 1
+KN_AUTO, KN_EIGEN, KN_NEWTON_SCHULZ = 0, 1, 2
 
 MAX_DIM_SKETCH = 160
 MAX_DIM_SKETCH_WENYIN = 80
@@ -49,7 +49,8 @@ class Problem(ctypes.Structure):
                 ("lda", ctypes.c_int64), ("seed", ctypes.c_uint64), ("integrator", ctypes.c_int),
                 ("former", ctypes.c_int), ("max_iteration", ctypes.c_int), ("tolerance", ctypes.c_double),
                 ("precision", ctypes.c_int), ("S", ctypes.c_void_p), ("U", ctypes.c_void_p), ("V", ctypes.c_void_p),
-                ("iteration", ctypes.c_int), ("status", ctypes.c_int), ("seconds", ctypes.c_double)]
+                ("iteration", ctypes.c_int), ("status", ctypes.c_int), ("seconds", ctypes.c_double),
+                ("latency", ctypes.c_double)]
 
 
 class McnlaError(RuntimeError):

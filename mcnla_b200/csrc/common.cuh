@@ -27,6 +27,7 @@ namespace mb {
 
 void set_last_cuda_error(cudaError_t e, const char* what, const char* file, int line);
 void set_last_message(const std::string& msg);
+const char* last_error_text();
 
 // Element (i, j) of a strided matrix lives at p[i * rs + j * cs].
 struct CMat { const double* p; int64_t rs, cs; };
@@ -51,7 +52,10 @@ struct DevScalars {
   int status;         // device-side error code (0 = ok)
   int sweeps;         // Jacobi sweeps used by the last small solve
   int stop_it;        // iteration at which an integrator converged (INT_MAX: not yet)
-  int pad;
+  int kn_fallback;    // 1: the series KN step declined this iteration (||Z|| too large)
+  unsigned bar_count; // grid barrier of cooperative kernels: arrivals
+  unsigned bar_gen;   //   and generation
+  int pad[2];
 };
 
 // Per-device context: one stream, a growable workspace arena, timing events.

@@ -8,6 +8,7 @@
 // 32 lanes x 8 bytes.
 #include "dgemm.cuh"
 #include <algorithm>
+#include <atomic>
 
 namespace mb {
 namespace {
@@ -250,11 +251,13 @@ __global__ void splitk_reduce_kernel(const double* ws, int splits, int batch, in
 
 template <class C>
 int launch(Context* ctx, const KArgs& g, int batch) {
-  static bool attr_set = false;
+  // the shared-memory opt-in is a per-device property of the function: one bit per device
+  static std::atomic<uint64_t> attr_set{0};
   auto kern = dgemm_kernel<C>;
-  if (!attr_set) {
+  const uint64_t bit = uint64_t(1) << (ctx->device & 63);
+  if (!(attr_set.load(std::memory_order_acquire) & bit)) {
     MB_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(C::SMEM)));
-    attr_set = true;
+    attr_set.fetch_or(bit, std::memory_order_acq_rel);
   }
   dim3 grid(unsigned(cdiv(g.N, C::BN)), unsigned(cdiv(g.M, C::BM)), unsigned(batch * g.splits));
   kern<<<grid, C::THREADS, C::SMEM, ctx->stream>>>(g);

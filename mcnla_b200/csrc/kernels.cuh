@@ -24,13 +24,27 @@ int launch_scale_cols_rsqrt(Context* c, int n, int batch, const double* V, const
 //       outn = [Fc; inv(C)/N]          (optional)
 //       ffn  = ff * Fc                 (optional, ff/ffn l x l)
 // scal->norm := || s - 1 ||_2, s = sqrt(1/2 + sqrt(1/4 - eig(Z))).
-// vwork: l*l doubles of global scratch used when V does not fit on chip.
+// vwork: kn_series_work_doubles(l) doubles of global scratch.
+// Method (mcnla_b200_set_kn_method): KN_AUTO runs the series kernel and, for
+// the iterations it declines, the Newton-Schulz kernel (l <= 80) or the
+// eigendecomposition; KN_NEWTON_SCHULZ starts at Newton-Schulz; KN_EIGEN
+// always uses the eigendecomposition.
 // When the context's iteration guard is set, the step is skipped for an
 // iteration past convergence, and scal->stop_it is set to the guard
 // iteration when ||s - 1||_2 < tol fails to hold as "norm >= tol" (a NaN norm
 // converges, like the reference's !(nrm2 >= tol)).
 int launch_kn_step(Context* c, int l, const double* z, const double* dd, double inv_n, double* out, double* outn,
                    const double* ff, double* ffn, double* vwork, double tol);
+// Global scratch (doubles) the KN step needs in vwork.
+size_t kn_series_work_doubles(int l);
+// The series form of the step on ceil(l/8) cooperative CTAs (kn_series.cu);
+// same operands as launch_kn_step.  Sets scal->kn_fallback when ||Z|| is too
+// large for the series; the launcher then runs the other form after it.
+int launch_kn_series(Context* c, int l, const double* z, const double* dd, double inv_n, double* out, double* outn,
+                     const double* ff, double* ffn, double* work, double tol);
+// Opts a kernel in to the device's whole dynamic shared memory (once per
+// device and kernel); fails when `bytes` exceeds it.
+int set_smem(const Context* c, const void* fn, size_t bytes);
 
 // Wen-Yin line-search trial (one CTA): from dd = [Dc | Dgc] and tau builds the
 // 2l x 2l C, inverts it and writes F = [Fc; Fgc] (2l x l) and optionally

@@ -3,6 +3,9 @@
 #include "small.cuh"
 #include "philox.cuh"
 #include <algorithm>
+#include <mutex>
+#include <map>
+#include <utility>
 
 namespace mb {
 namespace {
@@ -119,9 +122,10 @@ __global__ void __launch_bounds__(kSmallThreads) k_kn_step(int l, const double* 
                                                            double inv_n, double* out, double* outn,
                                                            const double* ff, double* ffn, double* vwork,
                                                            int v_smem, DevScalars* scal, double tol,
-                                                           const int* guard_stop, int guard_it) {
+                                                           const int* guard_stop, int guard_it, const int* only_if) {
   extern __shared__ __align__(16) char smem_raw[];
   if (guard_stop && *guard_stop < guard_it) return;
+  if (only_if && *only_if == 0) return;
   SmemCarve sc(smem_raw);
   const int ld = l + 1;
   double* a = sc.take<double>(size_t(l) * ld);
@@ -307,9 +311,10 @@ __global__ void __launch_bounds__(kSmallThreads) k_kn_step_ns(int l, const doubl
                                                               double inv_n, double* out, double* outn,
                                                               const double* ff, double* ffn, double* vwork,
                                                               DevScalars* scal, double tol, const int* guard_stop,
-                                                              int guard_it) {
+                                                              int guard_it, const int* only_if) {
   extern __shared__ __align__(16) char smem_raw[];
   if (guard_stop && *guard_stop < guard_it) return;
+  if (only_if && *only_if == 0) return;
   const int tid = threadIdx.x, nt = blockDim.x;
   const int lp = (l + 15) & ~15, ld = lp + 4;
   const size_t mat = size_t(lp) * ld;
@@ -805,12 +810,30 @@ size_t small_smem_syev(int n, bool v_smem) {
   return mat * (v_smem ? 2 : 1) + jacobi_scratch_bytes(n) + (n + 4) * sizeof(int) + 64;
 }
 
-int set_smem(const void* fn, size_t bytes) {
-  MB_CHECK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
-  return MCNLA_B200_OK;
-}
+
 
 }  // namespace
+
+// Opts a kernel in to all the dynamic shared memory the device allows it (the
+// per-block opt-in limit less its static shared memory), once per (device,
+// kernel).  The limit is a property of the function shared by every host
+// thread, so it is never lowered to one launch's size (a concurrent launch of
+// the same kernel with a larger size on another thread would then fail).
+int set_smem(const Context* c, const void* fn, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, size_t> limits;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = limits.find({c->device, fn});
+  if (it == limits.end()) {
+    // static shared memory of the kernel counts against the same per-block limit
+    cudaFuncAttributes fa;
+    MB_CHECK_CUDA(cudaFuncGetAttributes(&fa, fn));
+    const size_t limit = c->smem_optin > fa.sharedSizeBytes ? c->smem_optin - fa.sharedSizeBytes : 0;
+    MB_CHECK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(limit)));
+    it = limits.emplace(std::make_pair(c->device, fn), limit).first;
+  }
+  return bytes <= it->second ? MCNLA_B200_OK : MCNLA_B200_ERR_UNSUPPORTED;
+}
 
 int reduce_partials(const Context* c) { return c->num_sms * 2; }
 
@@ -826,7 +849,7 @@ int launch_syev(Context* c, int n, int batch, const double* A, int64_t lda, int6
   }
   const size_t smem = small_smem_syev(n, v_smem);
   if (smem > c->smem_optin) return MCNLA_B200_ERR_UNSUPPORTED;
-  MB_CHECK(set_smem(reinterpret_cast<const void*>(k_syev), smem));
+  MB_CHECK(set_smem(c, reinterpret_cast<const void*>(k_syev), smem));
   k_syev<<<batch, kSmallThreads, smem, c->stream>>>(n, A, lda, a_bs, W, V, order, v_smem ? 1 : 0, vwork);
   c->kernels_launched++;
   MB_CHECK_CUDA(cudaGetLastError());
@@ -844,14 +867,20 @@ int launch_scale_cols_rsqrt(Context* c, int n, int batch, const double* V, const
 int launch_kn_step(Context* c, int l, const double* z, const double* dd, double inv_n, double* out, double* outn,
                    const double* ff, double* ffn, double* vwork, double tol) {
   if (l < 1 || l > MCNLA_B200_MAX_DIM_SKETCH) return MCNLA_B200_ERR_UNSUPPORTED;
-  if (l <= kKnNsMaxDim && c->kn_mode == 0) {
+  // the series kernel first; the kernels below then run only when it declined
+  const int* only_if = nullptr;
+  if (c->kn_mode == MCNLA_B200_KN_AUTO) {
+    MB_CHECK(launch_kn_series(c, l, z, dd, inv_n, out, outn, ff, ffn, vwork, tol));
+    only_if = &c->scal->kn_fallback;
+  }
+  if (l <= kKnNsMaxDim && c->kn_mode != MCNLA_B200_KN_EIGEN) {
     const int lp = (l + 15) & ~15;
     const size_t smem = 4 * size_t(lp) * (lp + 4) * sizeof(double) + (64 + 96) * sizeof(double) +
                         jacobi_scratch_bytes(l) + 64;
     if (smem <= c->smem_optin) {
-      MB_CHECK(set_smem(reinterpret_cast<const void*>(k_kn_step_ns), smem));
+      MB_CHECK(set_smem(c, reinterpret_cast<const void*>(k_kn_step_ns), smem));
       k_kn_step_ns<<<1, kSmallThreads, smem, c->stream>>>(l, z, dd, inv_n, out, outn, ff, ffn, vwork, c->scal, tol,
-                                                          c->guard_stop, c->guard_it);
+                                                          c->guard_stop, c->guard_it, only_if);
       c->kernels_launched++;
       MB_CHECK_CUDA(cudaGetLastError());
       return MCNLA_B200_OK;
@@ -860,9 +889,9 @@ int launch_kn_step(Context* c, int l, const double* z, const double* dd, double 
   const bool v_smem = small_smem_syev(l, true) + l * 8 + 64 <= c->smem_optin;
   const size_t smem = small_smem_syev(l, v_smem) + l * 8 + 64;
   if (smem > c->smem_optin) return MCNLA_B200_ERR_UNSUPPORTED;
-  MB_CHECK(set_smem(reinterpret_cast<const void*>(k_kn_step), smem));
+  MB_CHECK(set_smem(c, reinterpret_cast<const void*>(k_kn_step), smem));
   k_kn_step<<<1, kSmallThreads, smem, c->stream>>>(l, z, dd, inv_n, out, outn, ff, ffn, vwork, v_smem ? 1 : 0,
-                                                    c->scal, tol, c->guard_stop, c->guard_it);
+                                                    c->scal, tol, c->guard_stop, c->guard_it, only_if);
   c->kernels_launched++;
   MB_CHECK_CUDA(cudaGetLastError());
   return MCNLA_B200_OK;
@@ -873,7 +902,7 @@ int launch_wy_trial(Context* c, int l, const double* dd, double tau, double inv_
   const int n = 2 * l;
   const size_t smem = size_t(n) * (n + 1) * 8 + 16 + n * 4 + 16 + n * 8 + 16 + 3 * 64 + 64;
   if (smem > c->smem_optin) return MCNLA_B200_ERR_UNSUPPORTED;
-  MB_CHECK(set_smem(reinterpret_cast<const void*>(k_wy_trial), smem));
+  MB_CHECK(set_smem(c, reinterpret_cast<const void*>(k_wy_trial), smem));
   k_wy_trial<<<1, kSmallThreads, smem, c->stream>>>(l, dd, tau, inv_n, F, FN, c->scal);
   c->kernels_launched++;
   MB_CHECK_CUDA(cudaGetLastError());
@@ -965,7 +994,7 @@ int launch_svd_small(Context* c, int n, const double* M, double* W, double* sig,
   if (smem > c->smem_optin) return MCNLA_B200_ERR_UNSUPPORTED;
   double* zwork = z_smem ? nullptr : ctx_take<double>(c, size_t(n) * n);
   if (!z_smem && !zwork) return MCNLA_B200_ERR_WORKSPACE;
-  MB_CHECK(set_smem(reinterpret_cast<const void*>(k_svd_small), smem));
+  MB_CHECK(set_smem(c, reinterpret_cast<const void*>(k_svd_small), smem));
   k_svd_small<<<1, kSmallThreads, smem, c->stream>>>(n, M, W, sig, Z, zwork, z_smem ? 1 : 0);
   c->kernels_launched++;
   MB_CHECK_CUDA(cudaGetLastError());
@@ -1006,7 +1035,7 @@ int launch_inverse(Context* c, int n, int batch, double* A) {
   if (n < 1 || n > 2 * MCNLA_B200_MAX_DIM_SKETCH_WENYIN || batch < 1) return MCNLA_B200_ERR_UNSUPPORTED;
   const size_t smem = size_t(n) * (n + 1) * 8 + 16 + n * 4 + 16 + n * 8 + 16 + 3 * 64 + 64;
   if (smem > c->smem_optin) return MCNLA_B200_ERR_UNSUPPORTED;
-  MB_CHECK(set_smem(reinterpret_cast<const void*>(k_inverse), smem));
+  MB_CHECK(set_smem(c, reinterpret_cast<const void*>(k_inverse), smem));
   k_inverse<<<batch, kSmallThreads, smem, c->stream>>>(n, A, c->scal);
   c->kernels_launched++;
   MB_CHECK_CUDA(cudaGetLastError());

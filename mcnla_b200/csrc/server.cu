@@ -9,9 +9,11 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <condition_variable>
 #include <deque>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <unordered_map>
 #include <vector>
@@ -27,10 +29,14 @@ __global__ void k_f32_to_f64(const float* src, int64_t rows, int64_t cols, int64
   }
 }
 
+using Clock = std::chrono::steady_clock;
+
 struct Job {
   mcnla_b200_problem p;
   int64_t bytes = 0;
   bool done = false;
+  Clock::time_point submitted;
+  std::string error;        // the worker's error message when the solve failed
 };
 
 int64_t round8(int64_t x) { return (x + 7) & ~int64_t(7); }
@@ -158,9 +164,13 @@ void mcnla_b200_server::worker() {
     }
     p.status = st;
     p.seconds = ms * 1e-3;
+    std::string err;
+    if (st != MCNLA_B200_OK) err = ok ? mb::last_error_text() : "worker initialization failed";
     {
       std::lock_guard<std::mutex> lock(mu);
       mb::Job& j = jobs[ticket];
+      j.error = err;
+      p.latency = std::chrono::duration<double>(mb::Clock::now() - j.submitted).count();
       j.p = p;
       j.done = true;
       in_flight -= bytes;
@@ -206,7 +216,9 @@ int mcnla_b200_server_submit(mcnla_b200_server* s, const mcnla_b200_problem* pro
     j.p.iteration = 0;
     j.p.status = -1;
     j.p.seconds = 0;
+    j.p.latency = 0;
     j.bytes = mb::problem_bytes(*problem);
+    j.submitted = mb::Clock::now();
     s->jobs.emplace(t, j);
     s->queue.push_back(t);
     *ticket = t;
@@ -223,6 +235,7 @@ int mcnla_b200_server_wait(mcnla_b200_server* s, int64_t ticket, mcnla_b200_prob
   s->cv_done.wait(lock, [&] { return s->jobs[ticket].done; });
   if (out) *out = s->jobs[ticket].p;
   const int st = s->jobs[ticket].p.status;
+  if (st != MCNLA_B200_OK) mb::set_last_message("server job: " + s->jobs[ticket].error);
   s->jobs.erase(ticket);
   return st;
 }

@@ -159,6 +159,7 @@ int kn_loop(Context* c, int maxit, Body body, int* iters) {
     }
     launched = end;
     MB_CHECK(ctx_sync_scalars(c));
+    if (c->scal_host->status) return c->scal_host->status;
     const int stop = c->scal_host->stop_it;
     if (stop < launched) { done = stop + 1; break; }
   }
@@ -174,14 +175,14 @@ int run_kn(Context* c, const Dims& d, const double* Qs, int maxit, double tol, d
   const size_t wsb = gemm_ws(c, {{L, l, m, 1}, {l, l, L, 1}, {m, l, L, 1}, {m, l, l, 1}, {l, l, m, 1}, {m, l, 2 * l, 1}});
   Plan pl;
   pl.add(size_t(m) * 2 * l); pl.add(size_t(m) * 2 * l); pl.add(size_t(L) * l); pl.add(size_t(l) * l);
-  pl.add(size_t(l) * l); pl.add(size_t(2) * l * l); pl.add(size_t(l) * l); pl.add(wsb / 8 + 1);
+  pl.add(size_t(l) * l); pl.add(size_t(2) * l * l); pl.add(kn_series_work_doubles(l)); pl.add(wsb / 8 + 1);
   MB_CHECK(ctx_reserve(c, pl.bytes));
   double* QX[2] = {ctx_take<double>(c, size_t(m) * 2 * l), ctx_take<double>(c, size_t(m) * 2 * l)};
   double* B = ctx_take<double>(c, size_t(L) * l);
   double* D = ctx_take<double>(c, size_t(l) * l);
   double* Z = ctx_take<double>(c, size_t(l) * l);
   double* CC = ctx_take<double>(c, size_t(2) * l * l);
-  double* vwork = ctx_take<double>(c, size_t(l) * l);
+  double* vwork = ctx_take<double>(c, kn_series_work_doubles(l));
   double* ws = take_ws(c, wsb);
   MB_CHECK(check_arena(c));
   const int64_t lq = 2 * l;
@@ -224,13 +225,13 @@ int run_rb_kn(Context* c, const Dims& d, const double* Qs, int maxit, double tol
   const size_t wsb = gemm_ws(c, {{L, l, m, 1}, {m, l, L, 1}, {l, 2 * l, L, 1}, {m, l, 2 * l, 1}, {L, l, 2 * l, 1}});
   Plan pl;
   for (int i = 0; i < 2; ++i) { pl.add(size_t(m) * 2 * l); pl.add(size_t(L) * 2 * l); }
-  pl.add(size_t(2) * l * l); pl.add(size_t(2) * l * l); pl.add(size_t(l) * l); pl.add(wsb / 8 + 1);
+  pl.add(size_t(2) * l * l); pl.add(size_t(2) * l * l); pl.add(kn_series_work_doubles(l)); pl.add(wsb / 8 + 1);
   MB_CHECK(ctx_reserve(c, pl.bytes));
   double* QG[2] = {ctx_take<double>(c, size_t(m) * 2 * l), ctx_take<double>(c, size_t(m) * 2 * l)};
   double* BB[2] = {ctx_take<double>(c, size_t(L) * 2 * l), ctx_take<double>(c, size_t(L) * 2 * l)};
   double* DD = ctx_take<double>(c, size_t(2) * l * l);
   double* FC = ctx_take<double>(c, size_t(2) * l * l);
-  double* vwork = ctx_take<double>(c, size_t(l) * l);
+  double* vwork = ctx_take<double>(c, kn_series_work_doubles(l));
   double* ws = take_ws(c, wsb);
   MB_CHECK(check_arena(c));
   const int64_t l2 = 2 * l;
@@ -290,7 +291,7 @@ int run_rb_gramian_kn(Context* c, const Dims& d, const double* Qs, int maxit, do
   Plan pl;
   pl.add(size_t(L) * L); pl.add(size_t(L) * l3); pl.add(size_t(L) * l3); pl.add(size_t(l2) * l);
   pl.add(size_t(l2) * l); pl.add(size_t(l2) * l); pl.add(size_t(l) * l); pl.add(size_t(l) * l);
-  pl.add(size_t(L) * l); pl.add(size_t(l) * l); pl.add(wsb / 8 + 1);
+  pl.add(size_t(L) * l); pl.add(kn_series_work_doubles(l)); pl.add(wsb / 8 + 1);
   MB_CHECK(ctx_reserve(c, pl.bytes));
   double* Bs = ctx_take<double>(c, size_t(L) * L);
   double* EB[2] = {ctx_take<double>(c, size_t(L) * l3), ctx_take<double>(c, size_t(L) * l3)};
@@ -299,7 +300,7 @@ int run_rb_gramian_kn(Context* c, const Dims& d, const double* Qs, int maxit, do
   double* FCN = ctx_take<double>(c, size_t(l2) * l);
   double* FF[2] = {ctx_take<double>(c, size_t(l) * l), ctx_take<double>(c, size_t(l) * l)};
   double* Ebar = ctx_take<double>(c, size_t(L) * l);
-  double* vwork = ctx_take<double>(c, size_t(l) * l);
+  double* vwork = ctx_take<double>(c, kn_series_work_doubles(l));
   double* ws = take_ws(c, wsb);
   MB_CHECK(check_arena(c));
   MB_CHECK(ctx_tic(c));
@@ -556,6 +557,8 @@ int run_integrate(Context* c, const Dims& d, int kind, const double* Qs, int max
                   int* iters) {
   if (!Qs || !Qbar || !iters) return MCNLA_B200_ERR_ARG;
   if (maxit < 0 || !(tol >= 0.0)) return MCNLA_B200_ERR_ARG;
+  // device status, convergence scalars and grid-barrier counters start clean
+  MB_CHECK_CUDA(cudaMemsetAsync(c->scal, 0, sizeof(DevScalars), c->stream));
   switch (kind) {
     case MCNLA_B200_KOLMOGOROV_NAGUMO: return run_kn(c, d, Qs, maxit, tol, Qbar, iters);
     case MCNLA_B200_ROW_BLOCK_KOLMOGOROV_NAGUMO: return run_rb_kn(c, d, Qs, maxit, tol, Qbar, iters);

@@ -52,37 +52,38 @@ def config3_sigma(r=200):
 # ----------------------------------------------------------------------------------------------
 # torch (GPU)
 # ----------------------------------------------------------------------------------------------
-def lowrank_torch(m, n, sigma, seed=0, noise=0.0, device="cuda", colmajor=False, chunk_rows=8192):
-    """A = U_r diag(sigma) V_r' + noise * G on the device, float64.
+def lowrank_torch(m, n, sigma, seed=0, noise=0.0, device="cuda", colmajor=False, chunk_rows=8192, dtype=None):
+    """A = U_r diag(sigma) V_r' + noise * G on the device, float64 (or `dtype`).
 
     U_r, V_r come from QR of seeded Gaussians; G is i.i.d. N(0,1).  Built in
     row chunks so the temporaries stay small next to A.  colmajor=True returns
     the m x n column-major view (transpose of a contiguous n x m buffer).
     """
     import torch
+    dt = torch.float64 if dtype is None else dtype
     g = torch.Generator(device=device)
     g.manual_seed(int(seed))
-    sig = torch.as_tensor(np.asarray(sigma, dtype=np.float64), device=device)
+    sig = torch.as_tensor(np.asarray(sigma, dtype=np.float64), device=device).to(dt)
     r = sig.numel()
-    u, _ = torch.linalg.qr(torch.randn(m, r, generator=g, dtype=torch.float64, device=device))
-    v, _ = torch.linalg.qr(torch.randn(n, r, generator=g, dtype=torch.float64, device=device))
+    u, _ = torch.linalg.qr(torch.randn(m, r, generator=g, dtype=dt, device=device))
+    v, _ = torch.linalg.qr(torch.randn(n, r, generator=g, dtype=dt, device=device))
     us = u * sig
     if colmajor:
-        at = torch.empty(n, m, dtype=torch.float64, device=device)
+        at = torch.empty(n, m, dtype=dt, device=device)
         for c0 in range(0, m, chunk_rows):
             c1 = min(m, c0 + chunk_rows)
             blk = v @ us[c0:c1].T
             if noise:
-                blk += noise * torch.randn(n, c1 - c0, generator=g, dtype=torch.float64, device=device)
+                blk += noise * torch.randn(n, c1 - c0, generator=g, dtype=dt, device=device)
             at[:, c0:c1] = blk
         del u, v, us
         return at.t()
-    a = torch.empty(m, n, dtype=torch.float64, device=device)
+    a = torch.empty(m, n, dtype=dt, device=device)
     for r0 in range(0, m, chunk_rows):
         r1 = min(m, r0 + chunk_rows)
         a[r0:r1] = us[r0:r1] @ v.T
         if noise:
-            a[r0:r1] += noise * torch.randn(r1 - r0, n, generator=g, dtype=torch.float64, device=device)
+            a[r0:r1] += noise * torch.randn(r1 - r0, n, generator=g, dtype=dt, device=device)
     del u, v, us
     return a
 
@@ -92,3 +93,31 @@ def omega_torch(n, L, seed=0, device="cuda"):
     g = torch.Generator(device=device)
     g.manual_seed(int(seed) + 7919)
     return torch.randn(n, L, generator=g, dtype=torch.float64, device=device)
+
+
+# ----------------------------------------------------------------------------------------------
+# uneven batches and served requests
+# ----------------------------------------------------------------------------------------------
+def batch_shapes(count, seed=0, r_max=256):
+    """`count` uneven problems: m ~ U[512, 16384], n ~ U[256, 4096], k in {8, 16, 32, 64},
+    p = k / 2, N = 8, sigma_j = j^-alpha with alpha ~ U[0.5, 2] (j = 1 .. min(m, n, r_max);
+    the spectrum is cut at r_max so the generator's QR stays cheap)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        m = int(rng.integers(512, 16385))
+        n = int(rng.integers(256, 4097))
+        k = int(rng.choice([8, 16, 32, 64]))
+        alpha = float(rng.uniform(0.5, 2.0))
+        r = min(m, n, r_max)
+        out.append({"m": m, "n": n, "k": k, "p": k // 2, "N": 8, "alpha": alpha,
+                    "sigma": np.arange(1, r + 1, dtype=np.float64) ** -alpha, "seed": int(seed) * 100003 + i})
+    return out
+
+
+def large_shape(seed=0, r_max=256):
+    """The large served request: m = 65536, n = 8192, k = 128, p = 32, N = 16."""
+    rng = np.random.default_rng(seed)
+    alpha = float(rng.uniform(0.5, 2.0))
+    return {"m": 65536, "n": 8192, "k": 128, "p": 32, "N": 16, "alpha": alpha,
+            "sigma": np.arange(1, r_max + 1, dtype=np.float64) ** -alpha, "seed": int(seed) * 100003 + 99991}

@@ -175,15 +175,15 @@ def test_kn_golden(cuda, golden, cls_name, oracle_name):
 @pytest.mark.parametrize("cls_name", ["KolmogorovNagumoIntegrator", "RowBlockKolmogorovNagumoIntegrator",
                                       "RowBlockGramianKolmogorovNagumoIntegrator"])
 def test_kn_step_methods_agree(cuda, golden, cls_name):
-    """The matrix-function KN step and the eigendecomposition step give the
-    same integrated basis and iteration count on the golden fixture."""
+    """The series, Newton-Schulz and eigendecomposition forms of the KN step
+    give the same integrated basis and iteration count on the golden fixture."""
     from mcnla_b200 import isvd, _lib
     m, l, N = golden["m"], golden["l"], golden["N"]
     prm = params(m, l, l, 0, N)
     out = []
     ctx = isvd.context()
     try:
-        for method in (_lib.KN_AUTO, _lib.KN_EIGEN):
+        for method in (_lib.KN_AUTO, _lib.KN_NEWTON_SCHULZ, _lib.KN_EIGEN):
             ctx.set_kn_method(method)
             integ = getattr(isvd, cls_name)(prm, 256, 1e-4)
             integ.initialize()
@@ -192,8 +192,39 @@ def test_kn_step_methods_agree(cuda, golden, cls_name):
             out.append((integ.iteration(), host(qbar)))
     finally:
         ctx.set_kn_method(_lib.KN_AUTO)
-    assert out[0][0] == out[1][0] == 81
-    assert np.abs(out[0][1] - out[1][1]).max() < TOL
+    assert out[0][0] == out[1][0] == out[2][0] == 81
+    assert np.abs(out[0][1] - out[2][1]).max() < TOL
+    assert np.abs(out[1][1] - out[2][1]).max() < TOL
+
+
+@pytest.mark.parametrize("l", [5, 48, 96, 160])
+@pytest.mark.parametrize("cls_name,oracle_name", [
+    ("KolmogorovNagumoIntegrator", "kn"),
+    ("RowBlockKolmogorovNagumoIntegrator", "rb_kn"),
+    ("RowBlockGramianKolmogorovNagumoIntegrator", "rb_gramian_kn"),
+])
+def test_kn_wide_sketches(cuda, l, cls_name, oracle_name):
+    """KN integrators up to the largest sketch (l = 160, past the one-CTA
+    matrix-function limit): every step method against the oracle."""
+    from mcnla_b200 import isvd, _lib, synthetic
+    m, n, N = 1500, 700, 4
+    a = synthetic.lowrank_np(m, n, np.arange(1, n + 1) ** -1.0, seed=l)
+    omega = np.random.default_rng(l).standard_normal((n, l * N))
+    qs = O.orthogonalize_gramian(a @ omega, l, N)
+    qo, it_ref = O.INTEGRATORS[oracle_name](qs, l, N, 256, 1e-5)
+    prm = params(m, n, l, 0, N)
+    ctx = isvd.context()
+    try:
+        for method in (_lib.KN_AUTO, _lib.KN_NEWTON_SCHULZ, _lib.KN_EIGEN):
+            ctx.set_kn_method(method)
+            integ = getattr(isvd, cls_name)(prm, 256, 1e-5)
+            integ.initialize()
+            qbar = prm.createMatrixQbar()
+            integ(dev(qs, cuda), qbar)
+            assert integ.iteration() == it_ref, method
+            assert np.abs(host(qbar) - qo).max() < TOL, method
+    finally:
+        ctx.set_kn_method(_lib.KN_AUTO)
 
 
 @pytest.mark.parametrize("cls_name,oracle_name", [
