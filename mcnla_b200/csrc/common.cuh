@@ -55,7 +55,8 @@ struct DevScalars {
   int kn_fallback;    // 1: the series KN step declined this iteration (||Z|| too large)
   unsigned bar_count; // grid barrier of cooperative kernels: arrivals
   unsigned bar_gen;   //   and generation
-  int pad[2];
+  int resume_it;      // persistent integrator: iteration it handed back to the host (-1: none)
+  int pad;
 };
 
 // Per-device context: one stream, a growable workspace arena, timing events.

@@ -34,7 +34,7 @@ int launch_scale_cols_rsqrt(Context* c, int n, int batch, const double* V, const
 // iteration when ||s - 1||_2 < tol fails to hold as "norm >= tol" (a NaN norm
 // converges, like the reference's !(nrm2 >= tol)).
 int launch_kn_step(Context* c, int l, const double* z, const double* dd, double inv_n, double* out, double* outn,
-                   const double* ff, double* ffn, double* vwork, double tol);
+                   const double* ff, double* ffn, double* vwork, double tol, bool allow_series = true);
 // Global scratch (doubles) the KN step needs in vwork.
 size_t kn_series_work_doubles(int l);
 // The series form of the step on ceil(l/8) cooperative CTAs (kn_series.cu);
@@ -42,6 +42,16 @@ size_t kn_series_work_doubles(int l);
 // large for the series; the launcher then runs the other form after it.
 int launch_kn_series(Context* c, int l, const double* z, const double* dd, double inv_n, double* out, double* outn,
                      const double* ff, double* ffn, double* work, double tol);
+// Persistent row-block Gramian KN integrator (gkn_persistent.cu): runs
+// iterations [it0, maxit) on one cooperative grid.  On return (after a
+// stream sync) scal->stop_it is the converged iteration, or scal->resume_it
+// the iteration whose KN step the series declined (to be run by the caller
+// with allow_series = false), or neither (maxit reached).  EB, FF, DD, FC,
+// FCN, work: the buffers of the launch-per-product loop.
+bool gkn_persistent_fits(const Context* c, int l, int64_t L);
+int launch_gkn_persistent(Context* c, int l, int64_t L, int N, double tol, int it0, int maxit, const double* Bs,
+                          double* const EB[2], double* const FF[2], double* DD, double* FC, double* FCN,
+                          double* work);
 // Opts a kernel in to the device's whole dynamic shared memory (once per
 // device and kernel); fails when `bytes` exceeds it.
 int set_smem(const Context* c, const void* fn, size_t bytes);

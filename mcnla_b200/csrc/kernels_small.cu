@@ -865,11 +865,11 @@ int launch_scale_cols_rsqrt(Context* c, int n, int batch, const double* V, const
 }
 
 int launch_kn_step(Context* c, int l, const double* z, const double* dd, double inv_n, double* out, double* outn,
-                   const double* ff, double* ffn, double* vwork, double tol) {
+                   const double* ff, double* ffn, double* vwork, double tol, bool allow_series) {
   if (l < 1 || l > MCNLA_B200_MAX_DIM_SKETCH) return MCNLA_B200_ERR_UNSUPPORTED;
   // the series kernel first; the kernels below then run only when it declined
   const int* only_if = nullptr;
-  if (c->kn_mode == MCNLA_B200_KN_AUTO) {
+  if (c->kn_mode == MCNLA_B200_KN_AUTO && allow_series) {
     MB_CHECK(launch_kn_series(c, l, z, dd, inv_n, out, outn, ff, ffn, vwork, tol));
     only_if = &c->scal->kn_fallback;
   }

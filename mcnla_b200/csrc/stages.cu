@@ -309,8 +309,7 @@ int run_rb_gramian_kn(Context* c, const Dims& d, const double* Qs, int maxit, do
   MB_CHECK(launch_fill(c, L, l, 0.0, EB[0], l3));
   MB_CHECK(launch_set_identity(c, l, FF[0], l));
   MB_CHECK(ctx_toc(c));
-  int it = 0;
-  MB_CHECK(kn_loop(c, maxit, [&](int i) -> int {
+  auto body = [&](int i, bool allow_series) -> int {
     const int cur = i & 1;
     double* Ec = EB[cur];
     double* Bc = EB[cur] + l;
@@ -320,13 +319,40 @@ int run_rb_gramian_kn(Context* c, const Dims& d, const double* Qs, int maxit, do
     // [Dc | Dgc] := 1/N Bc' [Bc | Bgc]   (:155-158)
     MB_CHECK(dgemm(c, l, l2, L, inv_n, cm(Bc, 1, l3), crow(Bc, l3), 0.0, drow(DD, l2), GemmBatch(), ws));
     // Z, eig, C, inv(C), Fc; F~+ := F~c Fc; convergence test   (:164-214)
-    MB_CHECK(launch_kn_step(c, l, nullptr, DD, inv_n, FC, FCN, FF[cur], FF[1 - cur], vwork, tol));
+    MB_CHECK(launch_kn_step(c, l, nullptr, DD, inv_n, FC, FCN, FF[cur], FF[1 - cur], vwork, tol, allow_series));
     // E~+ := E~c Fc + 1/N Bc inv(C) = [E~c Bc] [Fc; inv(C)/N]   (:194, :200)
     MB_CHECK(dgemm(c, L, l, l2, 1.0, crow(Ec, l3), crow(FCN, l), 0.0, drow(EB[1 - cur], l3), GemmBatch(), ws));
     // B+ := [Bc Bgc] [Fc; inv(C)]   (:203-204)
     MB_CHECK(dgemm(c, L, l, l2, 1.0, crow(Bc, l3), crow(FC, l), 0.0, drow(EB[1 - cur] + l, l3), GemmBatch(), ws));
     return MCNLA_B200_OK;
-  }, &it));
+  };
+  int it = 0;
+  if (c->kn_mode == MCNLA_B200_KN_AUTO && gkn_persistent_fits(c, l, L)) {
+    // whole iterations on one cooperative grid; an iteration whose KN step the
+    // series declines runs here on the launch-per-product path
+    MB_CHECK_CUDA(cudaMemsetAsync(&c->scal->stop_it, 0x7f, sizeof(int), c->stream));   // "not yet"
+    int it0 = 0, done = -1;
+    while (it0 < maxit && done < 0) {
+      MB_CHECK_CUDA(cudaMemsetAsync(&c->scal->resume_it, 0xff, sizeof(int), c->stream));   // -1
+      MB_CHECK(launch_gkn_persistent(c, l, L, d.N, tol, it0, maxit, Bs, EB, FF, DD, FC, FCN, vwork));
+      MB_CHECK(ctx_sync_scalars(c));
+      if (c->scal_host->status) return c->scal_host->status;
+      if (c->scal_host->stop_it < maxit) { done = c->scal_host->stop_it + 1; break; }
+      const int r = c->scal_host->resume_it;
+      if (r < 0) break;                                       // maxit reached
+      struct Reset { Context* c; ~Reset() { c->guard_stop = nullptr; c->guard_it = 0; } } reset{c};
+      c->guard_stop = &c->scal->stop_it;
+      c->guard_it = r;
+      MB_CHECK(body(r, false));
+      MB_CHECK(ctx_sync_scalars(c));
+      if (c->scal_host->status) return c->scal_host->status;
+      if (c->scal_host->stop_it == r) done = r + 1;
+      it0 = r + 1;
+    }
+    it = done < 0 ? maxit : done;
+  } else {
+    MB_CHECK(kn_loop(c, maxit, [&](int i) -> int { return body(i, true); }, &it));
+  }
   const int cur = it & 1;
   MB_CHECK(ctx_toc(c));
   // Qbar := Q0 F~ + Qs E~   (:225-226)

@@ -197,6 +197,28 @@ def test_kn_step_methods_agree(cuda, golden, cls_name):
     assert np.abs(out[1][1] - out[2][1]).max() < TOL
 
 
+def test_gramian_kn_runs_persistent(cuda, golden):
+    """With the default step method the row-block Gramian KN integrator runs
+    whole iterations in one cooperative kernel: far fewer launches than the
+    five or more per iteration of the launch-per-product loop."""
+    from mcnla_b200 import isvd, _lib
+    m, l, N = golden["m"], golden["l"], golden["N"]
+    prm = params(m, l, l, 0, N)
+    ctx = isvd.context()
+    counts = []
+    for method in (_lib.KN_AUTO, _lib.KN_NEWTON_SCHULZ):
+        ctx.set_kn_method(method)
+        integ = isvd.RowBlockGramianKolmogorovNagumoIntegrator(prm, 256, 1e-4)
+        integ.initialize()
+        qbar = prm.createMatrixQbar()
+        k0 = ctx.kernels_launched()
+        integ(dev(golden["qs"], cuda), qbar)
+        counts.append(ctx.kernels_launched() - k0)
+        assert integ.iteration() == 81
+    ctx.set_kn_method(_lib.KN_AUTO)
+    assert counts[0] < 40 and counts[1] > 5 * 81, counts
+
+
 @pytest.mark.parametrize("l", [5, 48, 96, 160])
 @pytest.mark.parametrize("cls_name,oracle_name", [
     ("KolmogorovNagumoIntegrator", "kn"),
