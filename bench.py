@@ -68,6 +68,9 @@ def parse():
     ap.add_argument("--serve-pool", type=int, default=256, help="distinct resident matrices the requests use")
     ap.add_argument("--serve-rates", default="200,1000,5000", help="Poisson arrival rates, requests/s")
     ap.add_argument("--serve-seconds", type=float, default=0.5, help="arrival window per rate (>= 400 requests)")
+    ap.add_argument("--serve-integrator", default="rb_gramian_kn", help="KN integrator of the batched / served solves")
+    ap.add_argument("--parts", type=int, default=2, help="BF16 parts of A in the mixed leg (2: 16 bits, 3: 24 bits)")
+    ap.add_argument("--serve-parts", type=int, default=3, help="BF16 parts of A in the batched / served mixed solves")
     args = ap.parse_args()
     if args.quick:
         args.m, args.n, args.k, args.p, args.N, args.rank_r = 8192, 4096, 16, 8, 16, 64
@@ -316,7 +319,7 @@ def run_b200(args, world, rank, local):
         torch.cuda.synchronize()
         e_s0, e_s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e_s0.record(stream)
-        split = isvd.split_bf16(a, True)
+        split = isvd.split_bf16(a, args.parts)
         e_s1.record(stream)
         torch.cuda.synchronize()
         split_s = e_s0.elapsed_time(e_s1) / 1e3
@@ -341,9 +344,9 @@ def run_b200(args, world, rank, local):
         qb = torch.empty(m, L, dtype=torch.float64, device=dev)
         sk_t = []
         for _ in range(3):
-            _lib.check(ctx.lib.mcnla_b200_sketch_bf16(ctx.bind(), ctypes.byref(prm_c), isvd._ptr(split[0]),
-                                                      isvd._ptr(split[1]), split[2], isvd._ptr(om_t), ldo,
-                                                      isvd._ptr(qb)), "sketch_bf16")
+            _lib.check(ctx.lib.mcnla_b200_sketch_bf16(ctx.bind(), ctypes.byref(prm_c), isvd._ptr(split.hi),
+                                                      isvd._ptr(split.lo), isvd._ptr(split.lo2), split.ld,
+                                                      isvd._ptr(om_t), ldo, isvd._ptr(qb)), "sketch_bf16")
             sk_t.append(ctx.last_times()[1])
         sk_bf16 = sum(sk_t) / len(sk_t)
         # accuracy of the mixed solve against the FP64 solve on the same A and Omega
@@ -355,17 +358,18 @@ def run_b200(args, world, rank, local):
         ang = float(torch.arccos(torch.clamp(torch.linalg.svdvals(u64.t() @ umx).min(), -1, 1)).item())
         orth = float(torch.linalg.norm(umx.t() @ umx - torch.eye(k, dtype=torch.float64, device=dev)).item())
         bf16_peak = _measured_peak("bf16_tflops")
-        ach = 2.0 * 2.0 * m * n * L / sk_bf16 / 1e12
+        ach = args.parts * 2.0 * m * n * L / sk_bf16 / 1e12
         mixed = {"value": round(world * args.steps / t_mixed, 5), "unit": "iSVD/s",
                  "ms_per_step": round(t_mixed / args.steps * 1e3, 3),
                  "speedup_vs_fp64": round((world * args.steps / t_mixed) / value, 3),
-                 "sketch": "A = A_hi + A_lo (BF16), Omega BF16, tcgen05 FP32 accumulation, FP64 out",
+                 "sketch": "A as %d BF16 parts (%d bits), Omega BF16, tcgen05 FP32 accumulation, FP64 out"
+                           % (args.parts, 8 * args.parts),
                  "split_s": round(split_s, 5), "sketch_gemm_s": round(sk_bf16, 5),
                  "sketch_roofline": {"bound": "tensor", "achieved": round(ach, 2),
                                      "peak": bf16_peak, "unit": "TFLOP/s",
                                      "frac": round(ach / bf16_peak, 4) if bf16_peak else None,
                                      "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst) of measured",
-                                     "algorithmic": "2 parts x 2 m n N l flops"},
+                                     "algorithmic": "%d parts x 2 m n N l flops" % args.parts},
                  "accuracy_vs_fp64_same_A_Omega": {"sigma_rel_err": rel, "max_principal_angle_U": ang,
                                                    "UtU_minus_I_fro": orth, "iterations": [itmx, it64]}}
         del split, qb, om_t, om64
@@ -452,7 +456,7 @@ def run_serving(args, dev):
     def request(i, mixed, a=None, sh=None):
         sh = shapes[i] if sh is None else sh
         return isvd.Request(pool[i] if a is None else a, sh["k"], sh["p"], sh["N"], seed=sh["seed"],
-                            integrator="kn", former="svd", maxit=256, tol=1e-5, mixed=mixed)
+                            integrator=args.serve_integrator, former="svd", maxit=256, tol=1e-5, mixed=mixed)
 
     order = sorted(range(len(shapes)), key=lambda i: -shapes[i]["m"] * shapes[i]["n"] * shapes[i]["k"])
 
@@ -486,7 +490,7 @@ def run_serving(args, dev):
 
     _, serial64 = timed_batch(1, False)
     _, batched64 = timed_batch(W, False)
-    mixed_reqs, batched_mx = timed_batch(W, True)
+    mixed_reqs, batched_mx = timed_batch(W, args.serve_parts)
 
     # accuracy of the mixed results against FP64 solves on the same A and Omega (BF16 Omega
     # drawn from the same seed, FP64 copy), and against FP64 dgesvd singular values of A
@@ -497,8 +501,8 @@ def run_serving(args, dev):
         k, L = sh["k"], (sh["k"] + sh["p"]) * sh["N"]
         a64 = pool[i].double()
         _, _, om64 = isvd.gaussian_bf16(sh["n"], L, sh["seed"], dev, with_fp64=True)
-        s64, u64, _, _ = isvd.solve(a64, k, sh["p"], sh["N"], omega=om64, integrator="kn", former="svd",
-                                    maxit=256, tol=1e-5)
+        s64, u64, _, _ = isvd.solve(a64, k, sh["p"], sh["N"], omega=om64, integrator=args.serve_integrator,
+                                    former="svd", maxit=256, tol=1e-5)
         acc["sigma_rel_err"] = max(acc["sigma_rel_err"], ((r.s - s64).abs() / s64).max().item())
         cosmin = torch.linalg.svdvals(u64.t() @ r.u).min().clamp(-1, 1)
         acc["max_principal_angle_U"] = max(acc["max_principal_angle_U"], float(torch.arccos(cosmin).item()))
@@ -533,8 +537,8 @@ def run_serving(args, dev):
     served = []
     rates = [float(x) for x in args.serve_rates.split(",") if x]
     with isvd.Server(workers=W, budget_bytes=budget, device=dev) as srv:
-        warm = [request(0, True, a=large[j], sh=lsh[j]) for j in range(2)] + \
-               [request(i, True) for i in range(min(keep, 2 * W))]
+        warm = [request(0, args.serve_parts, a=large[j], sh=lsh[j]) for j in range(2)] + \
+               [request(i, args.serve_parts) for i in range(min(keep, 2 * W))]
         for r in warm:
             srv.submit(r)
         for r in warm:
@@ -545,7 +549,8 @@ def run_serving(args, dev):
             arrivals = np.cumsum(rng.exponential(1.0 / rate, count))
             is_large = rng.random(count) < 0.05
             pick = rng.integers(0, keep, count)
-            reqs = [request(0, True, a=large[j % 2], sh=lsh[j % 2]) if is_large[j] else request(int(pick[j]), True)
+            reqs = [request(0, args.serve_parts, a=large[j % 2], sh=lsh[j % 2]) if is_large[j]
+                    else request(int(pick[j]), args.serve_parts)
                     for j in range(count)]
             torch.cuda.synchronize()
             t0 = time.perf_counter()
@@ -571,14 +576,14 @@ def run_serving(args, dev):
     torch.cuda.empty_cache()
     return {
         "workload": "%d uneven FP32 matrices (m~U[512,16384], n~U[256,4096], k in {8,16,32,64}, p=k/2, N=8, "
-                    "sigma_j=j^-alpha, alpha~U[0.5,2], spectrum cut at 256), KN tol 1e-5, SVD former"
-                    % len(shapes),
+                    "sigma_j=j^-alpha, alpha~U[0.5,2], spectrum cut at 256), %s tol 1e-5, SVD former"
+                    % (len(shapes), args.serve_integrator),
         "timing": "host wall clock, device synchronized on both sides; solves on the workers' own streams",
         "per_request_fp64": serial64, "batched_fp64": batched64, "batched_mixed": batched_mx,
         "mixed_speedup_vs_per_request_fp64": round(batched_mx["solves_per_s"] / serial64["solves_per_s"], 3),
         "mixed_speedup_vs_batched_fp64": round(batched_mx["solves_per_s"] / batched64["solves_per_s"], 3),
         "accuracy_mixed_vs_fp64_same_A_Omega": acc,
-        "served": {"precision": "mixed", "workers": W, "admission_cap_gb": budget / 1e9,
+        "served": {"precision": "mixed, A as %d BF16 parts" % args.serve_parts, "workers": W, "admission_cap_gb": budget / 1e9,
                    "large": "5%% of requests: 65536 x 8192 FP32, k=128 p=32 N=16 (%s)" % "two resident matrices",
                    "resident_pool": keep, "fp64_per_request_solves_per_s_same_mix": round(fp64_mix_rate, 2),
                    "fp64_large_request_s": round(t_large[-1], 4), "rates": served,

@@ -189,38 +189,41 @@ MCNLA_B200_API int mcnla_b200_isvd_host(mcnla_b200_ctx* ctx, const mcnla_b200_pa
 
 /* ---- mixed precision (BF16 tensor cores, tcgen05) ---------------------------
  * The sketch A * Omega is where the plain FP64 path spends most of its time.
- * The mixed path keeps A as two BF16 parts, A = A_hi + A_lo (16 bits of
- * mantissa), draws Omega directly in BF16, and runs the sketch on the
- * tcgen05 tensor cores with FP32 accumulation; the orthogonalizer,
- * integrator and former stay FP64.  BF16 buffers are uint16_t bit patterns,
- * K-major (row pitch a multiple of 8 elements, 16-byte aligned base).       */
+ * The mixed path keeps A as two or three BF16 parts, A = A_hi + A_lo (+
+ * A_lo2): 16 or 24 bits of mantissa (three parts hold an FP32 A exactly),
+ * draws Omega directly in BF16, and runs the sketch on the tcgen05 tensor
+ * cores with FP32 accumulation; the orthogonalizer, integrator and former
+ * stay FP64.  BF16 buffers are uint16_t bit patterns, K-major (row pitch a
+ * multiple of 8 elements, 16-byte aligned base).                            */
 
-/* hi := bf16(A), lo := bf16(A - hi) (lo may be NULL), row-major m x n with
- * pitch ldo, from FP64 A (row- or column-major).                            */
+/* hi := bf16(A), lo := bf16(A - hi), lo2 := bf16(A - hi - lo) (lo, lo2 may be
+ * NULL), row-major m x n with pitch ldo, from FP64 A (row- or column-major). */
 MCNLA_B200_API int mcnla_b200_split_bf16(mcnla_b200_ctx* ctx, const double* A, int a_layout, int64_t lda, int64_t m,
-                                         int64_t n, uint16_t* hi, uint16_t* lo, int64_t ldo);
+                                         int64_t n, uint16_t* hi, uint16_t* lo, uint16_t* lo2, int64_t ldo);
 /* Omega' (L x n, pitch ldo) in BF16 from the stream of mcnla_b200_gaussian
  * (element (i, j) of the n x L Omega is sample i*L + j) rounded to BF16;
  * omega (optional, n x L FP64) receives the same rounded values.            */
 MCNLA_B200_API int mcnla_b200_gaussian_bf16(mcnla_b200_ctx* ctx, uint64_t seed, int64_t n, int64_t L,
                                             uint16_t* omega_t, int64_t ldo, double* omega);
-/* D (M x N, FP64 when out_fp64 else FP32, pitch ldd) := (A_hi + A_lo) B' with
- * A_* M x K and B N x K BF16 K-major; a_lo may be NULL.  Synchronizes.      */
+/* D (M x N, FP64 when out_fp64 else FP32, pitch ldd) := (A_hi + A_lo + A_lo2) B'
+ * with A_* M x K and B N x K BF16 K-major; a_lo, a_lo2 may be NULL (a_lo2
+ * only with a_lo).  Synchronizes.                                            */
 MCNLA_B200_API int mcnla_b200_gemm_bf16(mcnla_b200_ctx* ctx, int64_t M, int64_t N, int64_t K, const uint16_t* a_hi,
-                                        const uint16_t* a_lo, int64_t lda, const uint16_t* b, int64_t ldb, void* D,
-                                        int64_t ldd, int out_fp64);
-/* Mixed-precision sketch: Q (m x N l, FP64) := (A_hi + A_lo) * Omega with
- * Omega' given in BF16 (L x n, pitch ldo).  Synchronizes.                    */
+                                        const uint16_t* a_lo, const uint16_t* a_lo2, int64_t lda, const uint16_t* b,
+                                        int64_t ldb, void* D, int64_t ldd, int out_fp64);
+/* Mixed-precision sketch: Q (m x N l, FP64) := (A_hi + A_lo + A_lo2) * Omega
+ * with Omega' given in BF16 (L x n, pitch ldo).  Synchronizes.               */
 MCNLA_B200_API int mcnla_b200_sketch_bf16(mcnla_b200_ctx* ctx, const mcnla_b200_params* params, const uint16_t* a_hi,
-                                          const uint16_t* a_lo, int64_t lda16, const uint16_t* omega_t, int64_t ldo,
-                                          double* Q);
+                                          const uint16_t* a_lo, const uint16_t* a_lo2, int64_t lda16,
+                                          const uint16_t* omega_t, int64_t ldo, double* Q);
 /* Whole solve with the mixed-precision sketch (Omega drawn in BF16 from seed)
  * and FP64 orthogonalizer, integrator and former (the former reads the FP64
- * A).  a_lo may be NULL (BF16 A_hi alone).                                   */
+ * A).  a_lo, a_lo2 may be NULL (fewer parts of A).                           */
 MCNLA_B200_API int mcnla_b200_isvd_mixed(mcnla_b200_ctx* ctx, const mcnla_b200_params* params, int integrator,
                                          int former, const double* A, int a_layout, int64_t lda, const uint16_t* a_hi,
-                                         const uint16_t* a_lo, int64_t lda16, uint64_t seed, int max_iteration,
-                                         double tolerance, double* S, double* U, double* V, int* iteration);
+                                         const uint16_t* a_lo, const uint16_t* a_lo2, int64_t lda16, uint64_t seed,
+                                         int max_iteration, double tolerance, double* S, double* U, double* V,
+                                         int* iteration);
 
 /* ---- batched and served solves ----------------------------------------------
  * Many independent solves of uneven sizes share the GPU: a pool of workers,
@@ -233,6 +236,7 @@ MCNLA_B200_API int mcnla_b200_isvd_mixed(mcnla_b200_ctx* ctx, const mcnla_b200_p
  * this has no counterpart there.)                                            */
 #define MCNLA_B200_PRECISION_FP64  0   /* FP64 sketch (plain path) */
 #define MCNLA_B200_PRECISION_MIXED 1   /* BF16 hi+lo tcgen05 sketch, FP64 elsewhere */
+#define MCNLA_B200_PRECISION_MIXED3 2  /* BF16 hi+lo+lo2 (24 bits: exact for FP32 A) */
 
 typedef struct mcnla_b200_problem {
   mcnla_b200_params params;

@@ -5,18 +5,19 @@
 
 namespace mb {
 
-// D (M x N) = (A_hi + A_lo) * B', all BF16 K-major (row pitch in elements,
-// multiple of 8), FP32 accumulation on tcgen05; D is FP64 (out_fp64) or FP32
-// row-major with leading dimension ldd.  a_lo may be null (one part).
-// Device-side wait timeouts are reported in c->scal->status.
-int bf16_gemm(Context* c, int64_t M, int64_t N, int64_t K, const uint16_t* a_hi, const uint16_t* a_lo, int64_t lda,
-              const uint16_t* b, int64_t ldb, void* D, int64_t ldd, bool out_fp64);
+// D (M x N) = (A_hi + A_lo + A_lo2) * B', all BF16 K-major (row pitch in
+// elements, multiple of 8), FP32 accumulation on tcgen05; D is FP64
+// (out_fp64) or FP32 row-major with leading dimension ldd.  a_lo, a_lo2 may
+// be null (fewer parts; a_lo2 only with a_lo).  Device-side wait timeouts
+// are reported in c->scal->status.
+int bf16_gemm(Context* c, int64_t M, int64_t N, int64_t K, const uint16_t* a_hi, const uint16_t* a_lo,
+              const uint16_t* a_lo2, int64_t lda, const uint16_t* b, int64_t ldb, void* D, int64_t ldd, bool out_fp64);
 
-// hi := bf16(A), lo := bf16(A - hi) (lo may be null), written row-major (K
-// contiguous) with pitch ldo, from row-major (layout 0) or column-major
-// (layout 1) FP64 A.
+// hi := bf16(A), lo := bf16(A - hi), lo2 := bf16(A - hi - lo) (lo, lo2 may be
+// null), written row-major (K contiguous) with pitch ldo, from row-major
+// (layout 0) or column-major (layout 1) FP64 A.
 int launch_split_bf16(Context* c, const double* A, int layout, int64_t lda, int64_t m, int64_t n, uint16_t* hi,
-                      uint16_t* lo, int64_t ldo);
+                      uint16_t* lo, uint16_t* lo2, int64_t ldo);
 
 // Omega' in BF16 (L x n, pitch ldo) from the same Philox stream as the FP64
 // generator (element (i, j) of the n x L Omega is sample i L + j), rounded to

@@ -11,30 +11,34 @@ namespace {
 
 __device__ __forceinline__ uint16_t bf16_bits(__nv_bfloat16 h) { return *reinterpret_cast<uint16_t*>(&h); }
 
-// hi = bf16(x) (round to nearest even), lo = bf16(x - hi)
-__device__ __forceinline__ void split(double x, uint16_t& hi, uint16_t& lo) {
+// hi = bf16(x), lo = bf16(x - hi), lo2 = bf16(x - hi - lo) (round to nearest
+// even; the differences are exact in FP64)
+__device__ __forceinline__ void split(double x, uint16_t& hi, uint16_t& lo, uint16_t& lo2) {
   const __nv_bfloat16 h = __double2bfloat16(x);
   hi = bf16_bits(h);
   const double r = x - double(__bfloat162float(h));
-  lo = bf16_bits(__double2bfloat16(r));
+  const __nv_bfloat16 l = __double2bfloat16(r);
+  lo = bf16_bits(l);
+  lo2 = bf16_bits(__double2bfloat16(r - double(__bfloat162float(l))));
 }
 
 __global__ void k_split_rowmajor(const double* A, int64_t lda, int64_t m, int64_t n, uint16_t* hi, uint16_t* lo,
-                                 int64_t ldo) {
+                                 uint16_t* lo2, int64_t ldo) {
   const int64_t total = m * n;
   for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x) {
     const int64_t i = e / n, j = e % n;
-    uint16_t h, l;
-    split(A[i * lda + j], h, l);
+    uint16_t h, l, l2;
+    split(A[i * lda + j], h, l, l2);
     hi[i * ldo + j] = h;
     if (lo) lo[i * ldo + j] = l;
+    if (lo2) lo2[i * ldo + j] = l2;
   }
 }
 
 // column-major A (element (i, j) at A[i + j lda]) to row-major hi/lo through
 // 32 x 32 shared-memory tiles (coalesced on both sides)
 __global__ void k_split_colmajor(const double* A, int64_t lda, int64_t m, int64_t n, uint16_t* hi, uint16_t* lo,
-                                 int64_t ldo) {
+                                 uint16_t* lo2, int64_t ldo) {
   __shared__ double tile[32][33];
   const int64_t i0 = int64_t(blockIdx.x) * 32, j0 = int64_t(blockIdx.y) * 32;
   const int tx = threadIdx.x, ty = threadIdx.y;   // 32 x 8
@@ -46,10 +50,11 @@ __global__ void k_split_colmajor(const double* A, int64_t lda, int64_t m, int64_
   for (int r = ty; r < 32; r += 8) {
     const int64_t i = i0 + r, j = j0 + tx;
     if (i < m && j < n) {
-      uint16_t h, l;
-      split(tile[tx][r], h, l);
+      uint16_t h, l, l2;
+      split(tile[tx][r], h, l, l2);
       hi[i * ldo + j] = h;
       if (lo) lo[i * ldo + j] = l;
+      if (lo2) lo2[i * ldo + j] = l2;
     }
   }
 }
@@ -84,16 +89,16 @@ __global__ void k_gaussian_bf16(uint64_t seed, int64_t n, int64_t L, uint16_t* o
 }  // namespace
 
 int launch_split_bf16(Context* c, const double* A, int layout, int64_t lda, int64_t m, int64_t n, uint16_t* hi,
-                      uint16_t* lo, int64_t ldo) {
+                      uint16_t* lo, uint16_t* lo2, int64_t ldo) {
   if (m <= 0 || n <= 0) return MCNLA_B200_OK;
   if (layout == MCNLA_B200_ROW_MAJOR) {
     const int64_t total = m * n;
     const int blocks = int(std::min<int64_t>(cdiv(total, 256), int64_t(c->num_sms) * 32));
-    k_split_rowmajor<<<blocks, 256, 0, c->stream>>>(A, lda, m, n, hi, lo, ldo);
+    k_split_rowmajor<<<blocks, 256, 0, c->stream>>>(A, lda, m, n, hi, lo, lo2, ldo);
   } else {
     dim3 grid(unsigned(cdiv(m, 32)), unsigned(cdiv(n, 32)));
     if (grid.y > 65535) return MCNLA_B200_ERR_SHAPE;
-    k_split_colmajor<<<grid, dim3(32, 8), 0, c->stream>>>(A, lda, m, n, hi, lo, ldo);
+    k_split_colmajor<<<grid, dim3(32, 8), 0, c->stream>>>(A, lda, m, n, hi, lo, lo2, ldo);
   }
   c->kernels_launched++;
   MB_CHECK_CUDA(cudaGetLastError());

@@ -3,8 +3,9 @@
 //
 //   D (M x N, FP64 or FP32, row-major) = sum_p A_p (M x K, BF16, K-major) * B (N x K, BF16, K-major)'
 //
-// with p over one or two parts of A (A = A_hi + A_lo, both BF16: 16 bits of
-// mantissa in total) and FP32 accumulation in tensor memory.
+// with p over one to three parts of A (A = A_hi + A_lo + A_lo2, all BF16: 8,
+// 16 or 24 bits of mantissa in total) and FP32 accumulation in tensor memory.
+// The parts extend the K loop: the same B tiles are streamed once per part.
 //
 // One CTA computes a 128 x 256 tile of D: warp 0 (one lane) streams 128 x 64
 // and 256 x 64 BF16 tiles of A and B into a 4-stage shared-memory ring with
@@ -43,7 +44,7 @@ constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(BN >>
 struct Args {
   int M, N;
   int KT;          // k-tiles per part of A
-  int parts;       // 1 (A_hi) or 2 (A_hi + A_lo)
+  int parts;       // 1 (A_hi), 2 (A_hi + A_lo) or 3 (A_hi + A_lo + A_lo2)
   void* D;
   int64_t ldd;
   int* status;     // device status word: set to MCNLA_B200_ERR_DEVICE_TIMEOUT on a run-out wait
@@ -132,6 +133,7 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
 template <class OutT>
 __global__ void __launch_bounds__(THREADS, 1) bf16_gemm_kernel(const __grid_constant__ CUtensorMap tm_a_hi,
                                                                const __grid_constant__ CUtensorMap tm_a_lo,
+                                                               const __grid_constant__ CUtensorMap tm_a_lo2,
                                                                const __grid_constant__ CUtensorMap tm_b, Args g) {
   extern __shared__ uint8_t smem_dyn[];
   __shared__ __align__(8) uint64_t full_bar[STAGES];
@@ -175,7 +177,7 @@ __global__ void __launch_bounds__(THREADS, 1) bf16_gemm_kernel(const __grid_cons
       uint8_t* sb = sa + A_TILE_BYTES;
       const int part = kt / g.KT, kk = kt % g.KT;
       mbar_expect_tx(&full_bar[s], STAGE_BYTES);
-      tma_load_2d(sa, part ? &tm_a_lo : &tm_a_hi, &full_bar[s], kk * BK, m0);
+      tma_load_2d(sa, part == 0 ? &tm_a_hi : (part == 1 ? &tm_a_lo : &tm_a_lo2), &full_bar[s], kk * BK, m0);
       tma_load_2d(sb, &tm_b, &full_bar[s], kk * BK, n0);
       ++issued;
     }
@@ -274,24 +276,27 @@ int make_map(CUtensorMap* map, const void* base, int64_t rows, int64_t cols, int
 
 }  // namespace
 
-int bf16_gemm(Context* c, int64_t M, int64_t N, int64_t K, const uint16_t* a_hi, const uint16_t* a_lo, int64_t lda,
-              const uint16_t* b, int64_t ldb, void* D, int64_t ldd, bool out_fp64) {
+int bf16_gemm(Context* c, int64_t M, int64_t N, int64_t K, const uint16_t* a_hi, const uint16_t* a_lo,
+              const uint16_t* a_lo2, int64_t lda, const uint16_t* b, int64_t ldb, void* D, int64_t ldd, bool out_fp64) {
   if (M <= 0 || N <= 0 || K <= 0) return MCNLA_B200_ERR_SHAPE;
   if (M > (int64_t(1) << 31) - 1 || N > (int64_t(1) << 31) - 1) return MCNLA_B200_ERR_SHAPE;
   // TMA: 16-byte aligned bases and row pitches
   auto al16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
-  if (!al16(a_hi) || (a_lo && !al16(a_lo)) || !al16(b) || (lda * 2) % 16 || (ldb * 2) % 16)
+  if (a_lo2 && !a_lo) return MCNLA_B200_ERR_ARG;
+  if (!al16(a_hi) || (a_lo && !al16(a_lo)) || (a_lo2 && !al16(a_lo2)) || !al16(b) || (lda * 2) % 16 ||
+      (ldb * 2) % 16)
     return MCNLA_B200_ERR_LAYOUT;
   if (lda < K || ldb < K) return MCNLA_B200_ERR_SHAPE;
-  CUtensorMap ta_hi, ta_lo, tb;
+  CUtensorMap ta_hi, ta_lo, ta_lo2, tb;
   MB_CHECK(make_map(&ta_hi, a_hi, M, K, lda, BM));
   MB_CHECK(make_map(&ta_lo, a_lo ? a_lo : a_hi, M, K, lda, BM));
+  MB_CHECK(make_map(&ta_lo2, a_lo2 ? a_lo2 : a_hi, M, K, lda, BM));
   MB_CHECK(make_map(&tb, b, N, K, ldb, BN));
   Args g;
   g.M = int(M);
   g.N = int(N);
   g.KT = int(cdiv(K, BK));
-  g.parts = a_lo ? 2 : 1;
+  g.parts = a_lo2 ? 3 : (a_lo ? 2 : 1);
   g.D = D;
   g.ldd = ldd;
   g.status = &c->scal->status;
@@ -300,11 +305,11 @@ int bf16_gemm(Context* c, int64_t M, int64_t N, int64_t K, const uint16_t* a_hi,
   if (out_fp64) {
     MB_CHECK_CUDA(cudaFuncSetAttribute(bf16_gemm_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        int(SMEM_BYTES)));
-    bf16_gemm_kernel<double><<<grid, THREADS, SMEM_BYTES, c->stream>>>(ta_hi, ta_lo, tb, g);
+    bf16_gemm_kernel<double><<<grid, THREADS, SMEM_BYTES, c->stream>>>(ta_hi, ta_lo, ta_lo2, tb, g);
   } else {
     MB_CHECK_CUDA(cudaFuncSetAttribute(bf16_gemm_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        int(SMEM_BYTES)));
-    bf16_gemm_kernel<float><<<grid, THREADS, SMEM_BYTES, c->stream>>>(ta_hi, ta_lo, tb, g);
+    bf16_gemm_kernel<float><<<grid, THREADS, SMEM_BYTES, c->stream>>>(ta_hi, ta_lo, ta_lo2, tb, g);
   }
   c->kernels_launched++;
   MB_CHECK_CUDA(cudaGetLastError());

@@ -28,6 +28,7 @@ struct KArgs {
   int64_t kps;
   const int* guard_stop;   // skip the launch when *guard_stop < guard_it
   int guard_it;
+  int lower;               // 1: only tiles touching the lower triangle (row >= column) are computed
 };
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes) {
@@ -136,6 +137,7 @@ __global__ void __launch_bounds__(C::THREADS) dgemm_kernel(KArgs g) {
 
   const int64_t n0 = int64_t(blockIdx.x) * C::BN;
   const int64_t m0 = int64_t(blockIdx.y) * C::BM;
+  if (g.lower && n0 >= m0 + C::BM) return;        // every element of the tile has column > row
   const int bz = blockIdx.z / g.splits;
   const int split = blockIdx.z % g.splits;
   const double* A = g.A + bz * g.a_bs;
@@ -231,7 +233,7 @@ __global__ void __launch_bounds__(C::THREADS) dgemm_kernel(KArgs g) {
 
 __global__ void splitk_reduce_kernel(const double* ws, int splits, int batch, int64_t M, int64_t N, double alpha,
                                      double beta, double* C, int64_t c_rs, int64_t c_cs, int64_t c_bs,
-                                     const int* guard_stop, int guard_it) {
+                                     const int* guard_stop, int guard_it, int lower) {
   if (guard_stop && *guard_stop < guard_it) return;
   const int64_t MN = M * N;
   const int64_t total = MN * batch;
@@ -239,6 +241,7 @@ __global__ void splitk_reduce_kernel(const double* ws, int splits, int batch, in
        idx += int64_t(gridDim.x) * blockDim.x) {
     const int64_t b = idx / MN, e = idx % MN;
     const int64_t r = e / N, c = e % N;
+    if (lower && c > r) continue;
     const double* w = ws + b * splits * MN + e;
     double s = 0.0;
     for (int k = 0; k < splits; ++k) s += w[k * MN];
@@ -321,7 +324,7 @@ size_t dgemm_workspace_bytes(const Context* c, int64_t M, int64_t N, int64_t K, 
 }
 
 int dgemm(Context* ctx, int64_t M, int64_t N, int64_t K, double alpha, CMat A, CMat B, double beta, DMat Cm,
-          GemmBatch batch, double* ws, int force_splits) {
+          GemmBatch batch, double* ws, int force_splits, bool lower_only) {
   if (M < 0 || N < 0 || K < 0 || batch.count < 1) return MCNLA_B200_ERR_SHAPE;
   if (M == 0 || N == 0) return MCNLA_B200_OK;
   bool AK, BKM;
@@ -342,6 +345,7 @@ int dgemm(Context* ctx, int64_t M, int64_t N, int64_t K, double alpha, CMat A, C
   g.ws = nullptr;
   g.guard_stop = ctx->guard_stop;
   g.guard_it = ctx->guard_it;
+  g.lower = lower_only ? 1 : 0;
   if (p.splits > 1) {
     const size_t need = size_t(p.splits) * batch.count * M * N * sizeof(double);
     if (!ws || ws != ctx->gws || need > ctx->gws_bytes) return MCNLA_B200_ERR_WORKSPACE;
@@ -363,7 +367,7 @@ int dgemm(Context* ctx, int64_t M, int64_t N, int64_t K, double alpha, CMat A, C
     const int blocks = int(std::min<int64_t>(cdiv(total, threads), int64_t(ctx->num_sms) * 8));
     splitk_reduce_kernel<<<blocks, threads, 0, ctx->stream>>>(ws, p.splits, batch.count, M, N, alpha, beta, Cm.p,
                                                              Cm.rs, Cm.cs, batch.c, ctx->guard_stop,
-                                                             ctx->guard_it);
+                                                             ctx->guard_it, g.lower);
     ctx->kernels_launched++;
     MB_CHECK_CUDA(cudaGetLastError());
   }

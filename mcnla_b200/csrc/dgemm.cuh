@@ -26,8 +26,10 @@ size_t dgemm_workspace_bytes(const Context* c, int64_t M, int64_t N, int64_t K, 
 
 // Launches C := alpha*A*B + beta*C on ctx->stream.  ws may be null when
 // dgemm_workspace_bytes() is 0.  force_splits > 0 overrides the split choice
-// (tests use it to cover the split-K path at small sizes).
+// (tests use it to cover the split-K path at small sizes).  lower_only: C is
+// square and only its lower triangle is needed (SYRK-like: tiles strictly
+// above the diagonal are skipped and the elements above it are unspecified).
 int dgemm(Context* ctx, int64_t M, int64_t N, int64_t K, double alpha, CMat A, CMat B, double beta, DMat C,
-          GemmBatch batch = GemmBatch(), double* ws = nullptr, int force_splits = 0);
+          GemmBatch batch = GemmBatch(), double* ws = nullptr, int force_splits = 0, bool lower_only = false);
 
 }  // namespace mb

@@ -53,6 +53,7 @@ int64_t problem_bytes(const mcnla_b200_problem& p) {
   bytes += stage + (int64_t(64) << 20);                                         // + split-K partials, small terms
   if (!p.A && p.A32) bytes += m * n * 8;                                        // FP64 copy of an FP32 A
   if (p.precision == MCNLA_B200_PRECISION_MIXED) bytes += 2 * m * round8(n) * 2 + L * round8(n) * 2;
+  if (p.precision == MCNLA_B200_PRECISION_MIXED3) bytes += 3 * m * round8(n) * 2 + L * round8(n) * 2;
   return bytes;
 }
 
@@ -80,6 +81,7 @@ int mcnla_b200_server::run(mcnla_b200_ctx* ctx, mcnla_b200_problem& p, double*& 
                            uint16_t*& split, size_t& split_bytes) {
   const int64_t m = p.params.nrow, n = p.params.ncol;
   if (m <= 0 || n <= 0) return MCNLA_B200_ERR_SHAPE;
+  if (p.precision < MCNLA_B200_PRECISION_FP64 || p.precision > MCNLA_B200_PRECISION_MIXED3) return MCNLA_B200_ERR_ARG;
   const double* A = p.A;
   int layout = p.a_layout;
   int64_t lda = p.lda;
@@ -100,9 +102,10 @@ int mcnla_b200_server::run(mcnla_b200_ctx* ctx, mcnla_b200_problem& p, double*& 
     A = a64;
     lda = cols;
   }
-  if (p.precision == MCNLA_B200_PRECISION_MIXED) {
+  if (p.precision == MCNLA_B200_PRECISION_MIXED || p.precision == MCNLA_B200_PRECISION_MIXED3) {
+    const int nparts = p.precision == MCNLA_B200_PRECISION_MIXED3 ? 3 : 2;
     const int64_t ldo = (n + 7) & ~int64_t(7);
-    const size_t need = 2 * size_t(m) * ldo * sizeof(uint16_t);
+    const size_t need = nparts * size_t(m) * ldo * sizeof(uint16_t);
     if (need > split_bytes) {
       if (split) MB_CHECK_CUDA(cudaFreeAsync(split, ctx->stream));
       split = nullptr;
@@ -112,8 +115,9 @@ int mcnla_b200_server::run(mcnla_b200_ctx* ctx, mcnla_b200_problem& p, double*& 
     }
     uint16_t* hi = split;
     uint16_t* lo = split + size_t(m) * ldo;
-    MB_CHECK(mcnla_b200_split_bf16(ctx, A, layout, lda, m, n, hi, lo, ldo));
-    return mcnla_b200_isvd_mixed(ctx, &p.params, p.integrator, p.former, A, layout, lda, hi, lo, ldo, p.seed,
+    uint16_t* lo2 = nparts == 3 ? split + 2 * size_t(m) * ldo : nullptr;
+    MB_CHECK(mcnla_b200_split_bf16(ctx, A, layout, lda, m, n, hi, lo, lo2, ldo));
+    return mcnla_b200_isvd_mixed(ctx, &p.params, p.integrator, p.former, A, layout, lda, hi, lo, lo2, ldo, p.seed,
                                  p.max_iteration, p.tolerance, p.S, p.U, p.V, &p.iteration);
   }
   return mcnla_b200_isvd(ctx, &p.params, p.integrator, p.former, A, layout, lda, nullptr, p.seed, p.max_iteration,

@@ -263,9 +263,11 @@ int run_rb_kn(Context* c, const Dims& d, const double* Qs, int maxit, double tol
   return MCNLA_B200_OK;
 }
 
-// Bs := Qs' Qs with the reference's triangle convention (see launch_gramian_prepare).
+// Bs := Qs' Qs with the reference's triangle convention (see launch_gramian_prepare):
+// the lower triangle only (the reference's syrk), mirrored afterwards.
 int gramian_bs(Context* c, const Dims& d, const double* Qs, double* Bs, double* Bc, int64_t ldbc, double* ws) {
-  MB_CHECK(dgemm(c, d.L, d.L, d.m, 1.0, cm(Qs, 1, d.L), crow(Qs, d.L), 0.0, drow(Bs, d.L), GemmBatch(), ws));
+  MB_CHECK(dgemm(c, d.L, d.L, d.m, 1.0, cm(Qs, 1, d.L), crow(Qs, d.L), 0.0, drow(Bs, d.L), GemmBatch(), ws, 0,
+                 true));
   MB_CHECK(launch_gramian_prepare(c, d.L, d.l, Bs, Bc, ldbc));
   return MCNLA_B200_OK;
 }
@@ -736,8 +738,8 @@ int run_isvd(Context* c, const Dims& d, int integrator, int former, const double
 
 // Mixed solve: Omega drawn in BF16, sketch on tcgen05, FP64 afterwards.
 int run_isvd_mixed(Context* c, const Dims& d, int integrator, int former, const double* A, int layout, int64_t lda,
-                   const uint16_t* a_hi, const uint16_t* a_lo, int64_t lda16, uint64_t seed, int maxit, double tol,
-                   double* S, double* U, double* V, int* iters, char* pbase) {
+                   const uint16_t* a_hi, const uint16_t* a_lo, const uint16_t* a_lo2, int64_t lda16, uint64_t seed,
+                   int maxit, double tol, double* S, double* U, double* V, int* iters, char* pbase) {
   auto take = [&](size_t bytes) {
     char* p = pbase;
     pbase += (bytes + 511) & ~size_t(511);
@@ -751,7 +753,7 @@ int run_isvd_mixed(Context* c, const Dims& d, int integrator, int former, const 
   MB_CHECK(ctx_tic(c));
   MB_CHECK(launch_gaussian_bf16(c, seed, d.n, d.L, omega_t, ldo, nullptr));
   MB_CHECK(ctx_toc(c));
-  MB_CHECK(bf16_gemm(c, d.m, d.L, d.n, a_hi, a_lo, lda16, omega_t, ldo, Q, d.L, true));
+  MB_CHECK(bf16_gemm(c, d.m, d.L, d.n, a_hi, a_lo, a_lo2, lda16, omega_t, ldo, Q, d.L, true));
   MB_CHECK(ctx_toc(c));
   MB_CHECK(run_orthogonalize(c, d, Q));
   MB_CHECK(run_integrate(c, d, integrator, Q, maxit, tol, Qbar, iters));
@@ -922,12 +924,12 @@ int mcnla_b200_inverse_batched(mcnla_b200_ctx* ctx, int n, int batch, double* A)
 }
 
 int mcnla_b200_split_bf16(mcnla_b200_ctx* ctx, const double* A, int a_layout, int64_t lda, int64_t m, int64_t n,
-                          uint16_t* hi, uint16_t* lo, int64_t ldo) {
-  if (!ctx || !A || !hi || m < 0 || n < 0) return MCNLA_B200_ERR_ARG;
+                          uint16_t* hi, uint16_t* lo, uint16_t* lo2, int64_t ldo) {
+  if (!ctx || !A || !hi || m < 0 || n < 0 || (lo2 && !lo)) return MCNLA_B200_ERR_ARG;
   if (a_layout != MCNLA_B200_ROW_MAJOR && a_layout != MCNLA_B200_COL_MAJOR) return MCNLA_B200_ERR_ARG;
   if (ldo < n || (a_layout == MCNLA_B200_ROW_MAJOR ? lda < n : lda < m)) return MCNLA_B200_ERR_SHAPE;
   MB_CHECK_CUDA(cudaSetDevice(ctx->device));
-  return mb::launch_split_bf16(ctx, A, a_layout, lda, m, n, hi, lo, ldo);
+  return mb::launch_split_bf16(ctx, A, a_layout, lda, m, n, hi, lo, lo2, ldo);
 }
 
 int mcnla_b200_gaussian_bf16(mcnla_b200_ctx* ctx, uint64_t seed, int64_t n, int64_t L, uint16_t* omega_t,
@@ -938,18 +940,19 @@ int mcnla_b200_gaussian_bf16(mcnla_b200_ctx* ctx, uint64_t seed, int64_t n, int6
 }
 
 int mcnla_b200_gemm_bf16(mcnla_b200_ctx* ctx, int64_t M, int64_t N, int64_t K, const uint16_t* a_hi,
-                         const uint16_t* a_lo, int64_t lda, const uint16_t* b, int64_t ldb, void* D, int64_t ldd,
-                         int out_fp64) {
+                         const uint16_t* a_lo, const uint16_t* a_lo2, int64_t lda, const uint16_t* b, int64_t ldb,
+                         void* D, int64_t ldd, int out_fp64) {
   if (!ctx || !a_hi || !b || !D || ldd < N) return MCNLA_B200_ERR_ARG;
   MB_CHECK_CUDA(cudaSetDevice(ctx->device));
   MB_CHECK_CUDA(cudaMemsetAsync(ctx->scal, 0, sizeof(mb::DevScalars), ctx->stream));
-  MB_CHECK(mb::bf16_gemm(ctx, M, N, K, a_hi, a_lo, lda, b, ldb, D, ldd, out_fp64 != 0));
+  MB_CHECK(mb::bf16_gemm(ctx, M, N, K, a_hi, a_lo, a_lo2, lda, b, ldb, D, ldd, out_fp64 != 0));
   MB_CHECK(mb::ctx_sync_scalars(ctx));
   return ctx->scal_host->status ? ctx->scal_host->status : MCNLA_B200_OK;
 }
 
 int mcnla_b200_sketch_bf16(mcnla_b200_ctx* ctx, const mcnla_b200_params* params, const uint16_t* a_hi,
-                           const uint16_t* a_lo, int64_t lda16, const uint16_t* omega_t, int64_t ldo, double* Q) {
+                           const uint16_t* a_lo, const uint16_t* a_lo2, int64_t lda16, const uint16_t* omega_t,
+                           int64_t ldo, double* Q) {
   if (!ctx || !a_hi || !omega_t || !Q) return MCNLA_B200_ERR_ARG;
   Dims d;
   MB_CHECK(mb::get_dims(params, d));
@@ -957,7 +960,7 @@ int mcnla_b200_sketch_bf16(mcnla_b200_ctx* ctx, const mcnla_b200_params* params,
   MB_CHECK_CUDA(cudaMemsetAsync(ctx->scal, 0, sizeof(mb::DevScalars), ctx->stream));
   MB_CHECK(mb::ctx_tic(ctx));
   MB_CHECK(mb::ctx_toc(ctx));
-  MB_CHECK(mb::bf16_gemm(ctx, d.m, d.L, d.n, a_hi, a_lo, lda16, omega_t, ldo, Q, d.L, true));
+  MB_CHECK(mb::bf16_gemm(ctx, d.m, d.L, d.n, a_hi, a_lo, a_lo2, lda16, omega_t, ldo, Q, d.L, true));
   MB_CHECK(mb::ctx_toc(ctx));
   MB_CHECK(mb::ctx_sync_scalars(ctx));
   return ctx->scal_host->status ? ctx->scal_host->status : MCNLA_B200_OK;
@@ -965,15 +968,16 @@ int mcnla_b200_sketch_bf16(mcnla_b200_ctx* ctx, const mcnla_b200_params* params,
 
 int mcnla_b200_isvd_mixed(mcnla_b200_ctx* ctx, const mcnla_b200_params* params, int integrator, int former,
                           const double* A, int a_layout, int64_t lda, const uint16_t* a_hi, const uint16_t* a_lo,
-                          int64_t lda16, uint64_t seed, int max_iteration, double tolerance, double* S, double* U,
-                          double* V, int* iteration) {
+                          const uint16_t* a_lo2, int64_t lda16, uint64_t seed, int max_iteration, double tolerance,
+                          double* S, double* U, double* V, int* iteration) {
   if (!ctx || !A || !a_hi || !iteration) return MCNLA_B200_ERR_ARG;
   Dims d;
   MB_CHECK(mb::get_dims(params, d));
   MB_CHECK_CUDA(cudaSetDevice(ctx->device));
   MB_CHECK(mb::ctx_reserve_pipeline(ctx, mb::pipeline_bytes_mixed(d)));
-  return mb::run_isvd_mixed(ctx, d, integrator, former, A, a_layout, lda, a_hi, a_lo, lda16, seed, max_iteration,
-                            tolerance, S, U, V, iteration, static_cast<char*>(ctx->parena));
+  if (a_lo2 && !a_lo) return MCNLA_B200_ERR_ARG;
+  return mb::run_isvd_mixed(ctx, d, integrator, former, A, a_layout, lda, a_hi, a_lo, a_lo2, lda16, seed,
+                            max_iteration, tolerance, S, U, V, iteration, static_cast<char*>(ctx->parena));
 }
 
 int mcnla_b200_syev_batched(mcnla_b200_ctx* ctx, int n, int batch, const double* A, double* W, double* V,

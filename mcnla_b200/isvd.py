@@ -34,7 +34,7 @@ __all__ = [
     "KolmogorovNagumoIntegrator", "RowBlockKolmogorovNagumoIntegrator", "RowBlockGramianKolmogorovNagumoIntegrator",
     "RowBlockWenYinIntegrator", "RowBlockGramianWenYinIntegrator",
     "SvdFormer", "GramianFormer", "RowBlockGramianFormer", "ColBlockGramianFormer",
-    "solve", "solve_host", "split_bf16", "gaussian_bf16", "gemm_bf16", "solve_mixed",
+    "solve", "solve_host", "Split", "split_bf16", "gaussian_bf16", "gemm_bf16", "solve_mixed",
     "Request", "Server", "solve_batched",
 ]
 
@@ -626,17 +626,38 @@ def _bf16_buffer(rows, cols, dev):
     return buf[:, :cols], ld
 
 
-def split_bf16(a, with_lo=True):
-    """A = A_hi + A_lo in BF16 (row-major views with 16-byte pitch).  Returns (hi, lo, pitch)."""
+class Split(tuple):
+    """BF16 parts of A: (hi, lo, lo2, pitch); lo / lo2 are None when not split out."""
+    __slots__ = ()
+
+    def __new__(cls, hi, lo, lo2, ld):
+        return tuple.__new__(cls, (hi, lo, lo2, ld))
+
+    hi = property(lambda self: self[0])
+    lo = property(lambda self: self[1])
+    lo2 = property(lambda self: self[2])
+    ld = property(lambda self: self[3])
+
+    @property
+    def parts(self):
+        return 1 + (self[1] is not None) + (self[2] is not None)
+
+
+def split_bf16(a, parts=2):
+    """A = A_hi + A_lo (+ A_lo2) in BF16 (row-major views with 16-byte pitch), parts in 1..3:
+    8, 16 or 24 bits of mantissa (three parts hold an FP32 A exactly).  Returns a Split."""
+    if parts not in (1, 2, 3):
+        raise ValueError("parts must be 1, 2 or 3")
     _check_dev(a, "A")
     layout, lda = _layout(a)
     m, n = a.shape
     hi, ld = _bf16_buffer(m, n, a.device)
-    lo = _bf16_buffer(m, n, a.device)[0] if with_lo else None
+    lo = _bf16_buffer(m, n, a.device)[0] if parts >= 2 else None
+    lo2 = _bf16_buffer(m, n, a.device)[0] if parts >= 3 else None
     ctx = context(a.device)
-    _lib.check(ctx.lib.mcnla_b200_split_bf16(ctx.bind(), _ptr(a), layout, lda, m, n, _ptr(hi), _ptr(lo), ld),
-               "split_bf16")
-    return hi, lo, ld
+    _lib.check(ctx.lib.mcnla_b200_split_bf16(ctx.bind(), _ptr(a), layout, lda, m, n, _ptr(hi), _ptr(lo), _ptr(lo2),
+                                             ld), "split_bf16")
+    return Split(hi, lo, lo2, ld)
 
 
 def gaussian_bf16(n, L, seed, device=None, with_fp64=False):
@@ -650,28 +671,28 @@ def gaussian_bf16(n, L, seed, device=None, with_fp64=False):
     return omega_t, ld, omega
 
 
-def gemm_bf16(a_hi, a_lo, lda, b, ldb, out_dtype=torch.float64):
-    """D = (A_hi + A_lo) B' on tcgen05 (BF16 in, FP32 accumulation)."""
+def gemm_bf16(a_hi, a_lo, lda, b, ldb, out_dtype=torch.float64, a_lo2=None):
+    """D = (A_hi + A_lo + A_lo2) B' on tcgen05 (BF16 in, FP32 accumulation)."""
     M, K = a_hi.shape
     N = b.shape[0]
     d = torch.empty(M, N, dtype=out_dtype, device=a_hi.device)
     ctx = context(a_hi.device)
-    _lib.check(ctx.lib.mcnla_b200_gemm_bf16(ctx.bind(), M, N, K, _ptr(a_hi), _ptr(a_lo), lda, _ptr(b), ldb, _ptr(d),
-                                            N, 1 if out_dtype == torch.float64 else 0), "gemm_bf16")
+    _lib.check(ctx.lib.mcnla_b200_gemm_bf16(ctx.bind(), M, N, K, _ptr(a_hi), _ptr(a_lo), _ptr(a_lo2), lda, _ptr(b),
+                                            ldb, _ptr(d), N, 1 if out_dtype == torch.float64 else 0), "gemm_bf16")
     return d
 
 
 def solve_mixed(a, k, p, N, seed=0, integrator="kn", former="svd", maxit=256, tol=1e-4, split=None, with_v=True,
-                with_lo=True):
+                parts=2):
     """Whole iSVD with the BF16 tensor-core sketch (Omega drawn in BF16 from seed) and FP64
-    orthogonalizer / integrator / former.  `split` = (hi, lo, pitch) reuses a resident BF16 copy.
-    Returns (S, U, V, iterations)."""
+    orthogonalizer / integrator / former.  `split` (a Split) reuses a resident BF16 copy of A;
+    otherwise A is split into `parts` BF16 parts.  Returns (S, U, V, iterations)."""
     m, n = a.shape
     _check_dev(a, "A")
     layout, lda = _layout(a)
     if split is None:
-        split = split_bf16(a, with_lo)
-    hi, lo, ld16 = split
+        split = split_bf16(a, parts)
+    hi, lo, lo2, ld16 = split
     prm = _lib.Params(m, n, k, p, N)
     dev = a.device
     s = torch.empty(k, dtype=torch.float64, device=dev)
@@ -680,7 +701,8 @@ def solve_mixed(a, k, p, N, seed=0, integrator="kn", former="svd", maxit=256, to
     ctx = context(dev)
     it = ctypes.c_int()
     _lib.check(ctx.lib.mcnla_b200_isvd_mixed(ctx.bind(), ctypes.byref(prm), INTEGRATORS[integrator], FORMERS[former],
-                                             _ptr(a), layout, lda, _ptr(hi), _ptr(lo), ld16, ctypes.c_uint64(seed),
+                                             _ptr(a), layout, lda, _ptr(hi), _ptr(lo), _ptr(lo2), ld16,
+                                             ctypes.c_uint64(seed),
                                              maxit, tol, _ptr(s), _ptr(u), _ptr(v), ctypes.byref(it)), "isvd_mixed")
     return s, u, v, it.value
 
@@ -690,7 +712,8 @@ def solve_mixed(a, k, p, N, seed=0, integrator="kn", former="svd", maxit=256, to
 # ----------------------------------------------------------------------------------------------
 class Request:
     """One solve for the server: A (CUDA float64 or float32, row- or column-major) and its
-    parameters; the outputs S, U, V are allocated here on A's device."""
+    parameters; the outputs S, U, V are allocated here on A's device.  mixed: False (FP64),
+    True or 2 (BF16 hi+lo sketch) or 3 (BF16 hi+lo+lo2 sketch)."""
 
     def __init__(self, a, k, p, N, seed=0, integrator="kn", former="svd", maxit=256, tol=1e-4, mixed=False,
                  with_v=True):
@@ -714,7 +737,14 @@ class Request:
         pr.former = FORMERS[former]
         pr.max_iteration = maxit
         pr.tolerance = tol
-        pr.precision = _lib.PRECISION_MIXED if mixed else _lib.PRECISION_FP64
+        if mixed is False or mixed is None or mixed == 0:
+            pr.precision = _lib.PRECISION_FP64
+        elif mixed is True or mixed == 2:
+            pr.precision = _lib.PRECISION_MIXED
+        elif mixed == 3:
+            pr.precision = _lib.PRECISION_MIXED3
+        else:
+            raise ValueError("mixed must be False, True, 2 or 3")
         pr.S = self.s.data_ptr()
         pr.U = self.u.data_ptr()
         pr.V = self.v.data_ptr() if self.v is not None else None

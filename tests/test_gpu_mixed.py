@@ -18,16 +18,19 @@ def _bf16_mat(rows, cols, dev, g, scale=1.0):
 
 
 @pytest.mark.parametrize("M,N,K,parts", [(128, 256, 64, 1), (300, 500, 1000, 1), (1000, 4096, 2000, 2),
-                                         (129, 257, 65, 2), (4096, 320, 2000, 1)])
+                                         (129, 257, 65, 2), (4096, 320, 2000, 1), (500, 300, 777, 3),
+                                         (1024, 512, 4096, 3)])
 def test_gemm_bf16_against_fp64(cuda, M, N, K, parts):
     from mcnla_b200 import isvd
     g = torch.Generator(device=cuda).manual_seed(M + N + K)
     a_hi, lda = _bf16_mat(M, K, cuda, g)
-    a_lo = _bf16_mat(M, K, cuda, g, 1e-3)[0] if parts == 2 else None
+    a_lo = _bf16_mat(M, K, cuda, g, 1e-3)[0] if parts >= 2 else None
+    a_lo2 = _bf16_mat(M, K, cuda, g, 1e-6)[0] if parts >= 3 else None
     b, ldb = _bf16_mat(N, K, cuda, g)
     for out in (torch.float64, torch.float32):
-        d = isvd.gemm_bf16(a_hi, a_lo, lda, b, ldb, out)
-        a64 = a_hi.double() + (a_lo.double() if a_lo is not None else 0)
+        d = isvd.gemm_bf16(a_hi, a_lo, lda, b, ldb, out, a_lo2=a_lo2)
+        a64 = a_hi.double() + (a_lo.double() if a_lo is not None else 0) + \
+            (a_lo2.double() if a_lo2 is not None else 0)
         ref = a64 @ b.double().t()
         bound = a64.abs() @ b.double().abs().t()
         err = (d.double() - ref).abs()
@@ -39,11 +42,19 @@ def test_split_bf16_layouts(cuda):
     g = torch.Generator(device=cuda).manual_seed(3)
     a = torch.randn(333, 517, generator=g, dtype=torch.float64, device=cuda)
     for view in (a, a.t().contiguous().t()):
-        hi, lo, ld = isvd.split_bf16(view)
+        hi, lo, lo2, ld = isvd.split_bf16(view, 3)
         assert ld % 8 == 0
         assert torch.equal(hi, a.to(torch.bfloat16))
         rec = hi.double() + lo.double()
         assert bool(torch.all((rec - a).abs() <= 2.0 ** -16 * a.abs() + 1e-300))
+        rec3 = rec + lo2.double()
+        assert bool(torch.all((rec3 - a).abs() <= 2.0 ** -24 * a.abs() + 1e-300))
+    # three parts hold an FP32 matrix exactly
+    a32 = a.float().double()
+    hi, lo, lo2, ld = isvd.split_bf16(a32, 3)
+    assert torch.equal(hi.double() + lo.double() + lo2.double(), a32)
+    two = isvd.split_bf16(a, 2)
+    assert two.lo2 is None and two.parts == 2
 
 
 def test_gaussian_bf16_matches_fp64_stream(cuda):
@@ -92,8 +103,12 @@ def test_mixed_matches_fp64_isvd(cuda, case):
     assert orth <= 1e-10, orth
     # hi-only sketch: coarser (8-bit A), reported not asserted to 1e-6
     s1, _, _, _ = isvd.solve_mixed(at, k, p, N, seed=seed, integrator="rb_gramian_kn", former="svd", tol=1e-6,
-                                   with_lo=False)
+                                   parts=1)
     rel1 = np.max(np.abs(s1.cpu().numpy() - s64.cpu().numpy()) / s64.cpu().numpy())
-    print("%s: sigma rel err hi+lo %.2e (hi only %.2e), max principal angle %.2e, ||U'U-I|| %.2e, it %d/%d"
-          % (case, rel, rel1, ang, orth, it, it64))
+    s3, _, _, _ = isvd.solve_mixed(at, k, p, N, seed=seed, integrator="rb_gramian_kn", former="svd", tol=1e-6,
+                                   parts=3)
+    rel3 = np.max(np.abs(s3.cpu().numpy() - s64.cpu().numpy()) / s64.cpu().numpy())
+    print("%s: sigma rel err hi+lo %.2e (hi only %.2e, hi+lo+lo2 %.2e), max principal angle %.2e, ||U'U-I|| %.2e, "
+          "it %d/%d" % (case, rel, rel1, rel3, ang, orth, it, it64))
     assert rel1 <= 1e-2
+    assert rel3 <= 1e-6, rel3

@@ -22,7 +22,7 @@ def _problems(cuda, count=10, seed=0):
         at = torch.as_tensor(a, device=cuda).to(dtype)
         if i % 4 == 3:
             at = at.t().contiguous().t()          # column-major
-        mixed = i % 2 == 1
+        mixed = (False, True, False, 3)[i % 4]
         integ = ["kn", "rb_gramian_kn", "rb_gramian_wy", "rb_kn"][i % 4]
         reqs.append(isvd.Request(at, k, p, N, seed=1000 + i, integrator=integ, former="svd", tol=1e-5,
                                  mixed=mixed))
@@ -36,8 +36,8 @@ def _alone(req):
     integ = {v: k for k, v in isvd.INTEGRATORS.items()}[pr.integrator]
     args = dict(seed=pr.seed, integrator=integ, former="svd", maxit=pr.max_iteration, tol=pr.tolerance)
     k, p, N = pr.params.rank, pr.params.over_rank, pr.params.num_sketch
-    if pr.precision == 1:
-        return isvd.solve_mixed(a, k, p, N, **args)
+    if pr.precision in (1, 2):
+        return isvd.solve_mixed(a, k, p, N, parts=pr.precision + 1, **args)
     return isvd.solve(a, k, p, N, **args)
 
 
