@@ -4,18 +4,30 @@
 //   D (M x N, FP64 or FP32, row-major) = sum_p A_p (M x K, BF16, K-major) * B (N x K, BF16, K-major)'
 //
 // with p over one to three parts of A (A = A_hi + A_lo + A_lo2, all BF16: 8,
-// 16 or 24 bits of mantissa in total) and FP32 accumulation in tensor memory.
-// The parts extend the K loop: the same B tiles are streamed once per part.
+// 16 or 24 bits of mantissa in total).  A stage of the shared-memory ring holds
+// the k-tile of every part of A and one k-tile of B, so B is streamed once
+// whatever the number of parts, and the MMAs of all parts accumulate from it.
 //
-// One CTA computes a 128 x 256 tile of D: warp 0 (one lane) streams 128 x 64
-// and 256 x 64 BF16 tiles of A and B into a 4-stage shared-memory ring with
-// TMA (128-byte swizzle), warp 1 (one lane) issues tcgen05.mma (M=128, N=256,
-// K=16, four per stage) into a 256-column TMEM accumulator and releases each
-// stage with tcgen05.commit, and warps 4-7 read the accumulator back with
-// tcgen05.ld (one TMEM lane = one row per thread) and store D.  Every
-// mbarrier wait is bounded: when one runs out the kernel records the fact in
-// a device status word, lets the work already in flight drain (also with
-// bounded waits) and frees its TMEM before returning.
+// Warp 0 (one lane) streams 128 x 64 BF16 tiles of A and BN x 64 tiles of B
+// into a 3-stage shared-memory ring (64 KB stages) with TMA (128-byte
+// swizzle); warp 1 (one lane) issues tcgen05.mma (M = 128, N = BN, K = 16,
+// four per part per stage) and releases each stage with tcgen05.commit.  Two
+// tile configurations:
+//   wide     (one or two parts): a 128 x 256 tile per CTA, one FP32 TMEM
+//            accumulator over the whole K loop, read back by warps 4-7 (one
+//            TMEM lane quarter each) and stored;
+//   chunked  (three parts): the tensor cores accumulate in FP32 and the
+//            error of a long sum is no longer small next to the 24-bit
+//            representation of A, so the K loop is cut into chunks of 3
+//            k-tiles (36 MMAs of K = 16 over the three parts: 576 products
+//            per element).  A 128 x 128 tile per CTA; chunks alternate
+//            between two 128-column TMEM
+//            accumulators, and warps 2-9 (two per TMEM lane quarter, 64
+//            columns each) add every finished chunk into FP64 registers while
+//            the next chunk is accumulated; D is stored once at the end.
+// Every mbarrier wait is bounded: when one runs out the kernel records the
+// fact in a device status word, lets the work already in flight drain (also
+// with bounded waits) and frees its TMEM before returning.
 #include "common.cuh"
 #include "bf16.cuh"
 
@@ -28,22 +40,30 @@
 namespace mb {
 namespace {
 
-constexpr int BM = 128, BN = 256, BK = 64, STAGES = 4;
+constexpr int BM = 128, BK = 64;
 constexpr int A_TILE_BYTES = BM * BK * 2;                 // 16 KB
-constexpr int B_TILE_BYTES = BN * BK * 2;                 // 32 KB
-constexpr int STAGE_BYTES = A_TILE_BYTES + B_TILE_BYTES;  // 48 KB
-constexpr uint32_t TMEM_COLS = 256;
-constexpr int THREADS = 256;
-constexpr size_t SMEM_BYTES = size_t(STAGES) * STAGE_BYTES + 1024;   // + alignment slack
+constexpr int CHUNK_KT = 3;                               // k-tiles per FP32 accumulation chunk (chunked)
+constexpr int MAX_PARTS = 3;
 constexpr long long kWaitCycles = 4000000000LL;           // ~2 s at 2 GHz: a bounded wait
 
-// instruction descriptor, kind::f16: D f32, A bf16, B bf16, both K-major, M=128, N=256
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(BN >> 3) << 17) |
-                            (uint32_t(BM >> 4) << 24);
+template <bool CHUNKED>
+struct TileCfg {
+  static constexpr int BN = CHUNKED ? 128 : 256;
+  static constexpr int STAGES = 3;
+  static constexpr int A_PARTS = CHUNKED ? 3 : 2;                   // A tiles per stage
+  static constexpr int B_TILE_BYTES = BN * BK * 2;
+  static constexpr int STAGE_BYTES = A_PARTS * A_TILE_BYTES + B_TILE_BYTES;   // 64 KB
+  static constexpr uint32_t TMEM_COLS = CHUNKED ? 2 * BN : BN;      // two accumulators / one
+  static constexpr int THREADS = CHUNKED ? 320 : 256;              // epilogue warps 2-9 / 4-7
+  static constexpr size_t SMEM_BYTES = size_t(STAGES) * STAGE_BYTES + 1024;   // + alignment slack
+  // instruction descriptor, kind::f16: D f32, A bf16, B bf16, both K-major, M = 128, N = BN
+  static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(BN >> 3) << 17) |
+                                    (uint32_t(BM >> 4) << 24);
+};
 
 struct Args {
   int M, N;
-  int KT;          // k-tiles per part of A
+  int KT;          // k-tiles
   int parts;       // 1 (A_hi), 2 (A_hi + A_lo) or 3 (A_hi + A_lo + A_lo2)
   void* D;
   int64_t ldd;
@@ -101,12 +121,13 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
   return d;
 }
 
-__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-      ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate));
+      ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
 
 __device__ __forceinline__ void umma_commit(uint64_t* bar) {
@@ -128,27 +149,50 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
         "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
       : "r"(taddr));
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+  // the values are read only after the wait (register dependencies on a volatile asm)
+#pragma unroll
+  for (int j = 0; j < 32; ++j) asm volatile("" : "+r"(r[j]));
 }
 
-template <class OutT>
-__global__ void __launch_bounds__(THREADS, 1) bf16_gemm_kernel(const __grid_constant__ CUtensorMap tm_a_hi,
-                                                               const __grid_constant__ CUtensorMap tm_a_lo,
-                                                               const __grid_constant__ CUtensorMap tm_a_lo2,
-                                                               const __grid_constant__ CUtensorMap tm_b, Args g) {
+// The same load without the wait: the caller issues tcgen05.wait::ld before
+// reading r.
+__device__ __forceinline__ void tmem_ld32_nowait(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+}
+
+template <class OutT, bool CHUNKED>
+__global__ void __launch_bounds__(TileCfg<CHUNKED>::THREADS, 1)
+    bf16_gemm_kernel(const __grid_constant__ CUtensorMap tm_a_hi, const __grid_constant__ CUtensorMap tm_a_lo,
+                     const __grid_constant__ CUtensorMap tm_a_lo2, const __grid_constant__ CUtensorMap tm_b, Args g) {
+  using T = TileCfg<CHUNKED>;
+  constexpr int BN = T::BN, STAGES = T::STAGES, STAGE_BYTES = T::STAGE_BYTES;
   extern __shared__ uint8_t smem_dyn[];
   __shared__ __align__(8) uint64_t full_bar[STAGES];
   __shared__ __align__(8) uint64_t empty_bar[STAGES];
-  __shared__ __align__(8) uint64_t accum_bar;
+  __shared__ __align__(8) uint64_t acc_full[2];     // a chunk is in accumulator b
+  __shared__ __align__(8) uint64_t acc_empty[2];    // accumulator b has been read
+  __shared__ __align__(8) uint64_t mma_done;
   __shared__ uint32_t tmem_base_s;
 
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_dyn) + 1023) & ~uintptr_t(1023));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int n0 = blockIdx.x * BN, m0 = blockIdx.y * BM;
-  const int total_kt = g.KT * g.parts;
+  const int total_kt = g.KT;
+  const int chunk_kt = CHUNKED ? CHUNK_KT : total_kt;
+  const int chunks = (total_kt + chunk_kt - 1) / chunk_kt;
+  constexpr int EPI_WARPS = CHUNKED ? 8 : 4;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_s)),
-                 "r"(TMEM_COLS));
+                 "r"(T::TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (threadIdx.x == 32) {
@@ -156,7 +200,11 @@ __global__ void __launch_bounds__(THREADS, 1) bf16_gemm_kernel(const __grid_cons
       mbar_init(&full_bar[s], 1);
       mbar_init(&empty_bar[s], 1);
     }
-    mbar_init(&accum_bar, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b], EPI_WARPS);
+    }
+    mbar_init(&mma_done, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   fence_before();
@@ -174,11 +222,12 @@ __global__ void __launch_bounds__(THREADS, 1) bf16_gemm_kernel(const __grid_cons
       const int s = kt % STAGES;
       if (kt >= STAGES && !mbar_wait(&empty_bar[s], ((kt / STAGES) & 1) ^ 1)) { ok = false; break; }
       uint8_t* sa = smem + s * STAGE_BYTES;
-      uint8_t* sb = sa + A_TILE_BYTES;
-      const int part = kt / g.KT, kk = kt % g.KT;
-      mbar_expect_tx(&full_bar[s], STAGE_BYTES);
-      tma_load_2d(sa, part == 0 ? &tm_a_hi : (part == 1 ? &tm_a_lo : &tm_a_lo2), &full_bar[s], kk * BK, m0);
-      tma_load_2d(sb, &tm_b, &full_bar[s], kk * BK, n0);
+      uint8_t* sb = sa + T::A_PARTS * A_TILE_BYTES;
+      mbar_expect_tx(&full_bar[s], uint32_t(g.parts * A_TILE_BYTES + T::B_TILE_BYTES));
+      tma_load_2d(sa, &tm_a_hi, &full_bar[s], kt * BK, m0);
+      if (g.parts > 1) tma_load_2d(sa + A_TILE_BYTES, &tm_a_lo, &full_bar[s], kt * BK, m0);
+      if (g.parts > 2) tma_load_2d(sa + 2 * A_TILE_BYTES, &tm_a_lo2, &full_bar[s], kt * BK, m0);
+      tma_load_2d(sb, &tm_b, &full_bar[s], kt * BK, n0);
       ++issued;
     }
     if (!ok) {
@@ -191,31 +240,88 @@ __global__ void __launch_bounds__(THREADS, 1) bf16_gemm_kernel(const __grid_cons
     // ---- MMA issuer
     for (int kt = 0; kt < total_kt; ++kt) {
       const int s = kt % STAGES;
+      const int c = kt / chunk_kt, b = c & 1;
+      const bool first = kt % chunk_kt == 0;
+      if (first && c >= 2) {
+        // accumulator b must have been read (chunk c - 2)
+        if (!mbar_wait(&acc_empty[b], ((c >> 1) - 1) & 1)) { atomicExch(g.status, MCNLA_B200_ERR_DEVICE_TIMEOUT); break; }
+        fence_after();
+      }
       if (!mbar_wait(&full_bar[s], (kt / STAGES) & 1)) { atomicExch(g.status, MCNLA_B200_ERR_DEVICE_TIMEOUT); break; }
       fence_after();
       const uint32_t sa = smem_u32(smem + s * STAGE_BYTES);
-      const uint32_t sb = sa + A_TILE_BYTES;
+      const uint32_t sb = sa + T::A_PARTS * A_TILE_BYTES;
+      for (int part = 0; part < g.parts; ++part) {
 #pragma unroll
-      for (int k = 0; k < BK / 16; ++k)   // 16 BF16 = 32 bytes along K per MMA
-        umma_bf16(tmem, sw128_desc(sa + k * 32), sw128_desc(sb + k * 32), (kt | k) != 0);
+        for (int k = 0; k < BK / 16; ++k)   // 16 BF16 = 32 bytes along K per MMA
+          umma_bf16(tmem + uint32_t(b * BN), sw128_desc(sa + part * A_TILE_BYTES + k * 32), sw128_desc(sb + k * 32),
+                    T::IDESC, !(first && part == 0 && k == 0));
+      }
       umma_commit(&empty_bar[s]);        // the stage is free once these MMAs have read it
+      if (kt % chunk_kt == chunk_kt - 1 || kt == total_kt - 1) umma_commit(&acc_full[b]);
     }
-    umma_commit(&accum_bar);             // all MMAs issued so far are complete
-  } else if (warp >= 4) {
-    // ---- epilogue: TMEM -> registers -> global
-    const int ew = warp - 4;             // TMEM lanes [32 ew, 32 ew + 32)
+    umma_commit(&mma_done);              // every MMA issued above has completed
+    mbar_wait(&mma_done, 0);
+  } else if (CHUNKED && warp >= 2) {
+    // ---- epilogue (chunked): per chunk TMEM -> FP64 registers; D stored at the end
+    const int q = warp & 3;              // TMEM lane quarter this warp may access
+    const int h = (warp - 2) >> 2;       // column half
+    const int row = m0 + q * 32 + lane;
+    double acc[BN / 2];
+#pragma unroll
+    for (int j = 0; j < BN / 2; ++j) acc[j] = 0.0;
+    bool ok = true;
+    for (int c = 0; c < chunks && ok; ++c) {
+      const int b = c & 1;
+      // warp-uniform outcome: the TMEM loads below are .sync.aligned
+      ok = __all_sync(0xffffffffu, mbar_wait(&acc_full[b], (c >> 1) & 1));
+      fence_after();
+      if (!ok) break;
+      uint32_t r0[32], r1[32];
+      const uint32_t ta = tmem + (uint32_t(q * 32) << 16) + uint32_t(b * BN + h * (BN / 2));
+      tmem_ld32_nowait(ta, r0);
+      tmem_ld32_nowait(ta + 32, r1);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+      for (int j = 0; j < 32; ++j) asm volatile("" : "+r"(r0[j]), "+r"(r1[j]));
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        acc[j] += double(__uint_as_float(r0[j]));
+        acc[32 + j] += double(__uint_as_float(r1[j]));
+      }
+      fence_before();
+      __syncwarp();
+      if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acc_empty[b])) : "memory");
+    }
+    if (!ok) {
+      if (lane == 0) atomicExch(g.status, MCNLA_B200_ERR_DEVICE_TIMEOUT);
+    } else if (row < g.M) {
+      OutT* drow = static_cast<OutT*>(g.D) + int64_t(row) * g.ldd;
+      const int col = n0 + h * (BN / 2);
+      if (col + BN / 2 <= g.N) {
+#pragma unroll
+        for (int j = 0; j < BN / 2; ++j) drow[col + j] = OutT(acc[j]);
+      } else {
+#pragma unroll
+        for (int j = 0; j < BN / 2; ++j)
+          if (col + j < g.N) drow[col + j] = OutT(acc[j]);
+      }
+    }
+  } else if (!CHUNKED && warp >= 4) {
+    // ---- epilogue (wide): TMEM -> registers -> global
+    const int q = warp & 3;
     // warp-uniform outcome: the TMEM loads below are .sync.aligned
-    const bool ok = __all_sync(0xffffffffu, mbar_wait(&accum_bar, 0));
+    const bool ok = __all_sync(0xffffffffu, mbar_wait(&acc_full[0], 0));
     fence_after();
     if (!ok) {
       if (lane == 0) atomicExch(g.status, MCNLA_B200_ERR_DEVICE_TIMEOUT);
     } else {
-      const int row = m0 + ew * 32 + lane;
+      const int row = m0 + q * 32 + lane;
       OutT* drow = static_cast<OutT*>(g.D) + int64_t(row) * g.ldd;
 #pragma unroll 1
       for (int c = 0; c < BN / 32; ++c) {
         uint32_t r[32];
-        tmem_ld32(tmem + (uint32_t(ew * 32) << 16) + uint32_t(c * 32), r);
+        tmem_ld32(tmem + (uint32_t(q * 32) << 16) + uint32_t(c * 32), r);
         const int col = n0 + c * 32;
         if (row < g.M) {
           if (col + 32 <= g.N) {
@@ -232,7 +338,7 @@ __global__ void __launch_bounds__(THREADS, 1) bf16_gemm_kernel(const __grid_cons
   __syncthreads();
   if (warp == 0) {
     __syncwarp();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(T::TMEM_COLS));
   }
 }
 
@@ -287,29 +393,38 @@ int bf16_gemm(Context* c, int64_t M, int64_t N, int64_t K, const uint16_t* a_hi,
       (ldb * 2) % 16)
     return MCNLA_B200_ERR_LAYOUT;
   if (lda < K || ldb < K) return MCNLA_B200_ERR_SHAPE;
+  // three parts: the chunked configuration (FP64 sums of FP32 chunks)
+  const bool chunked = a_lo2 != nullptr;
+  const int bn = chunked ? TileCfg<true>::BN : TileCfg<false>::BN;
   CUtensorMap ta_hi, ta_lo, ta_lo2, tb;
   MB_CHECK(make_map(&ta_hi, a_hi, M, K, lda, BM));
   MB_CHECK(make_map(&ta_lo, a_lo ? a_lo : a_hi, M, K, lda, BM));
   MB_CHECK(make_map(&ta_lo2, a_lo2 ? a_lo2 : a_hi, M, K, lda, BM));
-  MB_CHECK(make_map(&tb, b, N, K, ldb, BN));
+  MB_CHECK(make_map(&tb, b, N, K, ldb, bn));
   Args g;
   g.M = int(M);
   g.N = int(N);
   g.KT = int(cdiv(K, BK));
   g.parts = a_lo2 ? 3 : (a_lo ? 2 : 1);
+  static_assert(TileCfg<true>::A_PARTS >= MAX_PARTS, "the chunked stage holds every part");
   g.D = D;
   g.ldd = ldd;
   g.status = &c->scal->status;
-  dim3 grid(unsigned(cdiv(N, BN)), unsigned(cdiv(M, BM)));
+  dim3 grid(unsigned(cdiv(N, bn)), unsigned(cdiv(M, BM)));
   if (grid.y > 65535) return MCNLA_B200_ERR_SHAPE;
+  auto go = [&](auto kern, int threads, size_t smem) -> int {
+    MB_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    kern<<<grid, threads, smem, c->stream>>>(ta_hi, ta_lo, ta_lo2, tb, g);
+    return MCNLA_B200_OK;
+  };
+  using W = TileCfg<false>;
+  using Ch = TileCfg<true>;
   if (out_fp64) {
-    MB_CHECK_CUDA(cudaFuncSetAttribute(bf16_gemm_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       int(SMEM_BYTES)));
-    bf16_gemm_kernel<double><<<grid, THREADS, SMEM_BYTES, c->stream>>>(ta_hi, ta_lo, ta_lo2, tb, g);
+    MB_CHECK(chunked ? go(bf16_gemm_kernel<double, true>, Ch::THREADS, Ch::SMEM_BYTES)
+                     : go(bf16_gemm_kernel<double, false>, W::THREADS, W::SMEM_BYTES));
   } else {
-    MB_CHECK_CUDA(cudaFuncSetAttribute(bf16_gemm_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       int(SMEM_BYTES)));
-    bf16_gemm_kernel<float><<<grid, THREADS, SMEM_BYTES, c->stream>>>(ta_hi, ta_lo, ta_lo2, tb, g);
+    MB_CHECK(chunked ? go(bf16_gemm_kernel<float, true>, Ch::THREADS, Ch::SMEM_BYTES)
+                     : go(bf16_gemm_kernel<float, false>, W::THREADS, W::SMEM_BYTES));
   }
   c->kernels_launched++;
   MB_CHECK_CUDA(cudaGetLastError());
