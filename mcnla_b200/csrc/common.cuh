@@ -82,9 +82,12 @@ struct Context {
   // integrator converged earlier on the device).
   const int* guard_stop = nullptr;
   int guard_it = 0;
-  // KN step: 0 = matrix functions by Newton-Schulz when l <= 80 (eigen
-  // fallback), 1 = always the eigendecomposition (Jacobi) path
+  // KN step method (MCNLA_B200_KN_*)
   int kn_mode = 0;
+  // most CTAs a cooperative (persistent) grid of this context may take; 0:
+  // all SMs.  Concurrent solves (the server's workers) each take a share so
+  // that their persistent kernels can be resident together.
+  int coop_cta_limit = 0;
   DevScalars* scal = nullptr;       // device scalars
   DevScalars* scal_host = nullptr;  // pinned mirror
   // stage part timers (CUDA events), filled by the last stage call

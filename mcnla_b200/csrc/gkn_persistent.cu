@@ -147,11 +147,14 @@ __global__ void __launch_bounds__(kGknThreads, 1) k_gkn_persistent(GknArgs a) {
 
 }  // namespace
 
-// Grid: enough CTAs for two 8 x 8 tiles of Bs Bc each (at least the
-// ceil(l/8) CTAs of the KN step), at most one per SM.
+// Grid: enough CTAs for two 8 x 8 tiles of Bs Bc each, at most one per SM
+// or the context's share of the SMs, and at least the ceil(l/8) CTAs of the
+// KN step.
 int gkn_persistent_grid(const Context* c, int l, int64_t L) {
   const int64_t tiles = ((L + 7) / 8) * ((l + 7) / 8);
-  return int(std::min<int64_t>(c->num_sms, std::max<int64_t>((tiles + 1) / 2, (l + 7) / 8)));
+  int64_t cap = c->num_sms;
+  if (c->coop_cta_limit > 0) cap = std::min<int64_t>(cap, c->coop_cta_limit);
+  return int(std::max<int64_t>(std::min<int64_t>(cap, (tiles + 1) / 2), (l + 7) / 8));
 }
 
 bool gkn_persistent_fits(const Context* c, int l, int64_t L) {

@@ -63,6 +63,7 @@ struct mcnla_b200_server {
   int device = 0;
   int64_t budget = 0;
   std::vector<std::thread> threads;
+  int nworkers = 1;
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   std::deque<int64_t> queue;
@@ -132,6 +133,9 @@ void mcnla_b200_server::worker() {
   bool ok = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) == cudaSuccess &&
             mcnla_b200_create(&ctx, device, stream) == MCNLA_B200_OK && cudaEventCreate(&e0) == cudaSuccess &&
             cudaEventCreate(&e1) == cudaSuccess;
+  // each worker's persistent kernels take a share of the SMs, so that the
+  // workers' integrations (latency-bound chains of small products) run side by side
+  if (ok) ctx->coop_cta_limit = std::max(1, ctx->num_sms / nworkers);
   if (!ok) init_failures++;
   double* a64 = nullptr;
   size_t a64_bytes = 0;
@@ -204,6 +208,7 @@ int mcnla_b200_server_create(mcnla_b200_server** out, int device, int workers, i
   auto* s = new mcnla_b200_server();
   s->device = device;
   s->budget = budget_bytes;
+  s->nworkers = workers;
   for (int i = 0; i < workers; ++i) s->threads.emplace_back([s] { s->worker(); });
   *out = s;
   return MCNLA_B200_OK;
