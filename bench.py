@@ -62,6 +62,10 @@ def parse():
     ap.add_argument("--cpu-rows", type=int, default=0, help="row sample of the CPU baseline (0: auto)")
     ap.add_argument("--quick", action="store_true", help="small shape for a smoke run")
     ap.add_argument("--no-serving", action="store_true", help="skip the batched / served leg")
+    ap.add_argument("--kernel", choices=["sketch_bf16", "gkn"], default=None,
+                    help="time one kernel alone (profiling case) instead of the benchmark: the BF16 sketch GEMM "
+                         "on --m x --n x (--k + --p) --N with --parts parts, or the persistent row-block Gramian "
+                         "KN integrator on the sketches of a seeded --m x --n matrix (sigma_j = 1/j, tol 1e-5)")
     ap.add_argument("--only-serving", action="store_true", help="run the batched / served leg alone")
     ap.add_argument("--batch-count", type=int, default=1024, help="matrices in the uneven batch")
     ap.add_argument("--serve-workers", type=int, default=8, help="concurrent solves of the server")
@@ -592,6 +596,52 @@ def run_serving(args, dev):
 
 
 # ------------------------------------------------------------------------------------------------
+# single-kernel cases (profiling)
+# ------------------------------------------------------------------------------------------------
+def run_kernel_case(args, dev):
+    import numpy as np
+    import torch
+    from mcnla_b200 import isvd, synthetic, _lib
+    m, n, k, p, N = args.m, args.n, args.k, args.p, args.N
+    L = (k + p) * N
+    ctx = isvd.context(dev)
+    if args.kernel == "sketch_bf16":
+        a = torch.randn(m, n, dtype=torch.float64, device=dev)
+        sp = isvd.split_bf16(a, args.parts)
+        del a
+        om_t, ldo, _ = isvd.gaussian_bf16(n, L, 7, dev)
+        q = torch.empty(m, L, dtype=torch.float64, device=dev)
+        prm = _lib.Params(m, n, k, p, N)
+        ts = []
+        for _ in range(4):
+            _lib.check(ctx.lib.mcnla_b200_sketch_bf16(ctx.bind(), ctypes.byref(prm), isvd._ptr(sp.hi),
+                                                      isvd._ptr(sp.lo), isvd._ptr(sp.lo2), sp.ld, isvd._ptr(om_t),
+                                                      ldo, isvd._ptr(q)), "sketch_bf16")
+            ts.append(ctx.last_times()[1])
+        t = min(ts[1:])
+        return {"kernel": "bf16_gemm_kernel (sketch)", "shape": "%dx%dx%d" % (m, n, L), "parts": args.parts,
+                "ms": round(t * 1e3, 4), "tflops": round(args.parts * 2.0 * m * n * L / t / 1e12, 2)}
+    a = synthetic.lowrank_torch(m, n, np.arange(1, min(m, n, 256) + 1) ** -1.0, seed=1, device=dev)
+    prm = isvd.Parameters(device=dev).setSize(m, n).setRank(k).setOverRank(p).setNumSketch(N).sync()
+    q = prm.createCollectionQ()
+    sk = isvd.GaussianProjectionSketcher(prm, 5)
+    sk.initialize()
+    sk(a, q)
+    orth = isvd.GramianOrthogonalizer(prm)
+    orth.initialize()
+    orth(q)
+    integ = isvd.RowBlockGramianKolmogorovNagumoIntegrator(prm, 256, 1e-5)
+    integ.initialize()
+    qbar = prm.createMatrixQbar()
+    runs = []
+    for _ in range(2):
+        integ(q, qbar)
+        runs.append(integ.times())
+    return {"kernel": "k_gkn_persistent (row-block Gramian KN integrator)", "m": m, "n": n, "l": k + p, "N": N,
+            "iterations": integ.iteration(), "stage_ms": [round(x * 1e3, 4) for x in runs[-1]]}
+
+
+# ------------------------------------------------------------------------------------------------
 # CPU: the reference's own stages on a bounded row sample
 # ------------------------------------------------------------------------------------------------
 def cpu_sample(args, rows=None):
@@ -673,6 +723,10 @@ def main():
     world, rank, local = dist_init(args)
     if args.impl == "reference":
         res = run_reference(args, world, rank)
+    elif args.kernel:
+        import torch
+        torch.cuda.set_device(local)
+        res = run_kernel_case(args, torch.device("cuda", local))
     elif args.only_serving:
         import torch
         torch.cuda.set_device(local)
