@@ -121,11 +121,13 @@ def barrier(world):
 
 
 def max_over_ranks(x, world):
+    """Largest value of x over the ranks (a CUDA tensor on NCCL, a CPU tensor on gloo)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
