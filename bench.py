@@ -73,6 +73,8 @@ def parse():
     ap.add_argument("--serve-rates", default="200,1000,5000", help="Poisson arrival rates, requests/s")
     ap.add_argument("--serve-seconds", type=float, default=0.5, help="arrival window per rate (>= 400 requests)")
     ap.add_argument("--serve-integrator", default="rb_gramian_kn", help="KN integrator of the batched / served solves")
+    ap.add_argument("--serve-former", default="rb_gramian",
+                    help="former of the batched / served solves (the row-block driver's pairing by default)")
     ap.add_argument("--parts", type=int, default=2, help="BF16 parts of A in the mixed leg (2: 16 bits, 3: 24 bits)")
     ap.add_argument("--serve-parts", type=int, default=3, help="BF16 parts of A in the batched / served mixed solves")
     args = ap.parse_args()
@@ -462,7 +464,8 @@ def run_serving(args, dev):
     def request(i, mixed, a=None, sh=None):
         sh = shapes[i] if sh is None else sh
         return isvd.Request(pool[i] if a is None else a, sh["k"], sh["p"], sh["N"], seed=sh["seed"],
-                            integrator=args.serve_integrator, former="svd", maxit=256, tol=1e-5, mixed=mixed)
+                            integrator=args.serve_integrator, former=args.serve_former, maxit=256, tol=1e-5,
+                            mixed=mixed)
 
     order = sorted(range(len(shapes)), key=lambda i: -shapes[i]["m"] * shapes[i]["n"] * shapes[i]["k"])
 
@@ -508,7 +511,7 @@ def run_serving(args, dev):
         a64 = pool[i].double()
         _, _, om64 = isvd.gaussian_bf16(sh["n"], L, sh["seed"], dev, with_fp64=True)
         s64, u64, _, _ = isvd.solve(a64, k, sh["p"], sh["N"], omega=om64, integrator=args.serve_integrator,
-                                    former="svd", maxit=256, tol=1e-5)
+                                    former=args.serve_former, maxit=256, tol=1e-5)
         acc["sigma_rel_err"] = max(acc["sigma_rel_err"], ((r.s - s64).abs() / s64).max().item())
         cosmin = torch.linalg.svdvals(u64.t() @ r.u).min().clamp(-1, 1)
         acc["max_principal_angle_U"] = max(acc["max_principal_angle_U"], float(torch.arccos(cosmin).item()))
@@ -582,8 +585,8 @@ def run_serving(args, dev):
     torch.cuda.empty_cache()
     return {
         "workload": "%d uneven FP32 matrices (m~U[512,16384], n~U[256,4096], k in {8,16,32,64}, p=k/2, N=8, "
-                    "sigma_j=j^-alpha, alpha~U[0.5,2], spectrum cut at 256), %s tol 1e-5, SVD former"
-                    % (len(shapes), args.serve_integrator),
+                    "sigma_j=j^-alpha, alpha~U[0.5,2], spectrum cut at 256), %s tol 1e-5, %s former"
+                    % (len(shapes), args.serve_integrator, args.serve_former),
         "timing": "host wall clock, device synchronized on both sides; solves on the workers' own streams",
         "per_request_fp64": serial64, "batched_fp64": batched64, "batched_mixed": batched_mx,
         "mixed_speedup_vs_per_request_fp64": round(batched_mx["solves_per_s"] / serial64["solves_per_s"], 3),

@@ -94,14 +94,14 @@ __global__ void __launch_bounds__(kSmallThreads) k_syev(int n, const double* A, 
   if (v_smem) {
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
       const int i = e / n, j = e % n;
-      Vb[i * n + rank[j]] = v[i * ldv + j];
+      Vb[i * n + rank[j]] = v[j * ldv + i];
     }
   } else {
     __syncthreads();
-    // permute columns out of the global work copy
+    // eigenvectors (rows of the global work copy) to ranked columns
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
       const int i = e / n, j = e % n;
-      Vb[i * n + rank[j]] = v[i * ldv + j];
+      Vb[i * n + rank[j]] = v[j * ldv + i];
     }
   }
 }
@@ -168,8 +168,8 @@ __global__ void __launch_bounds__(kSmallThreads) k_kn_step(int l, const double* 
     const int i = e / l, j = e % l;
     double c = 0.0, ci = 0.0;
     for (int k = 0; k < l; ++k) {
-      const double x = v[i * ldv + k] * sv[k], y = v[j * ldv + k] * sv[k];
-      const double xi = v[i * ldv + k] / sv[k], yi = v[j * ldv + k] / sv[k];
+      const double x = v[k * ldv + i] * sv[k], y = v[k * ldv + j] * sv[k];
+      const double xi = v[k * ldv + i] / sv[k], yi = v[k * ldv + j] / sv[k];
       c = fma(x, y, c);
       ci = fma(xi, yi, ci);
     }
@@ -398,7 +398,7 @@ __global__ void __launch_bounds__(kSmallThreads) k_kn_step_ns(int l, const doubl
       double cc = 0.0, ci = 0.0;
       if (i < l && j < l) {
         for (int k = 0; k < l; ++k) {
-          const double x = v[i * (l + 1) + k], y = v[j * (l + 1) + k];
+          const double x = v[k * (l + 1) + i], y = v[k * (l + 1) + j];
           cc = fma(x * sv[k], y * sv[k], cc);
           ci = fma(x / sv[k], y / sv[k], ci);
         }
@@ -519,6 +519,13 @@ __global__ void __launch_bounds__(kSmallThreads) k_wy_trial(int l, const double*
 // ---------------------------------------------------------------------------
 // one-sided Jacobi SVD of a small square matrix
 // ---------------------------------------------------------------------------
+// One-sided (Hestenes) Jacobi SVD of one n x n matrix: columns p, q of a are
+// rotated until all pairs are orthogonal; a = W diag(sig), and the rotations
+// accumulated in z give M = W diag(sig) Z'.  Per round: the angles of the
+// n/2 disjoint pairs (a warp per pair: column dot products by shuffles), then
+// the rotations of a's columns and of z spread over the CTA as (pair, row)
+// items.  z is kept transposed (z[k * ldz + i] = Z(i, k)) so that a rotation
+// touches two contiguous rows when it lives in global memory.
 __global__ void __launch_bounds__(kSmallThreads) k_svd_small(int n, const double* M, double* W, double* sig,
                                                              double* Z, double* zwork, int z_smem) {
   extern __shared__ __align__(16) char smem_raw[];
@@ -532,6 +539,11 @@ __global__ void __launch_bounds__(kSmallThreads) k_svd_small(int n, const double
   int* count = sc.take<int>(4);
   int* rank = sc.take<int>(n);
   double* nrm = sc.take<double>(n);
+  const int P = (n + 1) & ~1, npairs = P / 2;
+  double* rc = sc.take<double>(npairs);
+  double* rs = sc.take<double>(npairs);
+  int* rp = sc.take<int>(npairs);
+  int* rq = sc.take<int>(npairs);
   const int tid = threadIdx.x, nt = blockDim.x;
   const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
   for (int e = tid; e < n * n; e += nt) {
@@ -540,48 +552,61 @@ __global__ void __launch_bounds__(kSmallThreads) k_svd_small(int n, const double
     z[i * ldz + j] = (i == j) ? 1.0 : 0.0;
   }
   __syncthreads();
-  const int P = (n + 1) & ~1, npairs = P / 2;
+  const int items = npairs * n;
   for (int sweep = 0; sweep < 40 && n > 1; ++sweep) {
-    if (tid == 0) *count = 0;
-    __syncthreads();
+    int rotated = 0;
     for (int r = 0; r < P - 1; ++r) {
+      // angles: a warp per pair
+      int mine = 0;
       for (int k = warp; k < npairs; k += nwarps) {
         int p, q;
         small::rr_pair(P, r, k, p, q);
-        if (q >= n) continue;
-        double al = 0.0, be = 0.0, ga = 0.0;
-        for (int i = lane; i < n; i += 32) {
-          const double x = a[i * ld + p], y = a[i * ld + q];
-          al = fma(x, x, al);
-          be = fma(y, y, be);
-          ga = fma(x, y, ga);
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-          al += __shfl_xor_sync(0xffffffffu, al, o);
-          be += __shfl_xor_sync(0xffffffffu, be, o);
-          ga += __shfl_xor_sync(0xffffffffu, ga, o);
-        }
-        if (fabs(ga) > 1e-15 * sqrt(al * be) && ga * ga > 1e-300) {
-          const double zeta = (be - al) / (2.0 * ga);
-          const double az = fabs(zeta);
-          const double t = (az > 1e150) ? 0.5 / zeta : ((zeta >= 0.0 ? 1.0 : -1.0) / (az + sqrt(1.0 + zeta * zeta)));
-          const double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
+        double c = 1.0, sn = 0.0;
+        if (q < n) {
+          double al = 0.0, be = 0.0, ga = 0.0;
           for (int i = lane; i < n; i += 32) {
             const double x = a[i * ld + p], y = a[i * ld + q];
-            a[i * ld + p] = c * x - s * y;
-            a[i * ld + q] = s * x + c * y;
-            const double zx = z[i * ldz + p], zy = z[i * ldz + q];
-            z[i * ldz + p] = c * zx - s * zy;
-            z[i * ldz + q] = s * zx + c * zy;
+            al = fma(x, x, al);
+            be = fma(y, y, be);
+            ga = fma(x, y, ga);
           }
-          if (lane == 0) atomicAdd(count, 1);
+          for (int o = 16; o > 0; o >>= 1) {
+            al += __shfl_xor_sync(0xffffffffu, al, o);
+            be += __shfl_xor_sync(0xffffffffu, be, o);
+            ga += __shfl_xor_sync(0xffffffffu, ga, o);
+          }
+          if (fabs(ga) > 1e-15 * sqrt(al * be) && ga * ga > 1e-300) {
+            const double zeta = (be - al) / (2.0 * ga);
+            const double az = fabs(zeta);
+            const double t = (az > 1e150) ? 0.5 / zeta : ((zeta >= 0.0 ? 1.0 : -1.0) / (az + sqrt(1.0 + zeta * zeta)));
+            c = 1.0 / sqrt(1.0 + t * t);
+            sn = c * t;
+            if (lane == 0) ++mine;
+          }
         }
+        if (lane == 0) { rc[k] = c; rs[k] = sn; rp[k] = p; rq[k] = q; }
+      }
+      // the barrier also counts the rotations set up this round
+      const int cnt = __syncthreads_count(mine);
+      if (cnt == 0) continue;
+      rotated += cnt;
+      // rotations: (pair, row) items over the CTA
+      for (int e = tid; e < items; e += nt) {
+        const int k = e / n, i = e - k * n;
+        const double sn = rs[k];
+        if (sn == 0.0) continue;
+        const double c = rc[k];
+        const int p = rp[k], q = rq[k];
+        const double x = a[i * ld + p], y = a[i * ld + q];
+        a[i * ld + p] = c * x - sn * y;
+        a[i * ld + q] = sn * x + c * y;
+        const double zx = z[p * ldz + i], zy = z[q * ldz + i];
+        z[p * ldz + i] = c * zx - sn * zy;
+        z[q * ldz + i] = sn * zx + c * zy;
       }
       __syncthreads();
     }
-    const int cnt = *count;
-    __syncthreads();
-    if (cnt == 0) break;
+    if (rotated == 0) break;
   }
   for (int j = warp; j < n; j += nwarps) {
     double s = 0.0;
@@ -601,7 +626,7 @@ __global__ void __launch_bounds__(kSmallThreads) k_svd_small(int n, const double
     const int i = e / n, j = e % n;
     const double sj = nrm[j];
     W[i * n + rank[j]] = sj > 0.0 ? a[i * ld + j] / sj : 0.0;
-    Z[i * n + rank[j]] = z[i * ldz + j];
+    Z[i * n + rank[j]] = z[j * ldz + i];
   }
 }
 
@@ -988,7 +1013,8 @@ int launch_wy_gramian_phis(Context* c, int l, const double* F, const double* dc,
 int launch_svd_small(Context* c, int n, const double* M, double* W, double* sig, double* Z) {
   if (n < 1 || n > MCNLA_B200_MAX_DIM_SKETCH) return MCNLA_B200_ERR_UNSUPPORTED;
   const size_t mat = size_t(n) * (n + 1) * 8 + 16;
-  const size_t extra = 64 + n * 4 + 16 + n * 8 + 16 + 64;
+  const int npairs = (n + 2) / 2;
+  const size_t extra = 64 + n * 4 + 16 + n * 8 + 16 + 2 * (npairs * 8 + 16) + 2 * (npairs * 4 + 16) + 64;
   const bool z_smem = 2 * mat + extra <= c->smem_optin;
   const size_t smem = (z_smem ? 2 : 1) * mat + extra;
   if (smem > c->smem_optin) return MCNLA_B200_ERR_UNSUPPORTED;

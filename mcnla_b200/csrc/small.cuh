@@ -63,9 +63,13 @@ __device__ inline double cta_frob2(const double* a, int lda, int n, double* red)
 
 // Eigendecomposition of the symmetric n x n matrix a (row stride lda, any
 // memory space; shared memory is fastest).  On return diag(a) holds the
-// eigenvalues (unsorted) and the columns of v (row stride ldv) the
-// eigenvectors.  When init_v is false, v must hold an orthogonal starting
-// basis in which a is expressed (warm start); otherwise v is set to I.
+// eigenvalues (unsorted) and the ROWS of v (row stride ldv) the eigenvectors:
+// v[k * ldv + i] is component i of eigenvector k (the transpose of the usual
+// V, so that a rotation of two eigenvectors touches two contiguous rows, which
+// matters when v lives in global memory).  When init_v is false, v must hold
+// an orthogonal starting basis (rows) in which a is expressed (warm start);
+// otherwise v is set to I.  Each phase of a round (angles; rows of a; columns
+// of a and rows of v) is spread over the whole CTA as (pair, element) items.
 // Returns the number of sweeps.
 __device__ inline int cta_jacobi_eig(double* a, int lda, double* v, int ldv, int n, bool init_v,
                                      const JacobiScratch& js, int max_sweeps) {
@@ -82,17 +86,17 @@ __device__ inline int cta_jacobi_eig(double* a, int lda, double* v, int ldv, int
   // (relative test) or below eps * ||A||_F (absolute floor: LAPACK's
   // eigensolvers are normwise accurate to that level, and below it rounding
   // in the rotations regenerates off-diagonal noise faster than a sweep
-  // removes it).
+  // removes it).  Both tests compare squares.
   const double eps = 2.220446049250313e-16;
-  const double abs_floor = eps * eps * fro2;
-  const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
+  const double eps2 = eps * eps;
+  const double abs_floor = eps2 * fro2;
+  const int items = npairs * n;
   int sweep = 0;
   for (; sweep < max_sweeps; ++sweep) {
     int rotated = 0;
     for (int r = 0; r < P - 1; ++r) {
-      if (tid == 0) *js.count = 0;
-      __syncthreads();
       // 1. angles, one thread per pair
+      int mine = 0;
       for (int k = tid; k < npairs; k += nt) {
         int p, q;
         rr_pair(P, r, k, p, q);
@@ -101,14 +105,14 @@ __device__ inline int cta_jacobi_eig(double* a, int lda, double* v, int ldv, int
           apq = a[p * lda + q];
           app = a[p * lda + p];
           aqq = a[q * lda + q];
-          const double thr = eps * sqrt(fabs(app) * fabs(aqq));
-          if (fabs(apq) > thr && apq * apq > abs_floor) {
+          const double apq2 = apq * apq;
+          if (apq2 > eps2 * fabs(app * aqq) && apq2 > abs_floor) {
             const double theta = (aqq - app) / (2.0 * apq);
             const double at = fabs(theta);
             t = (at > 1e150) ? 0.5 / theta : ((theta >= 0.0 ? 1.0 : -1.0) / (at + sqrt(1.0 + theta * theta)));
             c = 1.0 / sqrt(1.0 + t * t);
             s = t * c;
-            atomicAdd(js.count, 1);
+            ++mine;
           } else {
             apq = 0.0;
           }
@@ -116,46 +120,44 @@ __device__ inline int cta_jacobi_eig(double* a, int lda, double* v, int ldv, int
         js.c[k] = c; js.s[k] = s; js.t[k] = t; js.apq[k] = apq; js.app[k] = app; js.aqq[k] = aqq;
         js.p[k] = p; js.q[k] = q;
       }
-      __syncthreads();
-      const int cnt = *js.count;
-      if (cnt == 0) { __syncthreads(); continue; }
+      // the barrier also counts the threads that set up a rotation
+      const int cnt = __syncthreads_count(mine);
+      if (cnt == 0) continue;
       rotated += cnt;
-      // 2. rows: a <- J' a   (a warp per pair, lanes along the row)
-      for (int k = warp; k < npairs; k += nwarps) {
+      // 2. rows: a <- J' a   (item (k, j): element j of rows p, q of pair k)
+      for (int e = tid; e < items; e += nt) {
+        const int k = e / n, j = e - k * n;
         const double s = js.s[k];
         if (s == 0.0) continue;
         const double c = js.c[k];
         const int p = js.p[k], q = js.q[k];
-        for (int j = lane; j < n; j += 32) {
-          const double x = a[p * lda + j], y = a[q * lda + j];
-          a[p * lda + j] = c * x - s * y;
-          a[q * lda + j] = s * x + c * y;
-        }
+        const double x = a[p * lda + j], y = a[q * lda + j];
+        a[p * lda + j] = c * x - s * y;
+        a[q * lda + j] = s * x + c * y;
       }
       __syncthreads();
-      // 3. columns: a <- a J and v <- v J.  The 2x2 block of each pair is
-      //    written exactly: J' B J = diag(app - t apq, aqq + t apq).
-      for (int k = warp; k < npairs; k += nwarps) {
+      // 3. columns: a <- a J (the 2x2 block of each pair written exactly:
+      //    J' B J = diag(app - t apq, aqq + t apq)), and rows p, q of v
+      for (int e = tid; e < items; e += nt) {
+        const int k = e / n, i = e - k * n;
         const double s = js.s[k];
         if (s == 0.0) continue;
         const double c = js.c[k];
         const int p = js.p[k], q = js.q[k];
-        for (int i = lane; i < n; i += 32) {
-          if (i == p) {
-            a[p * lda + p] = js.app[k] - js.t[k] * js.apq[k];
-            a[p * lda + q] = 0.0;
-          } else if (i == q) {
-            a[q * lda + q] = js.aqq[k] + js.t[k] * js.apq[k];
-            a[q * lda + p] = 0.0;
-          } else {
-            const double x = a[i * lda + p], y = a[i * lda + q];
-            a[i * lda + p] = c * x - s * y;
-            a[i * lda + q] = s * x + c * y;
-          }
-          const double vx = v[i * ldv + p], vy = v[i * ldv + q];
-          v[i * ldv + p] = c * vx - s * vy;
-          v[i * ldv + q] = s * vx + c * vy;
+        if (i == p) {
+          a[p * lda + p] = js.app[k] - js.t[k] * js.apq[k];
+          a[p * lda + q] = 0.0;
+        } else if (i == q) {
+          a[q * lda + q] = js.aqq[k] + js.t[k] * js.apq[k];
+          a[q * lda + p] = 0.0;
+        } else {
+          const double x = a[i * lda + p], y = a[i * lda + q];
+          a[i * lda + p] = c * x - s * y;
+          a[i * lda + q] = s * x + c * y;
         }
+        const double vx = v[p * ldv + i], vy = v[q * ldv + i];
+        v[p * ldv + i] = c * vx - s * vy;
+        v[q * ldv + i] = s * vx + c * vy;
       }
       __syncthreads();
     }
