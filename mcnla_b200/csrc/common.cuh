@@ -53,8 +53,8 @@ struct DevScalars {
   int sweeps;         // Jacobi sweeps used by the last small solve
   int stop_it;        // iteration at which an integrator converged (INT_MAX: not yet)
   int kn_fallback;    // 1: the series KN step declined this iteration (||Z|| too large)
-  unsigned bar_count; // grid barrier of cooperative kernels: arrivals
-  unsigned bar_gen;   //   and generation
+  unsigned bar_count; // grid barrier of cooperative kernels: arrivals (only grows within a stage)
+  unsigned bar_spare;
   int resume_it;      // persistent integrator: iteration it handed back to the host (-1: none)
   int pad;
 };

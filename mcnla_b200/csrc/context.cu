@@ -20,17 +20,19 @@ void set_last_message(const std::string& msg) {
 
 const char* last_error_text() { return g_last_error; }
 
+// The arenas grow stream-ordered (cudaFreeAsync / cudaMallocAsync on the
+// context's stream): no device-wide synchronisation, so a growing context does
+// not stall the work of other contexts (the server's workers).
 int ctx_reserve(Context* c, size_t bytes) {
   c->arena_top = 0;
   if (bytes <= c->arena_bytes) return MCNLA_B200_OK;
   if (c->arena) {
-    MB_CHECK_CUDA(cudaStreamSynchronize(c->stream));
-    MB_CHECK_CUDA(cudaFree(c->arena));
+    MB_CHECK_CUDA(cudaFreeAsync(c->arena, c->stream));
     c->arena = nullptr;
     c->arena_bytes = 0;
   }
-  const size_t want = bytes + (bytes >> 3);   // grow with headroom
-  cudaError_t e = cudaMalloc(&c->arena, want);
+  const size_t want = bytes + (bytes >> 1);   // grow with headroom
+  cudaError_t e = cudaMallocAsync(&c->arena, want, c->stream);
   if (e != cudaSuccess) {
     (void)cudaGetLastError();
     set_last_cuda_error(e, "workspace cudaMalloc", __FILE__, __LINE__);
@@ -44,19 +46,19 @@ int ctx_reserve(Context* c, size_t bytes) {
 int ctx_reserve_pipeline(Context* c, size_t bytes) {
   if (bytes <= c->parena_bytes) return MCNLA_B200_OK;
   if (c->parena) {
-    MB_CHECK_CUDA(cudaStreamSynchronize(c->stream));
-    MB_CHECK_CUDA(cudaFree(c->parena));
+    MB_CHECK_CUDA(cudaFreeAsync(c->parena, c->stream));
     c->parena = nullptr;
     c->parena_bytes = 0;
   }
-  cudaError_t e = cudaMalloc(&c->parena, bytes);
+  const size_t want = bytes + (bytes >> 1);
+  cudaError_t e = cudaMallocAsync(&c->parena, want, c->stream);
   if (e != cudaSuccess) {
     (void)cudaGetLastError();
     set_last_cuda_error(e, "pipeline cudaMalloc", __FILE__, __LINE__);
     c->parena = nullptr;
     return MCNLA_B200_ERR_NOMEM;
   }
-  c->parena_bytes = bytes;
+  c->parena_bytes = want;
   return MCNLA_B200_OK;
 }
 
@@ -163,6 +165,9 @@ int mcnla_b200_destroy(mcnla_b200_ctx* c) {
 
 int mcnla_b200_set_stream(mcnla_b200_ctx* c, void* stream) {
   if (!c) return MCNLA_B200_ERR_ARG;
+  // the arenas are freed stream-ordered on the context's stream: work still
+  // queued on the old stream must finish before another stream may free them
+  if (c->stream != static_cast<cudaStream_t>(stream)) MB_CHECK_CUDA(cudaStreamSynchronize(c->stream));
   if (c->own_stream && c->stream) {
     MB_CHECK_CUDA(cudaStreamSynchronize(c->stream));
     MB_CHECK_CUDA(cudaStreamDestroy(c->stream));

@@ -89,32 +89,35 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
                : "d"(a), "d"(b));
 }
 
-// Barrier over the whole (co-resident) grid.  Returns false when the wait
+// Barrier over the whole (co-resident) grid.  scal->bar_count only grows: at
+// a launch it is a multiple of the grid size (zeroed with the scalars at the
+// start of a stage; every CTA passes the same number of barriers), so an
+// arriving CTA whose atomic returns `old` waits until the count reaches the
+// next multiple of gridDim.x.  One release (fence + relaxed add) per CTA and
+// acquire polls: no reset on the critical path.  Returns false when the wait
 // gave up (MCNLA_B200_ERR_DEVICE_TIMEOUT is recorded); the kernel returns.
 __device__ bool grid_sync(DevScalars* scal, volatile int* flag) {
   __syncthreads();
   if (gridDim.x == 1) return true;
   if (threadIdx.x == 0) {
-    volatile unsigned* gen = &scal->bar_gen;
-    const unsigned g = *gen;
-    __threadfence();
+    unsigned* cnt = &scal->bar_count;
+    unsigned old;
+    asm volatile("fence.acq_rel.gpu;" ::: "memory");
+    asm volatile("atom.add.relaxed.gpu.global.u32 %0, [%1], 1;" : "=r"(old) : "l"(cnt) : "memory");
+    const unsigned target = (old / gridDim.x + 1) * gridDim.x;
     int ok = 1;
-    if (atomicAdd(&scal->bar_count, 1u) == gridDim.x - 1) {
-      atomicExch(&scal->bar_count, 0u);
-      __threadfence();
-      atomicAdd(&scal->bar_gen, 1u);
-    } else {
-      const long long t0 = clock64();
-      while (*gen == g) {
-        if (clock64() - t0 > kBarrierCycles) {
-          ok = 0;
-          atomicExch(&scal->status, MCNLA_B200_ERR_DEVICE_TIMEOUT);
-          break;
-        }
-        __nanosleep(32);
+    const long long t0 = clock64();
+    while (true) {
+      unsigned cur;
+      asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(cur) : "l"(cnt) : "memory");
+      if (int(cur - target) >= 0) break;
+      if (clock64() - t0 > kBarrierCycles) {
+        ok = 0;
+        atomicExch(&scal->status, MCNLA_B200_ERR_DEVICE_TIMEOUT);
+        break;
       }
     }
-    __threadfence();
+    asm volatile("fence.acq_rel.gpu;" ::: "memory");
     *flag = ok;
   }
   __syncthreads();
