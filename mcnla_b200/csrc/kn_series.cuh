@@ -35,6 +35,7 @@ constexpr int kSerCoefs = 128;          // series coefficients kept in constant 
 constexpr int kSerMaxDegree = 94;       // degree search limit (s, q <= 10)
 constexpr int kSerMaxS = 10;            // power slabs Z^1 .. Z^s on chip
 constexpr int kSerDirectMax = 12;       // degree up to which plain powers replace Paterson-Stockmeyer
+constexpr int kSerZsMax = 112;          // l up to which Z is staged in shared memory for its products
 constexpr double kSerMaxRho = 0.5;      // 4 ||Z||_F above this: the step declines
 constexpr double kSerTail = 1e-17;
 constexpr long long kBarrierCycles = 4000000000LL;   // about 2 s at the boost clock
@@ -78,9 +79,11 @@ struct SeriesArgs {
   DevScalars* scal;
 };
 
-// Shared memory of the step: s_max + 4 slabs of 8 rows plus reduction space.
+// Shared memory of the step: s_max + 4 slabs of 8 rows, reduction space and,
+// for l <= kSerZsMax, a copy of Z (l rows, the slab row stride).
 __host__ __device__ constexpr size_t kn_series_smem_doubles(int l) {
-  return size_t(kSerMaxS + 4) * 8 * (((l + 7) & ~7) + 4) + 32;
+  return size_t(kSerMaxS + 4) * 8 * (((l + 7) & ~7) + 4) + 32 +
+         (l <= kSerZsMax ? size_t(l) * (((l + 7) & ~7) + 4) : 0);
 }
 
 __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
@@ -191,10 +194,10 @@ __device__ __forceinline__ void tile_acc2(FA1 fa1, FA2 fa2, FB fb, int kb, int k
 }
 
 // C1 = A1 Y (and C2 = A2 Y): A 8 x l slabs in shared memory (row stride ld,
-// zero beyond column l), Y l x l in global memory (row stride ldy), C slabs
-// in shared memory.  One warp per 8-column tile; the two products share the
-// Y fragments.  Ends with a block barrier.
-template <bool TRANS_Y = false>
+// zero beyond column l), Y l x l in global memory (row stride ldy; or in
+// shared memory for SMEM_Y), C slabs in shared memory.  One warp per 8-column
+// tile; the two products share the Y fragments.  Ends with a block barrier.
+template <bool TRANS_Y = false, bool SMEM_Y = false>
 __device__ void slab_mm(const double* A1, const double* A2, int ld, const double* Y, int ldy, int l, double* C1,
                         double* C2) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
@@ -205,7 +208,8 @@ __device__ void slab_mm(const double* A1, const double* A2, int ld, const double
     const bool nv = n < l;
     // Y(k, n), or Y(n, k) for TRANS_Y
     auto fy = [&](int k) {
-      return nv ? __ldcg(TRANS_Y ? Y + size_t(n) * ldy + k : Y + size_t(k) * ldy + n) : 0.0;
+      const double* y = TRANS_Y ? Y + size_t(n) * ldy + k : Y + size_t(k) * ldy + n;
+      return nv ? (SMEM_Y ? *y : __ldcg(y)) : 0.0;
     };
     double c0 = 0.0, c1 = 0.0;
     double* o1 = C1 + g * ld + t * 8 + 2 * t4;
@@ -332,6 +336,17 @@ __device__ int kn_series_step(const SeriesArgs& a, double* sm, volatile int* fla
   const int nq = (d + s) / s;                       // blocks of s coefficients: degree nq*s - 1 >= d
   double* cinv = a.out + size_t(l) * l;
   const bool rb = a.dd != nullptr;
+  // Z for the products below: a shared-memory copy when it fits
+  const bool zs_smem = l <= kSerZsMax;
+  double* zs = red + 32;
+  if (mine && zs_smem) {
+    for (int e = tid; e < l * l; e += nt) zs[(e / l) * ld + (e % l)] = __ldcg(a.zg + e);
+    __syncthreads();
+  }
+  auto mm_z = [&](const double* A1, const double* A2, double* C1, double* C2) {
+    if (zs_smem) slab_mm<false, true>(A1, A2, ld, zs, ld, l, C1, C2);
+    else slab_mm(A1, A2, ld, a.zg, l, l, C1, C2);
+  };
 
   if (d <= kSerDirectMax) {
     // ---- plain powers: C = sum f_j Z^j, inv(C) = sum g_j Z^j and, for the
@@ -354,7 +369,7 @@ __device__ int kn_series_step(const SeriesArgs& a, double* sm, volatile int* fla
       }
       __syncthreads();
       if (rb) {
-        slab_mm(tF, nullptr, ld, a.zg, l, l, Wa, nullptr);
+        mm_z(tF, nullptr, Wa, nullptr);
         for (int e = tid; e < 8 * lp8; e += nt) {
           const int o = (e / lp8) * ld + e % lp8;
           DW[o] += coefG[1] * Wa[o];
@@ -363,7 +378,7 @@ __device__ int kn_series_step(const SeriesArgs& a, double* sm, volatile int* fla
       }
       double *pc = Pa, *pn = Pb, *wc = Wa, *wn = Wb;
       for (int j = 2; j <= d; ++j) {
-        slab_mm(pc, rb ? wc : nullptr, ld, a.zg, l, l, pn, rb ? wn : nullptr);
+        mm_z(pc, rb ? wc : nullptr, pn, rb ? wn : nullptr);
         for (int e = tid; e < 8 * lp8; e += nt) {
           const int o = (e / lp8) * ld + e % lp8;
           accF[o] += coefF[j] * pn[o];
@@ -426,7 +441,7 @@ __device__ int kn_series_step(const SeriesArgs& a, double* sm, volatile int* fla
   // ---- rows of Z^2 .. Z^s (Z^s only when a Horner step needs it)
   if (mine) {
     const int top = nq > 1 ? s : s - 1;
-    for (int j = 2; j <= top; ++j) slab_mm(P + (j - 2) * slab, nullptr, ld, a.zg, l, l, P + (j - 1) * slab, nullptr);
+    for (int j = 2; j <= top; ++j) mm_z(P + (j - 2) * slab, nullptr, P + (j - 1) * slab, nullptr);
     if (nq > 1) {
       for (int e = tid; e < 8 * l; e += nt) {
         const int rr = e / l, j = e % l, i = r0 + rr;
