@@ -45,6 +45,7 @@ struct GknArgs {
   double* fcn;              // [Fc; inv(C)/N]
   double* work;             // series scratch (kn_series_work_doubles(l))
   DevScalars* scal;
+  int smax;                 // power slabs of the series step
 };
 
 // out(i, j) := sum_k A(i, k) B(k, j) for an M x N product over 8 x 8 tiles
@@ -83,7 +84,7 @@ __global__ void __launch_bounds__(kGknThreads, 1) k_gkn_persistent(GknArgs a) {
   extern __shared__ __align__(16) double sm[];
   __shared__ int s_flag;
   const int l = a.l, L = a.L, l3 = 3 * l;
-  double* red = sm + kn_series_smem_doubles(l);        // kGknWarps x 64 doubles
+  double* red = sm + kn_series_smem_doubles(l, a.smax);   // kGknWarps x 64 doubles
   for (int it = a.it0; it < a.maxit; ++it) {
     const int cur = it & 1;
     double* E = cur ? a.eb1 : a.eb0;                   // [E~c | Bc | Bgc]
@@ -115,6 +116,7 @@ __global__ void __launch_bounds__(kGknThreads, 1) k_gkn_persistent(GknArgs a) {
     s.zsg = a.work + size_t(l) * l;
     s.partials = a.work + 2 * size_t(l) * l;
     s.scal = a.scal;
+    s.smax = a.smax;
     double norm = 0.0;
     int degree = 0;
     const int r = kn_series_step(s, sm, &s_flag, true, &norm, &degree);
@@ -161,15 +163,15 @@ bool gkn_persistent_fits(const Context* c, int l, int64_t L) {
   // Bs Bc here reads its operands straight from L2; past L ~ 1536 the
   // smem-pipelined GEMM of the launch-per-product loop is faster
   if (l < 1 || l > MCNLA_B200_MAX_DIM_SKETCH || L > kGknMaxL) return false;
-  const size_t smem = (kn_series_smem_doubles(l) + kGknWarps * 64) * sizeof(double);
-  return smem + 1024 <= c->smem_optin && (l + 7) / 8 <= c->num_sms;
+  return kn_series_smax(l, c->smem_optin, kGknWarps * 64) > 0 && (l + 7) / 8 <= c->num_sms;
 }
 
 int launch_gkn_persistent(Context* c, int l, int64_t L, int N, double tol, int it0, int maxit, const double* Bs,
                           double* const EB[2], double* const FF[2], double* DD, double* FC, double* FCN,
                           double* work) {
   if (!gkn_persistent_fits(c, l, L)) return MCNLA_B200_ERR_UNSUPPORTED;
-  const size_t smem = (kn_series_smem_doubles(l) + kGknWarps * 64) * sizeof(double);
+  const int smax = kn_series_smax(l, c->smem_optin, kGknWarps * 64);
+  const size_t smem = (kn_series_smem_doubles(l, smax) + kGknWarps * 64) * sizeof(double);
   MB_CHECK(set_smem(c, reinterpret_cast<const void*>(k_gkn_persistent), smem));
   GknArgs a;
   a.l = l;
@@ -189,6 +191,7 @@ int launch_gkn_persistent(Context* c, int l, int64_t L, int N, double tol, int i
   a.fcn = FCN;
   a.work = work;
   a.scal = c->scal;
+  a.smax = smax;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(unsigned(G));
   cfg.blockDim = dim3(kGknThreads);

@@ -37,16 +37,18 @@ __global__ void __launch_bounds__(kSerThreads) k_kn_series(StepArgs a) {
 
 }  // namespace
 
-size_t kn_series_work_doubles(int l) { return 2 * size_t(l) * l + 2 * size_t((l + 7) / 8) + 8; }
+size_t kn_series_work_doubles(int l) { return 2 * size_t(l) * l + 3 * size_t((l + 7) / 8) + 8; }
 
 int launch_kn_series(Context* c, int l, const double* z, const double* dd, double inv_n, double* out, double* outn,
                      const double* ff, double* ffn, double* work, double tol) {
   if (l < 1 || l > MCNLA_B200_MAX_DIM_SKETCH) return MCNLA_B200_ERR_UNSUPPORTED;
   const int G = (l + 7) / 8;
-  const size_t smem = kn_series_smem_doubles(l) * sizeof(double);
+  const int smax = kn_series_smax(l, c->smem_optin, 0);
+  if (smax == 0) return MCNLA_B200_ERR_UNSUPPORTED;
+  const size_t smem = kn_series_smem_doubles(l, smax) * sizeof(double);
   MB_CHECK(set_smem(c, reinterpret_cast<const void*>(k_kn_series), smem));
   StepArgs a;
-  a.s = series_args(c, l, z, dd, inv_n, out, outn, ff, ffn, work);
+  a.s = series_args(c, l, z, dd, inv_n, out, outn, ff, ffn, work, smax);
   a.tol = tol;
   a.guard_stop = c->guard_stop;
   a.guard_it = c->guard_it;

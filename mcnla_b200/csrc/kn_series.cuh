@@ -31,12 +31,12 @@
 namespace mb {
 namespace {
 
-constexpr int kSerCoefs = 128;          // series coefficients kept in constant memory
-constexpr int kSerMaxDegree = 94;       // degree search limit (s, q <= 10)
-constexpr int kSerMaxS = 10;            // power slabs Z^1 .. Z^s on chip
+constexpr int kSerCoefs = 320;          // series coefficients kept in constant memory
+constexpr int kSerMaxDegree = 300;      // degree search limit
+constexpr int kSerMaxS = 18;            // most power slabs Z^1 .. Z^s on chip (fewer when they do not fit)
 constexpr int kSerDirectMax = 12;       // degree up to which plain powers replace Paterson-Stockmeyer
 constexpr int kSerZsMax = 112;          // l up to which Z is staged in shared memory for its products
-constexpr double kSerMaxRho = 0.5;      // 4 ||Z||_F above this: the step declines
+constexpr double kSerMaxRho = 0.9;      // 4 ||Z|| above this: the step declines
 constexpr double kSerTail = 1e-17;
 constexpr long long kBarrierCycles = 4000000000LL;   // about 2 s at the boost clock
 
@@ -75,15 +75,24 @@ struct SeriesArgs {
   double* ffn;            // F~c Fc
   double* zg;             // scratch: Z (l x l)
   double* zsg;            // scratch: Z^s (l x l)
-  double* partials;       // scratch: 2 * ceil(l/8)
+  double* partials;       // scratch: 3 * ceil(l/8)
   DevScalars* scal;
+  int smax;               // power slabs on chip (kn_series_smax)
 };
 
-// Shared memory of the step: s_max + 4 slabs of 8 rows, reduction space and,
+// Shared memory of the step: smax + 4 slabs of 8 rows, reduction space and,
 // for l <= kSerZsMax, a copy of Z (l rows, the slab row stride).
-__host__ __device__ constexpr size_t kn_series_smem_doubles(int l) {
-  return size_t(kSerMaxS + 4) * 8 * (((l + 7) & ~7) + 4) + 32 +
+__host__ __device__ constexpr size_t kn_series_smem_doubles(int l, int smax) {
+  return size_t(smax + 4) * 8 * (((l + 7) & ~7) + 4) + 32 +
          (l <= kSerZsMax ? size_t(l) * (((l + 7) & ~7) + 4) : 0);
+}
+
+// Most power slabs (<= kSerMaxS) whose step fits `optin` bytes of shared
+// memory next to `extra` doubles of the calling kernel (0 when even 4 do not).
+inline int kn_series_smax(int l, size_t optin, size_t extra) {
+  for (int smax = kSerMaxS; smax >= 4; --smax)
+    if ((kn_series_smem_doubles(l, smax) + extra) * sizeof(double) + 1024 <= optin) return smax;
+  return 0;
 }
 
 __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
@@ -231,7 +240,7 @@ __device__ void slab_mm(const double* A1, const double* A2, int ld, const double
 
 // Step operands with the scratch carved out of `work` (kn_series_work_doubles(l)).
 inline SeriesArgs series_args(Context* c, int l, const double* z, const double* dd, double inv_n, double* out,
-                       double* outn, const double* ff, double* ffn, double* work) {
+                       double* outn, const double* ff, double* ffn, double* work, int smax) {
   SeriesArgs a;
   a.l = l;
   a.z_in = z;
@@ -245,6 +254,7 @@ inline SeriesArgs series_args(Context* c, int l, const double* z, const double* 
   a.zsg = work + size_t(l) * l;
   a.partials = work + 2 * size_t(l) * l;
   a.scal = c->scal;
+  a.smax = smax;
   return a;
 }
 
@@ -253,7 +263,8 @@ enum : int { kStepTimeout = -1, kStepDeclined = 0, kStepDone = 1 };
 // One KN step (see the file comment).  Every CTA of the grid calls it; CTAs
 // [0, ceil(l/8)) do the work.  Returns kStepDone (C / Fc / inv(C) / F~+ in
 // global memory, *norm = ||C - I||_F and *degree in every thread),
-// kStepDeclined (4 ||Z||_F > 1/2 or not finite; nothing written but Z) or
+// kStepDeclined (4 min(||Z||_F, ||Z||_inf) > 0.9 or not finite; nothing
+// written but Z) or
 // kStepTimeout.  end_barrier: end with a grid barrier after [Fc; inv(C)] are
 // written (when other CTAs read them next); F~+ is written after it.
 __device__ int kn_series_step(const SeriesArgs& a, double* sm, volatile int* flag, bool end_barrier, double* norm,
@@ -267,7 +278,8 @@ __device__ int kn_series_step(const SeriesArgs& a, double* sm, volatile int* fla
   const int r0 = blockIdx.x * 8;
   const int slab = 8 * ld;
   double* P = sm;                                   // P + (j-1) slab: rows of Z^j, j = 1 .. s
-  double* accF = P + kSerMaxS * slab;
+  const int smax = a.smax;
+  double* accF = P + smax * slab;
   double* accG = accF + slab;
   double* tF = accG + slab;
   double* tG = tF + slab;
@@ -276,7 +288,7 @@ __device__ int kn_series_step(const SeriesArgs& a, double* sm, volatile int* fla
   const double* coefG = c_series.g;                 // c^(1/2):  inv(C)
   const int ldd = 2 * l;
   if (mine) {
-    for (int e = tid; e < (kSerMaxS + 4) * slab; e += nt) sm[e] = 0.0;
+    for (int e = tid; e < (smax + 4) * slab; e += nt) sm[e] = 0.0;
     __syncthreads();
     // ---- Z rows [r0, r0 + 8)
     if (a.dd != nullptr) {
@@ -306,14 +318,32 @@ __device__ int kn_series_step(const SeriesArgs& a, double* sm, volatile int* fla
     }
     part = block_sum(part, red);
     if (tid == 0) a.partials[blockIdx.x] = part;
+    // absolute row sums of the CTA's rows (a warp per row, fixed order) for
+    // the infinity-norm bound; red[16 ..] is clear of block_sum's slots
+    const int warp = tid >> 5, lane = tid & 31;
+    if (warp < 8) {
+      double rs = 0.0;
+      for (int j = lane; j < l; j += 32) rs += fabs(P[warp * ld + j]);
+      for (int o = 16; o > 0; o >>= 1) rs += __shfl_xor_sync(0xffffffffu, rs, o);
+      if (lane == 0) red[16 + warp] = rs;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      double mx = 0.0;
+      for (int w = 0; w < 8; ++w) mx = fmax(mx, red[16 + w]);
+      a.partials[2 * gkn + blockIdx.x] = mx;
+    }
   }
   if (!grid_sync(a.scal, flag)) return kStepTimeout;
 
-  // ---- degree from ||Z||_F (the same arithmetic in every CTA)
+  // ---- degree from z = min(||Z||_F, ||Z||_inf) >= ||Z||_2 (the same arithmetic in every CTA)
   if (tid == 0) {
-    double s2 = 0.0;
-    for (int b = 0; b < gkn; ++b) s2 += __ldcg(a.partials + b);
-    const double z = sqrt(s2);
+    double s2 = 0.0, zi = 0.0;
+    for (int b = 0; b < gkn; ++b) {
+      s2 += __ldcg(a.partials + b);
+      zi = fmax(zi, __ldcg(a.partials + 2 * gkn + b));
+    }
+    const double z = fmin(sqrt(s2), zi);
     int d = -1;
     if (4.0 * z <= kSerMaxRho) {                    // false for NaN
       const double scale = 1.0 / (1.0 - 4.0 * z);
@@ -326,6 +356,7 @@ __device__ int kn_series_step(const SeriesArgs& a, double* sm, volatile int* fla
     }
     int s = 1;
     while (d >= 0 && s * s < d + 1) ++s;
+    if (s > smax) s = smax;
     s_d = d;
     s_s = s;
   }
