@@ -88,6 +88,8 @@ struct Context {
   // all SMs.  Concurrent solves (the server's workers) each take a share so
   // that their persistent kernels can be resident together.
   int coop_cta_limit = 0;
+  // time the tile configurations of a GEMM shape on its first call (dgemm.cu)
+  bool autotune = true;
   DevScalars* scal = nullptr;       // device scalars
   DevScalars* scal_host = nullptr;  // pinned mirror
   // stage part timers (CUDA events), filled by the last stage call

@@ -179,6 +179,12 @@ int mcnla_b200_set_stream(mcnla_b200_ctx* c, void* stream) {
 
 int64_t mcnla_b200_kernels_launched(const mcnla_b200_ctx* c) { return c ? c->kernels_launched : 0; }
 
+int mcnla_b200_set_autotune(mcnla_b200_ctx* c, int on) {
+  if (!c) return MCNLA_B200_ERR_ARG;
+  c->autotune = on != 0;
+  return MCNLA_B200_OK;
+}
+
 int mcnla_b200_set_kn_method(mcnla_b200_ctx* c, int method) {
   if (!c || method < MCNLA_B200_KN_AUTO || method > MCNLA_B200_KN_NEWTON_SCHULZ) return MCNLA_B200_ERR_ARG;
   c->kn_mode = method;

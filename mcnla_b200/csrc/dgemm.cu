@@ -9,6 +9,9 @@
 #include "dgemm.cuh"
 #include <algorithm>
 #include <atomic>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 namespace mb {
 namespace {
@@ -323,6 +326,122 @@ size_t dgemm_workspace_bytes(const Context* c, int64_t M, int64_t N, int64_t K, 
   return p.splits > 1 ? size_t(p.splits) * batch * M * N * sizeof(double) : 0;
 }
 
+namespace {
+
+Plan plan_for(Shape shape, int64_t M, int64_t N, int64_t K, int batch, int splits) {
+  (void)batch;
+  Plan p;
+  p.shape = shape;
+  p.bm = (shape == S64x64 || shape == S64x32) ? 64 : 128;
+  p.bn = (shape == S128x32 || shape == S64x32) ? 32 : ((shape == S128x64 || shape == S64x64) ? 64 : 128);
+  (void)M; (void)N;
+  int64_t kps = cdiv(cdiv(K, splits), BK) * BK;
+  if (kps == 0) kps = BK;
+  p.splits = int(std::max<int64_t>(1, cdiv(K, kps)));
+  p.kps = kps;
+  return p;
+}
+
+// Launches g with plan p (the kernel, then the split-K reduction into g.C).
+int run_plan(Context* ctx, KArgs g, int batch, const Plan& p, bool AK, bool BKM, bool vec2) {
+  g.splits = p.splits;
+  g.kps = p.kps;
+  int st;
+  if (AK && BKM) st = vec2 ? dispatch_shape<true, true, 2>(ctx, g, batch, p.shape)
+                           : dispatch_shape<true, true, 1>(ctx, g, batch, p.shape);
+  else if (AK) st = vec2 ? dispatch_shape<true, false, 2>(ctx, g, batch, p.shape)
+                         : dispatch_shape<true, false, 1>(ctx, g, batch, p.shape);
+  else if (BKM) st = vec2 ? dispatch_shape<false, true, 2>(ctx, g, batch, p.shape)
+                          : dispatch_shape<false, true, 1>(ctx, g, batch, p.shape);
+  else st = vec2 ? dispatch_shape<false, false, 2>(ctx, g, batch, p.shape)
+                 : dispatch_shape<false, false, 1>(ctx, g, batch, p.shape);
+  if (st != MCNLA_B200_OK) return st;
+  if (p.splits > 1) {
+    const int64_t total = g.M * g.N * batch;
+    const int threads = 256;
+    const int blocks = int(std::min<int64_t>(cdiv(total, threads), int64_t(ctx->num_sms) * 8));
+    splitk_reduce_kernel<<<blocks, threads, 0, ctx->stream>>>(g.ws, p.splits, batch, g.M, g.N, g.alpha, g.beta, g.C,
+                                                             g.c_rs, g.c_cs, g.c_bs, g.guard_stop, g.guard_it,
+                                                             g.lower);
+    ctx->kernels_launched++;
+    MB_CHECK_CUDA(cudaGetLastError());
+  }
+  return MCNLA_B200_OK;
+}
+
+// ---- autotuner: the first call of a shape (up to kTuneMaxFlops) times every
+// tile configuration with the split counts its workspace allows and keeps the
+// fastest for the rest of the process.  Candidates run on the call's own
+// operands into a scratch output with the iteration guard off, so the tuning
+// neither depends on nor disturbs the state of an iteration loop.  One global
+// mutex: a key is tuned once, and every later call (in any context) uses the
+// same decision, so results do not depend on which context tuned it.
+struct TuneKey {
+  int device;
+  int64_t M, N, K;
+  int batch, layout, lower, max_splits;   // max_splits: what the call's workspace holds
+  bool operator<(const TuneKey& o) const {
+    return std::tie(device, M, N, K, batch, layout, lower, max_splits) <
+           std::tie(o.device, o.M, o.N, o.K, o.batch, o.layout, o.lower, o.max_splits);
+  }
+};
+
+constexpr double kTuneMaxFlops = 5e9;
+
+std::mutex g_tune_mu;
+std::map<TuneKey, Plan>& tune_cache() {
+  static std::map<TuneKey, Plan> m;
+  return m;
+}
+
+int tune(Context* ctx, const KArgs& g0, int batch, const Plan& heuristic, int max_splits, bool AK, bool BKM,
+         bool vec2, Plan* best) {
+  *best = heuristic;
+  const size_t out_bytes = size_t(batch) * g0.M * g0.N * sizeof(double);
+  double* scratch = nullptr;
+  MB_CHECK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&scratch), out_bytes, ctx->stream));
+  KArgs g = g0;
+  g.C = scratch;
+  g.c_rs = g0.N;
+  g.c_cs = 1;
+  g.c_bs = g0.M * g0.N;
+  g.beta = 0.0;
+  g.guard_stop = nullptr;
+  g.guard_it = 0;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int st = MCNLA_B200_OK;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) st = MCNLA_B200_ERR_CUDA;
+  float best_ms = 1e30f;
+  const Shape shapes[] = {S128x128w16, S128x128, S128x64, S64x64, S128x32, S64x32};
+  const int split_opts[] = {1, 2, 4, 8, 16, 32};
+  for (Shape sh : shapes) {
+    for (int so : split_opts) {
+      if (st != MCNLA_B200_OK) break;
+      if (so > 1 && g0.K < int64_t(so) * 4 * BK) continue;
+      const Plan p = plan_for(sh, g0.M, g0.N, g0.K, batch, so);
+      if (p.splits > max_splits) continue;
+      float ms = 0.f;
+      for (int rep = 0; rep < 2 && st == MCNLA_B200_OK; ++rep) {
+        cudaEventRecord(e0, ctx->stream);
+        st = run_plan(ctx, g, batch, p, AK, BKM, vec2);
+        cudaEventRecord(e1, ctx->stream);
+        if (cudaEventSynchronize(e1) != cudaSuccess) st = MCNLA_B200_ERR_CUDA;
+        cudaEventElapsedTime(&ms, e0, e1);
+      }
+      if (st == MCNLA_B200_OK && ms < best_ms) {
+        best_ms = ms;
+        *best = p;
+      }
+    }
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFreeAsync(scratch, ctx->stream);
+  return st;
+}
+
+}  // namespace
+
 int dgemm(Context* ctx, int64_t M, int64_t N, int64_t K, double alpha, CMat A, CMat B, double beta, DMat Cm,
           GemmBatch batch, double* ws, int force_splits, bool lower_only) {
   if (M < 0 || N < 0 || K < 0 || batch.count < 1) return MCNLA_B200_ERR_SHAPE;
@@ -346,32 +465,31 @@ int dgemm(Context* ctx, int64_t M, int64_t N, int64_t K, double alpha, CMat A, C
   g.guard_stop = ctx->guard_stop;
   g.guard_it = ctx->guard_it;
   g.lower = lower_only ? 1 : 0;
+  // split-K workspace available to this call (the planned need, or the stage's buffer)
+  const bool have_ws = ws && ws == ctx->gws;
+  const size_t ws_bytes = have_ws ? ctx->gws_bytes : 0;
+  g.ws = have_ws ? ws : nullptr;
+  if (ctx->autotune && force_splits == 0 && 2.0 * M * N * K * batch.count <= kTuneMaxFlops) {
+    const size_t out_bytes = size_t(batch.count) * M * N * sizeof(double);
+    const int max_splits = int(std::min<size_t>(32, std::max<size_t>(1, ws_bytes / out_bytes)));
+    const TuneKey key{ctx->device, M, N, K, batch.count, (AK ? 1 : 0) | (BKM ? 2 : 0) | (vec2 ? 4 : 0),
+                      lower_only ? 1 : 0, max_splits};
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = tune_cache().find(key);
+    if (it != tune_cache().end()) {
+      p = it->second;
+    } else {
+      Plan best;
+      MB_CHECK(tune(ctx, g, batch.count, p, max_splits, AK, BKM, vec2, &best));
+      tune_cache()[key] = best;
+      p = best;
+    }
+  }
   if (p.splits > 1) {
     const size_t need = size_t(p.splits) * batch.count * M * N * sizeof(double);
-    if (!ws || ws != ctx->gws || need > ctx->gws_bytes) return MCNLA_B200_ERR_WORKSPACE;
-    g.ws = ws;
+    if (!have_ws || need > ws_bytes) return MCNLA_B200_ERR_WORKSPACE;
   }
-  int st;
-  if (AK && BKM) st = vec2 ? dispatch_shape<true, true, 2>(ctx, g, batch.count, p.shape)
-                           : dispatch_shape<true, true, 1>(ctx, g, batch.count, p.shape);
-  else if (AK) st = vec2 ? dispatch_shape<true, false, 2>(ctx, g, batch.count, p.shape)
-                         : dispatch_shape<true, false, 1>(ctx, g, batch.count, p.shape);
-  else if (BKM) st = vec2 ? dispatch_shape<false, true, 2>(ctx, g, batch.count, p.shape)
-                          : dispatch_shape<false, true, 1>(ctx, g, batch.count, p.shape);
-  else st = vec2 ? dispatch_shape<false, false, 2>(ctx, g, batch.count, p.shape)
-                 : dispatch_shape<false, false, 1>(ctx, g, batch.count, p.shape);
-  if (st != MCNLA_B200_OK) return st;
-  if (p.splits > 1) {
-    const int64_t total = M * N * batch.count;
-    const int threads = 256;
-    const int blocks = int(std::min<int64_t>(cdiv(total, threads), int64_t(ctx->num_sms) * 8));
-    splitk_reduce_kernel<<<blocks, threads, 0, ctx->stream>>>(ws, p.splits, batch.count, M, N, alpha, beta, Cm.p,
-                                                             Cm.rs, Cm.cs, batch.c, ctx->guard_stop,
-                                                             ctx->guard_it, g.lower);
-    ctx->kernels_launched++;
-    MB_CHECK_CUDA(cudaGetLastError());
-  }
-  return MCNLA_B200_OK;
+  return run_plan(ctx, g, batch.count, p, AK, BKM, vec2);
 }
 
 }  // namespace mb

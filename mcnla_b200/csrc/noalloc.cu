@@ -70,6 +70,7 @@ extern "C" int mcnla_b200_dgemm_noalloc(void* stream, int64_t M, int64_t N, int6
   c.gws = scratch;
   c.gws_bytes = kScratchBytes;
   c.timing = false;
+  c.autotune = false;   // the tuner allocates a scratch output
   const size_t need = mb::dgemm_workspace_bytes(&c, M, N, K, 1);
   if (need > kScratchBytes) {
     mb::set_last_message("mcnla_b200_dgemm_noalloc: the split-K partial sums of this shape need " +

@@ -456,3 +456,32 @@ def test_integrators_maxit_zero(cuda, golden, name):
     integ(dev(golden["qs"], cuda), qbar)
     assert integ.iteration() == 0
     assert np.abs(host(qbar) - golden["qs"][:, :l]).max() < 1e-14
+
+
+@pytest.mark.parametrize("M,N,K", [(4096, 64, 4096), (384, 48, 8448), (64, 128, 4096), (1000, 96, 192)])
+def test_dgemm_autotuned_matches_heuristic(cuda, M, N, K):
+    """The tuned tile / split-K choice gives the product to the same accuracy as
+    the fixed heuristic, and later calls of the shape reuse the decision (bit
+    for bit the same result)."""
+    from mcnla_b200 import isvd, _lib
+    import ctypes
+    g = torch.Generator(device=cuda).manual_seed(M + N + K)
+    a = torch.randn(M, K, generator=g, dtype=torch.float64, device=cuda)
+    b = torch.randn(K, N, generator=g, dtype=torch.float64, device=cuda)
+    ctx = isvd.context()
+    outs = []
+    try:
+        for on in (False, True, True):
+            ctx.set_autotune(on)
+            c = torch.empty(M, N, dtype=torch.float64, device=cuda)
+            _lib.check(ctx.lib.mcnla_b200_dgemm(ctx.bind(), M, N, K, 1.0, ctypes.c_void_p(a.data_ptr()), K, 1,
+                                                ctypes.c_void_p(b.data_ptr()), N, 1, 0.0,
+                                                ctypes.c_void_p(c.data_ptr()), N, 1, 0), "dgemm")
+            outs.append(c)
+    finally:
+        ctx.set_autotune(True)
+    ref = a @ b
+    scale = (a.abs() @ b.abs()).max().item()
+    for c in outs:
+        assert (c - ref).abs().max().item() <= 1e-14 * scale * K ** 0.5
+    assert torch.equal(outs[1], outs[2])
