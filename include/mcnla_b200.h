@@ -112,11 +112,13 @@ MCNLA_B200_API int64_t mcnla_b200_kernels_launched(const mcnla_b200_ctx* ctx);
  * (l <= 80) or the eigendecomposition.  MCNLA_B200_KN_NEWTON_SCHULZ skips the
  * series; MCNLA_B200_KN_EIGEN always uses the eigendecomposition (parallel
  * Jacobi).                                                                   */
-/* GEMM tile autotuner (on by default): the first FP64 product of a shape of
- * at most 5 GFLOP times every tile configuration and split-K count that its
- * workspace allows, on the call's own operands into a scratch output, and
- * keeps the fastest for the rest of the process (shared by all contexts, so a
- * shape always runs the same configuration).  Off: a fixed shape heuristic. */
+/* GEMM tile autotuner (on by default): the first call of an FP64 product of
+ * at most 5 GFLOP inside an integrator's iteration loop (where the shape then
+ * repeats every iteration) times every tile configuration and split-K count
+ * that its workspace allows, on the call's own operands into a scratch
+ * output, and keeps the fastest for the rest of the process (shared by all
+ * contexts, so a shape always runs the same configuration).  Other products,
+ * and all products when off, use a fixed shape heuristic.                    */
 MCNLA_B200_API int mcnla_b200_set_autotune(mcnla_b200_ctx* ctx, int on);
 
 #define MCNLA_B200_KN_AUTO  0

@@ -88,8 +88,11 @@ struct Context {
   // all SMs.  Concurrent solves (the server's workers) each take a share so
   // that their persistent kernels can be resident together.
   int coop_cta_limit = 0;
-  // time the tile configurations of a GEMM shape on its first call (dgemm.cu)
+  // time the tile configurations of a GEMM shape on its first call (dgemm.cu);
+  // only the products of integrator iteration loops (tune_hot), whose shapes
+  // repeat for every iteration, are tuned
   bool autotune = true;
+  bool tune_hot = false;
   DevScalars* scal = nullptr;       // device scalars
   DevScalars* scal_host = nullptr;  // pinned mirror
   // stage part timers (CUDA events), filled by the last stage call

@@ -369,7 +369,8 @@ int run_plan(Context* ctx, KArgs g, int batch, const Plan& p, bool AK, bool BKM,
   return MCNLA_B200_OK;
 }
 
-// ---- autotuner: the first call of a shape (up to kTuneMaxFlops) times every
+// ---- autotuner: the first call of an iteration-loop shape (up to kTuneMaxFlops; the
+// context's tune_hot) times every
 // tile configuration with the split counts its workspace allows and keeps the
 // fastest for the rest of the process.  Candidates run on the call's own
 // operands into a scratch output with the iteration guard off, so the tuning
@@ -469,7 +470,7 @@ int dgemm(Context* ctx, int64_t M, int64_t N, int64_t K, double alpha, CMat A, C
   const bool have_ws = ws && ws == ctx->gws;
   const size_t ws_bytes = have_ws ? ctx->gws_bytes : 0;
   g.ws = have_ws ? ws : nullptr;
-  if (ctx->autotune && force_splits == 0 && 2.0 * M * N * K * batch.count <= kTuneMaxFlops) {
+  if (ctx->autotune && ctx->tune_hot && force_splits == 0 && 2.0 * M * N * K * batch.count <= kTuneMaxFlops) {
     const size_t out_bytes = size_t(batch.count) * M * N * sizeof(double);
     const int max_splits = int(std::min<size_t>(32, std::max<size_t>(1, ws_bytes / out_bytes)));
     const TuneKey key{ctx->device, M, N, K, batch.count, (AK ? 1 : 0) | (BKM ? 2 : 0) | (vec2 ? 4 : 0),

@@ -144,10 +144,19 @@ int run_orthogonalize(Context* c, const Dims& d, double* Q) {
 // norm converged (scal->stop_it), and every kernel launched for a later
 // iteration returns at once.  The host reads stop_it once per chunk.
 // Returns the number of executed bodies (the reference's iteration()).
+// Marks the products launched while it lives as iteration-loop products (the
+// GEMM autotuner tunes those shapes on their first call).
+struct HotLoop {
+  Context* c;
+  explicit HotLoop(Context* ctx) : c(ctx) { c->tune_hot = true; }
+  ~HotLoop() { c->tune_hot = false; }
+};
+
 template <class Body>
 int kn_loop(Context* c, int maxit, Body body, int* iters) {
   MB_CHECK_CUDA(cudaMemsetAsync(&c->scal->stop_it, 0x7f, sizeof(int), c->stream));   // "not yet"
   struct Reset { Context* c; ~Reset() { c->guard_stop = nullptr; c->guard_it = 0; } } reset{c};
+  HotLoop hot(c);
   c->guard_stop = &c->scal->stop_it;
   const int chunk = 8;
   int launched = 0, done = -1;
@@ -426,6 +435,7 @@ int run_rb_wy(Context* c, const Dims& d, const double* Qs, int maxit, double tol
   MB_CHECK(ctx_toc(c));
   int cur = 0, it = 0, fin = 0;
   bool is_odd = false;
+  HotLoop hot(c);
   for (; it < maxit;) {
     const int nx = 1 - cur;
     is_odd = !is_odd;
@@ -516,6 +526,7 @@ int run_rb_gramian_wy(Context* c, const Dims& d, const double* Qs, int maxit, do
   MB_CHECK(ctx_toc(c));
   int cur = 0, it = 0;
   bool is_odd = false;
+  HotLoop hot(c);
   for (; it < maxit;) {
     const int nx = 1 - cur;
     double* Ec = EB[cur];
@@ -910,6 +921,8 @@ int mcnla_b200_dgemm(mcnla_b200_ctx* ctx, int64_t M, int64_t N, int64_t K, doubl
     ctx->gws = ws;
     ctx->gws_bytes = ws ? wsb + 8 : 0;
   }
+  // a caller of the building block repeats its shapes: tune them like loop products
+  mb::HotLoop hot(ctx);
   return mb::dgemm(ctx, M, N, K, alpha, mb::cm(A, a_rs, a_cs), mb::cm(B, b_rs, b_cs), beta, mb::dm(C, c_rs, c_cs),
                    mb::GemmBatch(), ws, force_splits);
 }
