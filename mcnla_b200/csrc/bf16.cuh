@@ -10,8 +10,11 @@ namespace mb {
 // (out_fp64) or FP32 row-major with leading dimension ldd.  a_lo, a_lo2 may
 // be null (fewer parts; a_lo2 only with a_lo).  Device-side wait timeouts
 // are reported in c->scal->status.
+// accumulate: D += the product (FP64 D read back); lower: M == N and only the
+// tiles touching the lower triangle are computed (the others are left as they are).
 int bf16_gemm(Context* c, int64_t M, int64_t N, int64_t K, const uint16_t* a_hi, const uint16_t* a_lo,
-              const uint16_t* a_lo2, int64_t lda, const uint16_t* b, int64_t ldb, void* D, int64_t ldd, bool out_fp64);
+              const uint16_t* a_lo2, int64_t lda, const uint16_t* b, int64_t ldb, void* D, int64_t ldd, bool out_fp64,
+              bool accumulate = false, bool lower = false);
 
 // hi := bf16(A), lo := bf16(A - hi), lo2 := bf16(A - hi - lo) (lo, lo2 may be
 // null), written row-major (K contiguous) with pitch ldo, from row-major

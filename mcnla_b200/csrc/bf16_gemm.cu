@@ -68,6 +68,8 @@ struct Args {
   void* D;
   int64_t ldd;
   int* status;     // device status word: set to MCNLA_B200_ERR_DEVICE_TIMEOUT on a run-out wait
+  int accumulate;  // 1: D += result (D read back), 0: D = result
+  int lower;       // 1: tiles strictly above the diagonal (every column > every row) are skipped
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -185,6 +187,7 @@ __global__ void __launch_bounds__(TileCfg<CHUNKED>::THREADS, 1)
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_dyn) + 1023) & ~uintptr_t(1023));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int n0 = blockIdx.x * BN, m0 = blockIdx.y * BM;
+  if (g.lower && n0 >= m0 + BM) return;          // the whole CTA, before any allocation
   const int total_kt = g.KT;
   const int chunk_kt = CHUNKED ? CHUNK_KT : total_kt;
   const int chunks = (total_kt + chunk_kt - 1) / chunk_kt;
@@ -300,11 +303,11 @@ __global__ void __launch_bounds__(TileCfg<CHUNKED>::THREADS, 1)
       const int col = n0 + h * (BN / 2);
       if (col + BN / 2 <= g.N) {
 #pragma unroll
-        for (int j = 0; j < BN / 2; ++j) drow[col + j] = OutT(acc[j]);
+        for (int j = 0; j < BN / 2; ++j) drow[col + j] = OutT(g.accumulate ? double(drow[col + j]) + acc[j] : acc[j]);
       } else {
 #pragma unroll
         for (int j = 0; j < BN / 2; ++j)
-          if (col + j < g.N) drow[col + j] = OutT(acc[j]);
+          if (col + j < g.N) drow[col + j] = OutT(g.accumulate ? double(drow[col + j]) + acc[j] : acc[j]);
       }
     }
   } else if (!CHUNKED && warp >= 4) {
@@ -326,9 +329,15 @@ __global__ void __launch_bounds__(TileCfg<CHUNKED>::THREADS, 1)
         if (row < g.M) {
           if (col + 32 <= g.N) {
 #pragma unroll
-            for (int j = 0; j < 32; ++j) drow[col + j] = OutT(__uint_as_float(r[j]));
+            for (int j = 0; j < 32; ++j) {
+              const double v = __uint_as_float(r[j]);
+              drow[col + j] = OutT(g.accumulate ? double(drow[col + j]) + v : v);
+            }
           } else {
-            for (int j = 0; j < 32 && col + j < g.N; ++j) drow[col + j] = OutT(__uint_as_float(r[j]));
+            for (int j = 0; j < 32 && col + j < g.N; ++j) {
+              const double v = __uint_as_float(r[j]);
+              drow[col + j] = OutT(g.accumulate ? double(drow[col + j]) + v : v);
+            }
           }
         }
       }
@@ -383,7 +392,8 @@ int make_map(CUtensorMap* map, const void* base, int64_t rows, int64_t cols, int
 }  // namespace
 
 int bf16_gemm(Context* c, int64_t M, int64_t N, int64_t K, const uint16_t* a_hi, const uint16_t* a_lo,
-              const uint16_t* a_lo2, int64_t lda, const uint16_t* b, int64_t ldb, void* D, int64_t ldd, bool out_fp64) {
+              const uint16_t* a_lo2, int64_t lda, const uint16_t* b, int64_t ldb, void* D, int64_t ldd, bool out_fp64,
+              bool accumulate, bool lower) {
   if (M <= 0 || N <= 0 || K <= 0) return MCNLA_B200_ERR_SHAPE;
   if (M > (int64_t(1) << 31) - 1 || N > (int64_t(1) << 31) - 1) return MCNLA_B200_ERR_SHAPE;
   // TMA: 16-byte aligned bases and row pitches
@@ -410,6 +420,8 @@ int bf16_gemm(Context* c, int64_t M, int64_t N, int64_t K, const uint16_t* a_hi,
   g.D = D;
   g.ldd = ldd;
   g.status = &c->scal->status;
+  g.accumulate = accumulate ? 1 : 0;
+  g.lower = lower ? 1 : 0;
   dim3 grid(unsigned(cdiv(N, bn)), unsigned(cdiv(M, BM)));
   if (grid.y > 65535) return MCNLA_B200_ERR_SHAPE;
   auto go = [&](auto kern, int threads, size_t smem) -> int {

@@ -93,6 +93,8 @@ struct Context {
   // repeat for every iteration, are tuned
   bool autotune = true;
   bool tune_hot = false;
+  // precision form: the Gramian integrators form Bs = Qs' Qs from BF16 parts of Qs
+  bool mixed_gramian = false;
   DevScalars* scal = nullptr;       // device scalars
   DevScalars* scal_host = nullptr;  // pinned mirror
   // stage part timers (CUDA events), filled by the last stage call

@@ -272,11 +272,32 @@ int run_rb_kn(Context* c, const Dims& d, const double* Qs, int maxit, double tol
   return MCNLA_B200_OK;
 }
 
+// Precision form of Bs = Qs' Qs on the tensor cores: X = Qs' split into
+// three BF16 parts (24 bits), Bs = sum X_p X_q' over the six part products
+// with p + q <= 2 (the dropped ones are below 2^-24 relative): the 3-part
+// product runs in the chunked configuration (FP32 chunks summed in FP64), the
+// two smaller ones accumulate into Bs.  Lower-triangle tiles only.
+int gramian_bs_bf16(Context* c, const Dims& d, const double* Qs, double* Bs) {
+  const int64_t L = d.L, m = d.m, ldo = (m + 7) & ~int64_t(7);
+  const size_t part = size_t(L) * ldo;
+  uint16_t* x = nullptr;
+  MB_CHECK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&x), 3 * part * sizeof(uint16_t), c->stream));
+  struct Free { Context* c; uint16_t* p; ~Free() { cudaFreeAsync(p, c->stream); } } release{c, x};
+  uint16_t *hi = x, *lo = x + part, *lo2 = x + 2 * part;
+  // X (L x m) is Qs (m x L row-major) read column-major
+  MB_CHECK(launch_split_bf16(c, Qs, MCNLA_B200_COL_MAJOR, L, L, m, hi, lo, lo2, ldo));
+  MB_CHECK(bf16_gemm(c, L, L, m, hi, lo, lo2, ldo, hi, ldo, Bs, L, true, false, true));   // (hi + lo + lo2) hi'
+  MB_CHECK(bf16_gemm(c, L, L, m, hi, lo, nullptr, ldo, lo, ldo, Bs, L, true, true, true));  // + (hi + lo) lo'
+  MB_CHECK(bf16_gemm(c, L, L, m, hi, nullptr, nullptr, ldo, lo2, ldo, Bs, L, true, true, true));   // + hi lo2'
+  return MCNLA_B200_OK;
+}
+
 // Bs := Qs' Qs with the reference's triangle convention (see launch_gramian_prepare):
 // the lower triangle only (the reference's syrk), mirrored afterwards.
 int gramian_bs(Context* c, const Dims& d, const double* Qs, double* Bs, double* Bc, int64_t ldbc, double* ws) {
-  MB_CHECK(dgemm(c, d.L, d.L, d.m, 1.0, cm(Qs, 1, d.L), crow(Qs, d.L), 0.0, drow(Bs, d.L), GemmBatch(), ws, 0,
-                 true));
+  if (c->mixed_gramian) MB_CHECK(gramian_bs_bf16(c, d, Qs, Bs));
+  else MB_CHECK(dgemm(c, d.L, d.L, d.m, 1.0, cm(Qs, 1, d.L), crow(Qs, d.L), 0.0, drow(Bs, d.L), GemmBatch(), ws, 0,
+                      true));
   MB_CHECK(launch_gramian_prepare(c, d.L, d.l, Bs, Bc, ldbc));
   return MCNLA_B200_OK;
 }
@@ -767,7 +788,22 @@ int run_isvd_mixed(Context* c, const Dims& d, int integrator, int former, const 
   MB_CHECK(bf16_gemm(c, d.m, d.L, d.n, a_hi, a_lo, a_lo2, lda16, omega_t, ldo, Q, d.L, true));
   MB_CHECK(ctx_toc(c));
   MB_CHECK(run_orthogonalize(c, d, Q));
-  MB_CHECK(run_integrate(c, d, integrator, Q, maxit, tol, Qbar, iters));
+  {
+    // the Gramian integrators' Bs from BF16 parts of Qs (the precision form)
+    struct Mixed { Context* c; explicit Mixed(Context* x) : c(x) { c->mixed_gramian = true; }
+                   ~Mixed() { c->mixed_gramian = false; } } mixed(c);
+    MB_CHECK(run_integrate(c, d, integrator, Q, maxit, tol, Qbar, iters));
+  }
+  if (integrator == MCNLA_B200_ROW_BLOCK_GRAMIAN_KOLMOGOROV_NAGUMO ||
+      integrator == MCNLA_B200_ROW_BLOCK_GRAMIAN_WEN_YIN) {
+    // Bs carried the BF16 rounding of Qs into the iterates: one FP64 Gramian
+    // pass (Qbar := Qbar V S^(-1/2), an orthonormal basis of the same span)
+    // brings ||Qbar' Qbar - I|| back to FP64 rounding
+    Dims one = d;
+    one.N = 1;
+    one.L = d.l;
+    MB_CHECK(run_orthogonalize(c, one, Qbar));
+  }
   MB_CHECK(run_form(c, d, former, A, layout, lda, Qbar, S, U, V));
   MB_CHECK(ctx_sync_scalars(c));
   if (c->scal_host->status) return c->scal_host->status;
