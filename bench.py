@@ -76,6 +76,8 @@ def parse():
     ap.add_argument("--serve-former", default="rb_gramian",
                     help="former of the batched / served solves (the row-block driver's pairing by default)")
     ap.add_argument("--parts", type=int, default=2, help="BF16 parts of A in the mixed leg (2: 16 bits, 3: 24 bits)")
+    ap.add_argument("--former-parts", type=int, default=3, choices=[0, 1, 2, 3],
+                    help="BF16 parts of A' for the mixed leg's former (0: the former reads the FP64 A)")
     ap.add_argument("--serve-parts", type=int, default=3, help="BF16 parts of A in the batched / served mixed solves")
     args = ap.parse_args()
     if args.quick:
@@ -219,6 +221,47 @@ def fp64_peak_tflops():
     return 2 * n ** 3 / best / 1e12
 
 
+def stage_rooflines(m, n, k, l, N, integrator, former, stages, peak_tflops, hbm_gbs):
+    """Per-stage roofline of the FP64 solve: algorithmic flops and HBM bytes of each
+    stage (the minimum any implementation must do), the stage's roofline time
+    max(flops / FP64 tensor peak, bytes / HBM peak), and frac = roofline time /
+    measured time.  Integrator flops count the products each iteration needs at
+    this shape, times the measured iteration count."""
+    L = N * l
+    it = stages["integrate_iterations"]
+    per_it = {
+        # B = Qs'Qc, X = Qs B - Qc D, Z = X'X, Qc+ = [Qc X][C; inv(C)]
+        "kn": 4 * m * L * l + 8 * m * l * l,
+        # G = Qs B / N, Bg = Qs'G, Q+ = [Qc G][F; inv(C)], D, Dg
+        "rb_kn": 4 * m * L * l + 4 * m * l * l + 4 * L * l * l,
+        # Bg = Bs B, [D | Dg] = B'[B | Bg], E~+, B+
+        "rb_gramian_kn": 2 * L * L * l + 4 * L * l * l + 8 * L * l * l,
+        "rb_wy": 4 * m * L * l + 8 * m * l * l,
+        "rb_gramian_wy": 2 * L * L * l + 12 * L * l * l,
+    }[integrator]
+    once = {"rb_gramian_kn": L * L * m + 2 * m * L * l, "rb_gramian_wy": L * L * m + 2 * m * L * l}.get(integrator, 0)
+    integ_bytes = 8 * m * L + 8 * m * l + (8 * L * L if "gramian" in integrator else 0)
+    if former == "svd":
+        form_flops = 2 * m * n * l + 2 * m * l * k
+    else:
+        form_flops = 2 * m * n * l + 2 * n * l * l + 2 * m * l * k + 2 * n * l * k
+    rows = {
+        "sketch": (2 * m * n * L, 8 * (m * n + n * L + m * L), stages["sketch_gemm_s"]),
+        "orthogonalize": (4 * m * l * L, 8 * 3 * m * L, stages["orthogonalize_s"]),
+        "integrate": (once + per_it * it, integ_bytes, stages["integrate_s"]),
+        "form": (form_flops, 8 * (m * n + m * l + n * k + m * k), stages["form_s"]),
+    }
+    out = {}
+    for name, (fl, by, t) in rows.items():
+        t_c, t_m = fl / (peak_tflops * 1e12), by / (hbm_gbs * 1e9)
+        out[name] = {"bound": "tensor" if t_c >= t_m else "hbm", "flops": float(fl), "bytes": float(by),
+                     "s": round(t, 6), "achieved_tflops": round(fl / t / 1e12, 3),
+                     "achieved_gbs": round(by / t / 1e9, 1), "frac": round(max(t_c, t_m) / t, 4)}
+    out["peaks"] = {"fp64_tflops": round(peak_tflops, 3), "hbm_gbs": hbm_gbs,
+                    "source": "FP64: cuBLAS DGEMM measured in this run; HBM: MEASURED_PEAKS.json hbm_gbs of measured"}
+    return out
+
+
 def run_b200(args, world, rank, local):
     import numpy as np
     import torch
@@ -328,13 +371,14 @@ def run_b200(args, world, rank, local):
         e_s0, e_s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e_s0.record(stream)
         split = isvd.split_bf16(a, args.parts)
+        fsplit = isvd.split_bf16(a.t(), args.former_parts) if args.former_parts else None
         e_s1.record(stream)
         torch.cuda.synchronize()
         split_s = e_s0.elapsed_time(e_s1) / 1e3
 
         def mixed_solve(seed):
             return isvd.solve_mixed(a, k, p, N, seed=seed, integrator=args.integrator, former=args.former,
-                                    maxit=args.maxit, tol=args.tol, split=split)
+                                    maxit=args.maxit, tol=args.tol, split=split, former_split=fsplit)
         for w in range(max(args.warmup, 1)):
             mixed_solve(w)
         torch.cuda.synchronize()
@@ -361,7 +405,8 @@ def run_b200(args, world, rank, local):
         s64, u64, v64, it64 = isvd.solve(a, k, p, N, omega=om64, integrator=args.integrator, former=args.former,
                                          maxit=args.maxit, tol=args.tol)
         smx, umx, vmx, itmx = isvd.solve_mixed(a, k, p, N, seed=77, integrator=args.integrator,
-                                               former=args.former, maxit=args.maxit, tol=args.tol, split=split)
+                                               former=args.former, maxit=args.maxit, tol=args.tol, split=split,
+                                               former_split=fsplit)
         rel = ((smx - s64).abs() / s64).max().item()
         ang = float(torch.arccos(torch.clamp(torch.linalg.svdvals(u64.t() @ umx).min(), -1, 1)).item())
         orth = float(torch.linalg.norm(umx.t() @ umx - torch.eye(k, dtype=torch.float64, device=dev)).item())
@@ -372,6 +417,10 @@ def run_b200(args, world, rank, local):
                  "speedup_vs_fp64": round((world * args.steps / t_mixed) / value, 3),
                  "sketch": "A as %d BF16 parts (%d bits), Omega BF16, tcgen05 FP32 accumulation, FP64 out"
                            % (args.parts, 8 * args.parts),
+                 "former": ("Q' A on tcgen05 from A' as %d BF16 parts and Qbar as 3, split over K, FP64 sums "
+                            "of FP32 chunks" % args.former_parts) if fsplit is not None else "FP64 from A",
+                 "gramian": "Qs' Qs from 3 BF16 parts of Qs, then one FP64 re-orthonormalization of Qbar"
+                            if "gramian" in args.integrator else None,
                  "split_s": round(split_s, 5), "sketch_gemm_s": round(sk_bf16, 5),
                  "sketch_roofline": {"bound": "tensor", "achieved": round(ach, 2),
                                      "peak": bf16_peak, "unit": "TFLOP/s",
@@ -380,8 +429,10 @@ def run_b200(args, world, rank, local):
                                      "algorithmic": "%d parts x 2 m n N l flops" % args.parts},
                  "accuracy_vs_fp64_same_A_Omega": {"sigma_rel_err": rel, "max_principal_angle_U": ang,
                                                    "UtU_minus_I_fro": orth, "iterations": [itmx, it64]}}
-        del split, qb, om_t, om64
+        del split, fsplit, qb, om_t, om64
 
+    stage_roof = stage_rooflines(m, n, k, l, N, args.integrator, args.former, stages, peak64,
+                                 _measured_peak("hbm_gbs"))
     roofline = {"bound": "tensor", "kernel": "dgemm_kernel (sketch Y = A Omega, FP64 DMMA)",
                 "achieved": round(achieved, 3), "peak": round(peak64, 3), "unit": "TFLOP/s",
                 "frac": round(achieved / peak64, 4), "traffic": traffic,
@@ -428,7 +479,7 @@ def run_b200(args, world, rank, local):
         "p50_ms": round(step_ms[len(step_ms) // 2], 3),
         "p99_ms": round(step_ms[min(len(step_ms) - 1, int(0.99 * len(step_ms)))], 3),
         "iterations": iters[-1], "stages": stages, "integrators": variants, "mixed": mixed, "roofline": roofline,
-        "e2e": e2e,
+        "stage_roofline": stage_roof, "e2e": e2e,
         "gpu_launches": int(launches), "clocks": clk,
     }
     return result

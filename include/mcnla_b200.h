@@ -225,14 +225,28 @@ MCNLA_B200_API int mcnla_b200_gemm_bf16(mcnla_b200_ctx* ctx, int64_t M, int64_t 
 MCNLA_B200_API int mcnla_b200_sketch_bf16(mcnla_b200_ctx* ctx, const mcnla_b200_params* params, const uint16_t* a_hi,
                                           const uint16_t* a_lo, const uint16_t* a_lo2, int64_t lda16,
                                           const uint16_t* omega_t, int64_t ldo, double* Q);
-/* Whole solve with the mixed-precision sketch (Omega drawn in BF16 from seed)
- * and FP64 orthogonalizer, integrator and former (the former reads the FP64
- * A).  a_lo, a_lo2 may be NULL (fewer parts of A).                           */
+/* Precision-form former (svd_former.hpp:70-116, gramian_former.hpp:72-132):
+ * the product Q' A (l x n) that the former takes from A runs on tcgen05 from
+ * the BF16 parts of A' (n x m, pitch ldat: mcnla_b200_split_bf16 of A read
+ * with the other layout, e.g. row-major A as a column-major n x m matrix) and
+ * a three-part split of Qbar, the rest of the former in FP64.  Three parts of
+ * A' keep the former's products to 2^-24; at_lo, at_lo2 may be NULL.
+ * Synchronizes.                                                              */
+MCNLA_B200_API int mcnla_b200_form_bf16(mcnla_b200_ctx* ctx, const mcnla_b200_params* params, int former,
+                                        const uint16_t* at_hi, const uint16_t* at_lo, const uint16_t* at_lo2,
+                                        int64_t ldat, const double* Qbar, double* S, double* U, double* V);
+/* Whole solve with the mixed-precision sketch (Omega drawn in BF16 from seed),
+ * FP64 orthogonalizer and integrator steps (the Gramian integrators form
+ * Qs' Qs from BF16 parts of Qs and re-orthonormalize Qbar once in FP64), and
+ * the former in the precision form when at_hi is given (BF16 parts of A' as
+ * in mcnla_b200_form_bf16; A may then be NULL), else in FP64 from A.  a_lo,
+ * a_lo2, at_lo, at_lo2 may be NULL (fewer parts).                           */
 MCNLA_B200_API int mcnla_b200_isvd_mixed(mcnla_b200_ctx* ctx, const mcnla_b200_params* params, int integrator,
                                          int former, const double* A, int a_layout, int64_t lda, const uint16_t* a_hi,
-                                         const uint16_t* a_lo, const uint16_t* a_lo2, int64_t lda16, uint64_t seed,
-                                         int max_iteration, double tolerance, double* S, double* U, double* V,
-                                         int* iteration);
+                                         const uint16_t* a_lo, const uint16_t* a_lo2, int64_t lda16,
+                                         const uint16_t* at_hi, const uint16_t* at_lo, const uint16_t* at_lo2,
+                                         int64_t ldat, uint64_t seed, int max_iteration, double tolerance, double* S,
+                                         double* U, double* V, int* iteration);
 
 /* ---- batched and served solves ----------------------------------------------
  * Many independent solves of uneven sizes share the GPU: a pool of workers,

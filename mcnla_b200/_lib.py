@@ -98,8 +98,10 @@ SIGNATURES = {
     "mcnla_b200_gaussian_bf16": (_INT, [_P, ctypes.c_uint64, _I64, _I64, _P, _I64, _P]),
     "mcnla_b200_gemm_bf16": (_INT, [_P, _I64, _I64, _I64, _P, _P, _P, _I64, _P, _I64, _P, _I64, _INT]),
     "mcnla_b200_sketch_bf16": (_INT, [_P, ctypes.POINTER(Params), _P, _P, _P, _I64, _P, _I64, _P]),
+    "mcnla_b200_form_bf16": (_INT, [_P, ctypes.POINTER(Params), _INT, _P, _P, _P, _I64, _P, _P, _P, _P]),
     "mcnla_b200_isvd_mixed": (_INT, [_P, ctypes.POINTER(Params), _INT, _INT, _P, _INT, _I64, _P, _P, _P, _I64,
-                                     ctypes.c_uint64, _INT, _D, _P, _P, _P, ctypes.POINTER(_INT)]),
+                                     _P, _P, _P, _I64, ctypes.c_uint64, _INT, _D, _P, _P, _P,
+                                     ctypes.POINTER(_INT)]),
     "mcnla_b200_problem_bytes": (_I64, [ctypes.POINTER(Problem)]),
     "mcnla_b200_server_create": (_INT, [ctypes.POINTER(_P), _INT, _INT, _I64]),
     "mcnla_b200_server_submit": (_INT, [_P, ctypes.POINTER(Problem), ctypes.POINTER(_I64)]),

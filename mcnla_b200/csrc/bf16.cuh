@@ -16,6 +16,27 @@ int bf16_gemm(Context* c, int64_t M, int64_t N, int64_t K, const uint16_t* a_hi,
               const uint16_t* a_lo2, int64_t lda, const uint16_t* b, int64_t ldb, void* D, int64_t ldd, bool out_fp64,
               bool accumulate = false, bool lower = false);
 
+// Split-K plan of a bf16_gemm_split call: split z accumulates k-tiles
+// [z kt_per, min(KT, (z + 1) kt_per)) into its own D slice (D + z split_stride
+// elements); the slices are added afterwards by launch_sum_splits in a fixed
+// order.  chunked forces the chunked configuration (FP64 sums of FP32 chunks)
+// whatever the number of parts.
+struct Bf16Split {
+  int splits = 1;
+  int kt_per = 0;
+  int64_t split_stride = 0;
+  bool chunked = false;
+  int chunk_kt = 0;   // k-tiles per FP32 chunk in the chunked configuration (0: the default, 3)
+};
+int bf16_gemm_split(Context* c, int64_t M, int64_t N, int64_t K, const uint16_t* a_hi, const uint16_t* a_lo,
+                    const uint16_t* a_lo2, int64_t lda, const uint16_t* b, int64_t ldb, void* D, int64_t ldd,
+                    bool out_fp64, bool accumulate, bool lower, const Bf16Split& sp);
+Bf16Split plan_bf16_split(const Context* c, int64_t M, int64_t N, int64_t K, bool chunked, int max_splits);
+// D := sum over z of P + z stride (M x N, pitch ldp), added in order z = 0, 1, ...;
+// D is written N x M when transpose.
+int launch_sum_splits(Context* c, const double* P, int splits, int64_t stride, int64_t M, int64_t N, int64_t ldp,
+                      double* D, int64_t ldd, bool transpose);
+
 // hi := bf16(A), lo := bf16(A - hi), lo2 := bf16(A - hi - lo) (lo, lo2 may be
 // null), written row-major (K contiguous) with pitch ldo, from row-major
 // (layout 0) or column-major (layout 1) FP64 A.

@@ -20,8 +20,8 @@
 //            error of a long sum is no longer small next to the 24-bit
 //            representation of A, so the K loop is cut into chunks of 3
 //            k-tiles (36 MMAs of K = 16 over the three parts: 576 products
-//            per element).  A 128 x 128 tile per CTA; chunks alternate
-//            between two 128-column TMEM
+//            per element; a caller may ask for shorter chunks).  A 128 x
+//            128 tile per CTA; chunks alternate between two 128-column TMEM
 //            accumulators, and warps 2-9 (two per TMEM lane quarter, 64
 //            columns each) add every finished chunk into FP64 registers while
 //            the next chunk is accumulated; D is stored once at the end.
@@ -64,6 +64,9 @@ struct TileCfg {
 struct Args {
   int M, N;
   int KT;          // k-tiles
+  int kt_per;      // k-tiles per split (split z covers [z kt_per, min(KT, (z + 1) kt_per)))
+  int64_t split_stride;   // elements between the D slices of consecutive splits
+  int chunk_kt;    // k-tiles per FP32 accumulation chunk (chunked configuration)
   int parts;       // 1 (A_hi), 2 (A_hi + A_lo) or 3 (A_hi + A_lo + A_lo2)
   void* D;
   int64_t ldd;
@@ -188,8 +191,10 @@ __global__ void __launch_bounds__(TileCfg<CHUNKED>::THREADS, 1)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int n0 = blockIdx.x * BN, m0 = blockIdx.y * BM;
   if (g.lower && n0 >= m0 + BM) return;          // the whole CTA, before any allocation
-  const int total_kt = g.KT;
-  const int chunk_kt = CHUNKED ? CHUNK_KT : total_kt;
+  const int kt0 = int(blockIdx.z) * g.kt_per;     // this split's first k-tile
+  const int total_kt = min(g.KT - kt0, g.kt_per);
+  OutT* const dsplit = static_cast<OutT*>(g.D) + int64_t(blockIdx.z) * g.split_stride;
+  const int chunk_kt = CHUNKED ? g.chunk_kt : total_kt;
   const int chunks = (total_kt + chunk_kt - 1) / chunk_kt;
   constexpr int EPI_WARPS = CHUNKED ? 8 : 4;
 
@@ -227,10 +232,11 @@ __global__ void __launch_bounds__(TileCfg<CHUNKED>::THREADS, 1)
       uint8_t* sa = smem + s * STAGE_BYTES;
       uint8_t* sb = sa + T::A_PARTS * A_TILE_BYTES;
       mbar_expect_tx(&full_bar[s], uint32_t(g.parts * A_TILE_BYTES + T::B_TILE_BYTES));
-      tma_load_2d(sa, &tm_a_hi, &full_bar[s], kt * BK, m0);
-      if (g.parts > 1) tma_load_2d(sa + A_TILE_BYTES, &tm_a_lo, &full_bar[s], kt * BK, m0);
-      if (g.parts > 2) tma_load_2d(sa + 2 * A_TILE_BYTES, &tm_a_lo2, &full_bar[s], kt * BK, m0);
-      tma_load_2d(sb, &tm_b, &full_bar[s], kt * BK, n0);
+      const int kx = (kt0 + kt) * BK;
+      tma_load_2d(sa, &tm_a_hi, &full_bar[s], kx, m0);
+      if (g.parts > 1) tma_load_2d(sa + A_TILE_BYTES, &tm_a_lo, &full_bar[s], kx, m0);
+      if (g.parts > 2) tma_load_2d(sa + 2 * A_TILE_BYTES, &tm_a_lo2, &full_bar[s], kx, m0);
+      tma_load_2d(sb, &tm_b, &full_bar[s], kx, n0);
       ++issued;
     }
     if (!ok) {
@@ -254,11 +260,16 @@ __global__ void __launch_bounds__(TileCfg<CHUNKED>::THREADS, 1)
       fence_after();
       const uint32_t sa = smem_u32(smem + s * STAGE_BYTES);
       const uint32_t sb = sa + T::A_PARTS * A_TILE_BYTES;
-      for (int part = 0; part < g.parts; ++part) {
+      // smallest part first: the FP32 accumulator rounds each update to its
+      // own magnitude, so the small parts' updates cost least while it is small
+      bool fresh = first;
+      for (int part = g.parts - 1; part >= 0; --part) {
 #pragma unroll
-        for (int k = 0; k < BK / 16; ++k)   // 16 BF16 = 32 bytes along K per MMA
+        for (int k = 0; k < BK / 16; ++k) {   // 16 BF16 = 32 bytes along K per MMA
           umma_bf16(tmem + uint32_t(b * BN), sw128_desc(sa + part * A_TILE_BYTES + k * 32), sw128_desc(sb + k * 32),
-                    T::IDESC, !(first && part == 0 && k == 0));
+                    T::IDESC, fresh ? 0u : 1u);
+          fresh = false;
+        }
       }
       umma_commit(&empty_bar[s]);        // the stage is free once these MMAs have read it
       if (kt % chunk_kt == chunk_kt - 1 || kt == total_kt - 1) umma_commit(&acc_full[b]);
@@ -299,7 +310,7 @@ __global__ void __launch_bounds__(TileCfg<CHUNKED>::THREADS, 1)
     if (!ok) {
       if (lane == 0) atomicExch(g.status, MCNLA_B200_ERR_DEVICE_TIMEOUT);
     } else if (row < g.M) {
-      OutT* drow = static_cast<OutT*>(g.D) + int64_t(row) * g.ldd;
+      OutT* drow = dsplit + int64_t(row) * g.ldd;
       const int col = n0 + h * (BN / 2);
       if (col + BN / 2 <= g.N) {
 #pragma unroll
@@ -320,7 +331,7 @@ __global__ void __launch_bounds__(TileCfg<CHUNKED>::THREADS, 1)
       if (lane == 0) atomicExch(g.status, MCNLA_B200_ERR_DEVICE_TIMEOUT);
     } else {
       const int row = m0 + q * 32 + lane;
-      OutT* drow = static_cast<OutT*>(g.D) + int64_t(row) * g.ldd;
+      OutT* drow = dsplit + int64_t(row) * g.ldd;
 #pragma unroll 1
       for (int c = 0; c < BN / 32; ++c) {
         uint32_t r[32];
@@ -394,6 +405,13 @@ int make_map(CUtensorMap* map, const void* base, int64_t rows, int64_t cols, int
 int bf16_gemm(Context* c, int64_t M, int64_t N, int64_t K, const uint16_t* a_hi, const uint16_t* a_lo,
               const uint16_t* a_lo2, int64_t lda, const uint16_t* b, int64_t ldb, void* D, int64_t ldd, bool out_fp64,
               bool accumulate, bool lower) {
+  Bf16Split one;
+  return bf16_gemm_split(c, M, N, K, a_hi, a_lo, a_lo2, lda, b, ldb, D, ldd, out_fp64, accumulate, lower, one);
+}
+
+int bf16_gemm_split(Context* c, int64_t M, int64_t N, int64_t K, const uint16_t* a_hi, const uint16_t* a_lo,
+                    const uint16_t* a_lo2, int64_t lda, const uint16_t* b, int64_t ldb, void* D, int64_t ldd,
+                    bool out_fp64, bool accumulate, bool lower, const Bf16Split& sp) {
   if (M <= 0 || N <= 0 || K <= 0) return MCNLA_B200_ERR_SHAPE;
   if (M > (int64_t(1) << 31) - 1 || N > (int64_t(1) << 31) - 1) return MCNLA_B200_ERR_SHAPE;
   // TMA: 16-byte aligned bases and row pitches
@@ -404,7 +422,7 @@ int bf16_gemm(Context* c, int64_t M, int64_t N, int64_t K, const uint16_t* a_hi,
     return MCNLA_B200_ERR_LAYOUT;
   if (lda < K || ldb < K) return MCNLA_B200_ERR_SHAPE;
   // three parts: the chunked configuration (FP64 sums of FP32 chunks)
-  const bool chunked = a_lo2 != nullptr;
+  const bool chunked = a_lo2 != nullptr || sp.chunked;
   const int bn = chunked ? TileCfg<true>::BN : TileCfg<false>::BN;
   CUtensorMap ta_hi, ta_lo, ta_lo2, tb;
   MB_CHECK(make_map(&ta_hi, a_hi, M, K, lda, BM));
@@ -415,6 +433,13 @@ int bf16_gemm(Context* c, int64_t M, int64_t N, int64_t K, const uint16_t* a_hi,
   g.M = int(M);
   g.N = int(N);
   g.KT = int(cdiv(K, BK));
+  if (sp.splits < 1 || sp.kt_per < 0) return MCNLA_B200_ERR_ARG;
+  g.kt_per = sp.splits == 1 ? g.KT : sp.kt_per;
+  if (sp.splits > 1 && (g.kt_per < 1 || int64_t(g.kt_per) * (sp.splits - 1) >= g.KT ||
+                        int64_t(g.kt_per) * sp.splits < g.KT || sp.split_stride < M * ldd || lower))
+    return MCNLA_B200_ERR_ARG;   // every split gets at least one k-tile; slices do not overlap
+  g.split_stride = sp.split_stride;
+  g.chunk_kt = sp.chunk_kt > 0 ? sp.chunk_kt : CHUNK_KT;
   g.parts = a_lo2 ? 3 : (a_lo ? 2 : 1);
   static_assert(TileCfg<true>::A_PARTS >= MAX_PARTS, "the chunked stage holds every part");
   g.D = D;
@@ -422,8 +447,8 @@ int bf16_gemm(Context* c, int64_t M, int64_t N, int64_t K, const uint16_t* a_hi,
   g.status = &c->scal->status;
   g.accumulate = accumulate ? 1 : 0;
   g.lower = lower ? 1 : 0;
-  dim3 grid(unsigned(cdiv(N, bn)), unsigned(cdiv(M, BM)));
-  if (grid.y > 65535) return MCNLA_B200_ERR_SHAPE;
+  dim3 grid(unsigned(cdiv(N, bn)), unsigned(cdiv(M, BM)), unsigned(sp.splits));
+  if (grid.y > 65535 || grid.z > 65535) return MCNLA_B200_ERR_SHAPE;
   auto go = [&](auto kern, int threads, size_t smem) -> int {
     MB_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     kern<<<grid, threads, smem, c->stream>>>(ta_hi, ta_lo, ta_lo2, tb, g);
@@ -441,6 +466,58 @@ int bf16_gemm(Context* c, int64_t M, int64_t N, int64_t K, const uint16_t* a_hi,
   c->kernels_launched++;
   MB_CHECK_CUDA(cudaGetLastError());
   return MCNLA_B200_OK;
+}
+
+namespace {
+
+// D := sum_z P_z (z = 0, 1, ... in order: deterministic), P_z = P + z stride,
+// each M x N row-major with pitch ldp; D is N x M (transpose) or M x N.
+__global__ void k_sum_splits(const double* __restrict__ P, int splits, int64_t stride, int M, int N, int64_t ldp,
+                             double* __restrict__ D, int64_t ldd, int transpose) {
+  const int64_t total = int64_t(M) * N;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t i = e / N, j = e % N;
+    double v = 0.0;
+    for (int z = 0; z < splits; ++z) v += P[z * stride + i * ldp + j];
+    if (transpose) D[j * ldd + i] = v; else D[i * ldd + j] = v;
+  }
+}
+
+}  // namespace
+
+int launch_sum_splits(Context* c, const double* P, int splits, int64_t stride, int64_t M, int64_t N, int64_t ldp,
+                      double* D, int64_t ldd, bool transpose) {
+  if (M <= 0 || N <= 0 || splits < 1) return MCNLA_B200_ERR_SHAPE;
+  const int64_t total = M * N;
+  const int blocks = int(std::min<int64_t>(cdiv(total, 256), int64_t(c->num_sms) * 8));
+  k_sum_splits<<<blocks, 256, 0, c->stream>>>(P, splits, stride, int(M), int(N), ldp, D, ldd, transpose ? 1 : 0);
+  c->kernels_launched++;
+  MB_CHECK_CUDA(cudaGetLastError());
+  return MCNLA_B200_OK;
+}
+
+// Split count for an M x N x K product with tile width bn: the smallest
+// count (<= max_splits, each split at least 16 k-tiles) whose CTAs fill the
+// SMs' waves to at least 90 %, else the best found.
+Bf16Split plan_bf16_split(const Context* c, int64_t M, int64_t N, int64_t K, bool chunked, int max_splits) {
+  const int bn = chunked ? TileCfg<true>::BN : TileCfg<false>::BN;
+  const int64_t tiles = cdiv(M, BM) * cdiv(N, bn), kt = cdiv(K, BK), sms = std::max(1, c->num_sms);
+  Bf16Split best;
+  best.chunked = chunked;
+  double best_eff = 0.0;
+  for (int s = 1; s <= max_splits; ++s) {
+    const int64_t per = cdiv(kt, s);
+    if (s > 1 && (per < 16 || per * (s - 1) >= kt)) break;
+    const int64_t ctas = tiles * s;
+    const double eff = double(ctas) / double(cdiv(ctas, sms) * sms);
+    if (eff > best_eff + 1e-9) {
+      best_eff = eff;
+      best.splits = s;
+      best.kt_per = int(per);
+    }
+    if (eff >= 0.9) break;
+  }
+  return best;
 }
 
 }  // namespace mb

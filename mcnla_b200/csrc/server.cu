@@ -118,7 +118,8 @@ int mcnla_b200_server::run(mcnla_b200_ctx* ctx, mcnla_b200_problem& p, double*& 
     uint16_t* lo = split + size_t(m) * ldo;
     uint16_t* lo2 = nparts == 3 ? split + 2 * size_t(m) * ldo : nullptr;
     MB_CHECK(mcnla_b200_split_bf16(ctx, A, layout, lda, m, n, hi, lo, lo2, ldo));
-    return mcnla_b200_isvd_mixed(ctx, &p.params, p.integrator, p.former, A, layout, lda, hi, lo, lo2, ldo, p.seed,
+    return mcnla_b200_isvd_mixed(ctx, &p.params, p.integrator, p.former, A, layout, lda, hi, lo, lo2, ldo, nullptr,
+                                 nullptr, nullptr, 0, p.seed,
                                  p.max_iteration, p.tolerance, p.S, p.U, p.V, &p.iteration);
   }
   return mcnla_b200_isvd(ctx, &p.params, p.integrator, p.former, A, layout, lda, nullptr, p.seed, p.max_iteration,

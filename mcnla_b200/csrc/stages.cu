@@ -277,12 +277,12 @@ int run_rb_kn(Context* c, const Dims& d, const double* Qs, int maxit, double tol
 // with p + q <= 2 (the dropped ones are below 2^-24 relative): the 3-part
 // product runs in the chunked configuration (FP32 chunks summed in FP64), the
 // two smaller ones accumulate into Bs.  Lower-triangle tiles only.
-int gramian_bs_bf16(Context* c, const Dims& d, const double* Qs, double* Bs) {
+// BF16 elements of the three parts of Qs' that gramian_bs_bf16 writes (x).
+size_t gramian_bs16_count(const Dims& d) { return 3 * size_t(d.L) * size_t((d.m + 7) & ~int64_t(7)); }
+
+int gramian_bs_bf16(Context* c, const Dims& d, const double* Qs, double* Bs, uint16_t* x) {
   const int64_t L = d.L, m = d.m, ldo = (m + 7) & ~int64_t(7);
   const size_t part = size_t(L) * ldo;
-  uint16_t* x = nullptr;
-  MB_CHECK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&x), 3 * part * sizeof(uint16_t), c->stream));
-  struct Free { Context* c; uint16_t* p; ~Free() { cudaFreeAsync(p, c->stream); } } release{c, x};
   uint16_t *hi = x, *lo = x + part, *lo2 = x + 2 * part;
   // X (L x m) is Qs (m x L row-major) read column-major
   MB_CHECK(launch_split_bf16(c, Qs, MCNLA_B200_COL_MAJOR, L, L, m, hi, lo, lo2, ldo));
@@ -294,8 +294,10 @@ int gramian_bs_bf16(Context* c, const Dims& d, const double* Qs, double* Bs) {
 
 // Bs := Qs' Qs with the reference's triangle convention (see launch_gramian_prepare):
 // the lower triangle only (the reference's syrk), mirrored afterwards.
-int gramian_bs(Context* c, const Dims& d, const double* Qs, double* Bs, double* Bc, int64_t ldbc, double* ws) {
-  if (c->mixed_gramian) MB_CHECK(gramian_bs_bf16(c, d, Qs, Bs));
+// x: gramian_bs16_count(d) BF16 elements of workspace when c->mixed_gramian
+int gramian_bs(Context* c, const Dims& d, const double* Qs, double* Bs, double* Bc, int64_t ldbc, double* ws,
+               uint16_t* x) {
+  if (c->mixed_gramian) MB_CHECK(gramian_bs_bf16(c, d, Qs, Bs, x));
   else MB_CHECK(dgemm(c, d.L, d.L, d.m, 1.0, cm(Qs, 1, d.L), crow(Qs, d.L), 0.0, drow(Bs, d.L), GemmBatch(), ws, 0,
                       true));
   MB_CHECK(launch_gramian_prepare(c, d.L, d.l, Bs, Bc, ldbc));
@@ -324,7 +326,10 @@ int run_rb_gramian_kn(Context* c, const Dims& d, const double* Qs, int maxit, do
   pl.add(size_t(L) * L); pl.add(size_t(L) * l3); pl.add(size_t(L) * l3); pl.add(size_t(l2) * l);
   pl.add(size_t(l2) * l); pl.add(size_t(l2) * l); pl.add(size_t(l) * l); pl.add(size_t(l) * l);
   pl.add(size_t(L) * l); pl.add(kn_series_work_doubles(l)); pl.add(wsb / 8 + 1);
+  const size_t n16 = c->mixed_gramian ? gramian_bs16_count(d) : 0;
+  pl.add(n16, sizeof(uint16_t));
   MB_CHECK(ctx_reserve(c, pl.bytes));
+  uint16_t* bs16 = ctx_take<uint16_t>(c, n16);
   double* Bs = ctx_take<double>(c, size_t(L) * L);
   double* EB[2] = {ctx_take<double>(c, size_t(L) * l3), ctx_take<double>(c, size_t(L) * l3)};
   double* DD = ctx_take<double>(c, size_t(l2) * l);
@@ -337,7 +342,7 @@ int run_rb_gramian_kn(Context* c, const Dims& d, const double* Qs, int maxit, do
   MB_CHECK(check_arena(c));
   MB_CHECK(ctx_tic(c));
   // Bs := Qs' Qs; Bc := Bs(:, 0:l); F~ := I; E~ := 0   (:112-133)
-  MB_CHECK(gramian_bs(c, d, Qs, Bs, EB[0] + l, l3, ws));
+  MB_CHECK(gramian_bs(c, d, Qs, Bs, EB[0] + l, l3, ws, bs16));
   MB_CHECK(launch_fill(c, L, l, 0.0, EB[0], l3));
   MB_CHECK(launch_set_identity(c, l, FF[0], l));
   MB_CHECK(ctx_toc(c));
@@ -516,7 +521,10 @@ int run_rb_gramian_wy(Context* c, const Dims& d, const double* Qs, int maxit, do
   pl.add(size_t(l2) * l); pl.add(size_t(l2) * l); pl.add(size_t(L) * l2); pl.add(size_t(L) * l);
   pl.add(size_t(l) * l); pl.add(size_t(l) * l); pl.add(size_t(l) * l2); pl.add(size_t(L) * l);
   pl.add(size_t(np)); pl.add(wsb / 8 + 1);
+  const size_t n16 = c->mixed_gramian ? gramian_bs16_count(d) : 0;
+  pl.add(n16, sizeof(uint16_t));
   MB_CHECK(ctx_reserve(c, pl.bytes));
+  uint16_t* bs16 = ctx_take<uint16_t>(c, n16);
   double* Bs = ctx_take<double>(c, size_t(L) * L);
   double* EB[2] = {ctx_take<double>(c, size_t(L) * l3), ctx_take<double>(c, size_t(L) * l3)};
   double* DD[2] = {ctx_take<double>(c, size_t(l) * l2), ctx_take<double>(c, size_t(l) * l2)};
@@ -535,7 +543,7 @@ int run_rb_gramian_wy(Context* c, const Dims& d, const double* Qs, int maxit, do
   MB_CHECK_CUDA(cudaMemsetAsync(c->scal, 0, sizeof(DevScalars), c->stream));
   MB_CHECK(ctx_tic(c));
   // Initializing (:121-155)
-  MB_CHECK(gramian_bs(c, d, Qs, Bs, EB[0] + l, l3, ws));
+  MB_CHECK(gramian_bs(c, d, Qs, Bs, EB[0] + l, l3, ws, bs16));
   MB_CHECK(dgemm(c, L, l, L, inv_n, crow(Bs, L), crow(EB[0] + l, l3), 0.0, drow(EB[0] + l2, l3), GemmBatch(), ws));
   MB_CHECK(dgemm(c, l, l2, L, inv_n, cm(EB[0] + l, 1, l3), crow(EB[0] + l, l3), 0.0, drow(DD[0], l2), GemmBatch(), ws));
   MB_CHECK(launch_set_identity(c, l, FF[0], l));
@@ -637,7 +645,52 @@ int run_integrate(Context* c, const Dims& d, int kind, const double* Qs, int max
 // of Vt give Y2 (orthonormal rows spanning the same space), M := Vt Y2' is
 // formed by a GEMM, and M's SVD is taken by one-sided Jacobi:
 // Vt = M Y2 = W S (Y2' Z)'.
-int run_form_svd(Context* c, const Dims& d, const CMat& Am, const double* Qbar, double* S, double* U, double* V) {
+// BF16 parts of A' (n x m, K-major: row j of A' is column j of A) for the
+// precision-form former; lo and lo2 may be null.
+struct AtParts {
+  const uint16_t* hi = nullptr;
+  const uint16_t* lo = nullptr;
+  const uint16_t* lo2 = nullptr;
+  int64_t ld = 0;
+};
+
+// Precision-form former product Q' A (l x n) on tcgen05 from the BF16 parts
+// of A' and a three-part BF16 split of Qbar:
+//   (Q_hi + Q_lo + Q_lo2) A'_hi' + (Q_hi + Q_lo) A'_lo' + Q_hi A'_lo2'
+// (every product down to 2^-24 of the leading one), the first in the chunked
+// configuration (FP64 sums of FP32 chunks; the K loop runs over all m rows),
+// split over K so that the CTAs fill the SMs, the slices added in a fixed
+// order into out: Q' A (l x n, pitch ldo) or, with transpose, A' Q (n x l).
+constexpr int kFormMaxSplits = 16;
+
+// Workspace of form_product_bf16: BF16 elements (the three parts of Q') and
+// doubles (the split slices).
+size_t form16_count(const Dims& d) { return 3 * size_t(d.l) * size_t((d.m + 7) & ~int64_t(7)); }
+size_t form_split_doubles(const Context* c, const Dims& d) {
+  return size_t(plan_bf16_split(c, d.l, d.n, d.m, true, kFormMaxSplits).splits) * d.l * d.n;
+}
+
+int form_product_bf16(Context* c, const Dims& d, const AtParts& at, const double* Qbar, double* out, int64_t ldo,
+                      bool transpose, uint16_t* q16, double* parts) {
+  const int64_t l = d.l, m = d.m, n = d.n, ldq = (m + 7) & ~int64_t(7);
+  if (!at.hi || (at.lo2 && !at.lo) || at.ld < m) return MCNLA_B200_ERR_ARG;
+  Bf16Split sp = plan_bf16_split(c, l, n, m, true, kFormMaxSplits);
+  sp.split_stride = l * n;
+  sp.chunk_kt = 1;   // sigma takes this product's error to first order: 12 accumulator updates per chunk
+  const size_t qpart = size_t(l) * ldq;
+  uint16_t *qh = q16, *ql = q16 + qpart, *ql2 = q16 + 2 * qpart;
+  // Q' parts: Qbar (m x l, row-major) read as the column-major l x m matrix Q'
+  MB_CHECK(launch_split_bf16(c, Qbar, MCNLA_B200_COL_MAJOR, l, l, m, qh, ql, ql2, ldq));
+  MB_CHECK(bf16_gemm_split(c, l, n, m, qh, ql, ql2, ldq, at.hi, at.ld, parts, n, true, false, false, sp));
+  if (at.lo) MB_CHECK(bf16_gemm_split(c, l, n, m, qh, ql, nullptr, ldq, at.lo, at.ld, parts, n, true, true, false, sp));
+  if (at.lo2)
+    MB_CHECK(bf16_gemm_split(c, l, n, m, qh, nullptr, nullptr, ldq, at.lo2, at.ld, parts, n, true, true, false, sp));
+  MB_CHECK(launch_sum_splits(c, parts, sp.splits, sp.split_stride, l, n, n, out, ldo, transpose));
+  return MCNLA_B200_OK;
+}
+
+int run_form_svd(Context* c, const Dims& d, const CMat& Am, const double* Qbar, double* S, double* U, double* V,
+                 const AtParts* at) {
   const int l = d.l, k = d.k;
   const int64_t m = d.m, n = d.n;
   const size_t ll = size_t(l) * l;
@@ -647,7 +700,11 @@ int run_form_svd(Context* c, const Dims& d, const CMat& Am, const double* Qbar, 
   for (int i = 0; i < 6; ++i) pl.add(ll);
   pl.add(size_t(2) * l); pl.add(wsb / 8 + 1);
   for (int i = 0; i < 4; ++i) pl.add(ll);   // on-chip solver spill copies (l > 112)
+  const size_t n16 = at ? form16_count(d) : 0, nsp = at ? form_split_doubles(c, d) : 0;
+  pl.add(n16, sizeof(uint16_t)); pl.add(nsp);
   MB_CHECK(ctx_reserve(c, pl.bytes));
+  uint16_t* q16 = ctx_take<uint16_t>(c, n16);
+  double* slices = ctx_take<double>(c, nsp);
   double* Vt = ctx_take<double>(c, size_t(l) * n);
   double* Y1 = ctx_take<double>(c, size_t(l) * n);
   double* Y2 = ctx_take<double>(c, size_t(l) * n);
@@ -663,7 +720,8 @@ int run_form_svd(Context* c, const Dims& d, const CMat& Am, const double* Qbar, 
   MB_CHECK(check_arena(c));
   MB_CHECK(ctx_tic(c));
   // Vt := Q' A   (:99)
-  MB_CHECK(dgemm(c, l, n, m, 1.0, cm(Qbar, 1, l), Am, 0.0, drow(Vt, n), GemmBatch(), ws));
+  if (at) MB_CHECK(form_product_bf16(c, d, *at, Qbar, Vt, n, false, q16, slices));
+  else MB_CHECK(dgemm(c, l, n, m, 1.0, cm(Qbar, 1, l), Am, 0.0, drow(Vt, n), GemmBatch(), ws));
   MB_CHECK(ctx_toc(c));
   // svd(Vt)   (:106)
   const double* Yin = Vt;
@@ -690,7 +748,7 @@ int run_form_svd(Context* c, const Dims& d, const CMat& Am, const double* Qbar, 
 // (gramian_former.hpp:72-132; row_block_gramian_former.hpp:78-146;
 //  col_block_gramian_former.hpp:73-131): on one device the three agree.
 int run_form_gramian(Context* c, const Dims& d, const CMat& Am, const double* Qbar, double* S, double* U,
-                     double* V) {
+                     double* V, const AtParts* at) {
   const int l = d.l, k = d.k;
   const int64_t m = d.m, n = d.n;
   const size_t ll = size_t(l) * l;
@@ -699,7 +757,11 @@ int run_form_gramian(Context* c, const Dims& d, const CMat& Am, const double* Qb
   pl.add(size_t(n) * l); pl.add(ll); pl.add(ll); pl.add(ll); pl.add(size_t(2) * l);
   pl.add(wsb / 8 + 1);
   for (int i = 0; i < 2; ++i) pl.add(ll);   // on-chip solver spill copy (l > 112)
+  const size_t n16 = at ? form16_count(d) : 0, nsp = at ? form_split_doubles(c, d) : 0;
+  pl.add(n16, sizeof(uint16_t)); pl.add(nsp);
   MB_CHECK(ctx_reserve(c, pl.bytes));
+  uint16_t* q16 = ctx_take<uint16_t>(c, n16);
+  double* slices = ctx_take<double>(c, nsp);
   double* Z = ctx_take<double>(c, size_t(n) * l);
   double* W = ctx_take<double>(c, ll);
   double* Ue = ctx_take<double>(c, ll);
@@ -710,7 +772,8 @@ int run_form_gramian(Context* c, const Dims& d, const CMat& Am, const double* Qb
   MB_CHECK(check_arena(c));
   MB_CHECK(ctx_tic(c));
   // Z := A' Q   (gramian_former.hpp:101)
-  MB_CHECK(dgemm(c, n, l, m, 1.0, ctr(Am), crow(Qbar, l), 0.0, drow(Z, l), GemmBatch(), ws));
+  if (at) MB_CHECK(form_product_bf16(c, d, *at, Qbar, Z, l, true, q16, slices));
+  else MB_CHECK(dgemm(c, n, l, m, 1.0, ctr(Am), crow(Qbar, l), 0.0, drow(Z, l), GemmBatch(), ws));
   MB_CHECK(ctx_toc(c));
   // W := Z' Z; eig(W) = W S W' (descending); S := sqrt(S)   (:108-115)
   MB_CHECK(dgemm(c, l, l, n, 1.0, cm(Z, 1, l), crow(Z, l), 0.0, drow(W, l), GemmBatch(), ws));
@@ -729,17 +792,18 @@ int run_form_gramian(Context* c, const Dims& d, const CMat& Am, const double* Qb
 }
 
 int run_form(Context* c, const Dims& d, int kind, const double* A, int layout, int64_t lda, const double* Qbar,
-             double* S, double* U, double* V) {
-  if (!A || !Qbar) return MCNLA_B200_ERR_ARG;
+             double* S, double* U, double* V, const AtParts* at = nullptr) {
+  // the precision form (at) reads the BF16 parts of A' instead of A
+  if (!Qbar || (!A && !at)) return MCNLA_B200_ERR_ARG;
   if (layout != MCNLA_B200_ROW_MAJOR && layout != MCNLA_B200_COL_MAJOR) return MCNLA_B200_ERR_ARG;
-  if (layout == MCNLA_B200_ROW_MAJOR ? lda < d.n : lda < d.m) return MCNLA_B200_ERR_SHAPE;
+  if (A && (layout == MCNLA_B200_ROW_MAJOR ? lda < d.n : lda < d.m)) return MCNLA_B200_ERR_SHAPE;
   if (d.k > d.l) return MCNLA_B200_ERR_SHAPE;
   const CMat Am = layout == MCNLA_B200_ROW_MAJOR ? crow(A, lda) : ccol(A, lda);
   switch (kind) {
-    case MCNLA_B200_SVD_FORMER: return run_form_svd(c, d, Am, Qbar, S, U, V);
+    case MCNLA_B200_SVD_FORMER: return run_form_svd(c, d, Am, Qbar, S, U, V, at);
     case MCNLA_B200_GRAMIAN_FORMER:
     case MCNLA_B200_ROW_BLOCK_GRAMIAN_FORMER:
-    case MCNLA_B200_COL_BLOCK_GRAMIAN_FORMER: return run_form_gramian(c, d, Am, Qbar, S, U, V);
+    case MCNLA_B200_COL_BLOCK_GRAMIAN_FORMER: return run_form_gramian(c, d, Am, Qbar, S, U, V, at);
     default: return MCNLA_B200_ERR_ARG;
   }
 }
@@ -770,8 +834,9 @@ int run_isvd(Context* c, const Dims& d, int integrator, int former, const double
 
 // Mixed solve: Omega drawn in BF16, sketch on tcgen05, FP64 afterwards.
 int run_isvd_mixed(Context* c, const Dims& d, int integrator, int former, const double* A, int layout, int64_t lda,
-                   const uint16_t* a_hi, const uint16_t* a_lo, const uint16_t* a_lo2, int64_t lda16, uint64_t seed,
-                   int maxit, double tol, double* S, double* U, double* V, int* iters, char* pbase) {
+                   const uint16_t* a_hi, const uint16_t* a_lo, const uint16_t* a_lo2, int64_t lda16,
+                   const AtParts* at, uint64_t seed, int maxit, double tol, double* S, double* U, double* V,
+                   int* iters, char* pbase) {
   auto take = [&](size_t bytes) {
     char* p = pbase;
     pbase += (bytes + 511) & ~size_t(511);
@@ -804,7 +869,7 @@ int run_isvd_mixed(Context* c, const Dims& d, int integrator, int former, const 
     one.L = d.l;
     MB_CHECK(run_orthogonalize(c, one, Qbar));
   }
-  MB_CHECK(run_form(c, d, former, A, layout, lda, Qbar, S, U, V));
+  MB_CHECK(run_form(c, d, former, A, layout, lda, Qbar, S, U, V, at));
   MB_CHECK(ctx_sync_scalars(c));
   if (c->scal_host->status) return c->scal_host->status;
   return MCNLA_B200_OK;
@@ -1015,18 +1080,45 @@ int mcnla_b200_sketch_bf16(mcnla_b200_ctx* ctx, const mcnla_b200_params* params,
   return ctx->scal_host->status ? ctx->scal_host->status : MCNLA_B200_OK;
 }
 
+int mcnla_b200_form_bf16(mcnla_b200_ctx* ctx, const mcnla_b200_params* params, int former, const uint16_t* at_hi,
+                         const uint16_t* at_lo, const uint16_t* at_lo2, int64_t ldat, const double* Qbar, double* S,
+                         double* U, double* V) {
+  if (!ctx || !at_hi || !Qbar) return MCNLA_B200_ERR_ARG;
+  if (at_lo2 && !at_lo) return MCNLA_B200_ERR_ARG;
+  Dims d;
+  MB_CHECK(mb::get_dims(params, d));
+  MB_CHECK_CUDA(cudaSetDevice(ctx->device));
+  MB_CHECK_CUDA(cudaMemsetAsync(ctx->scal, 0, sizeof(mb::DevScalars), ctx->stream));
+  mb::AtParts at;
+  at.hi = at_hi;
+  at.lo = at_lo;
+  at.lo2 = at_lo2;
+  at.ld = ldat;
+  MB_CHECK(mb::ctx_tic(ctx));
+  MB_CHECK(mb::run_form(ctx, d, former, nullptr, MCNLA_B200_ROW_MAJOR, 0, Qbar, S, U, V, &at));
+  MB_CHECK(mb::ctx_sync_scalars(ctx));
+  return ctx->scal_host->status ? ctx->scal_host->status : MCNLA_B200_OK;
+}
+
 int mcnla_b200_isvd_mixed(mcnla_b200_ctx* ctx, const mcnla_b200_params* params, int integrator, int former,
                           const double* A, int a_layout, int64_t lda, const uint16_t* a_hi, const uint16_t* a_lo,
-                          const uint16_t* a_lo2, int64_t lda16, uint64_t seed, int max_iteration, double tolerance,
+                          const uint16_t* a_lo2, int64_t lda16, const uint16_t* at_hi, const uint16_t* at_lo,
+                          const uint16_t* at_lo2, int64_t ldat, uint64_t seed, int max_iteration, double tolerance,
                           double* S, double* U, double* V, int* iteration) {
-  if (!ctx || !A || !a_hi || !iteration) return MCNLA_B200_ERR_ARG;
+  if (!ctx || (!A && !at_hi) || !a_hi || !iteration) return MCNLA_B200_ERR_ARG;
+  if ((a_lo2 && !a_lo) || (at_lo2 && !at_lo)) return MCNLA_B200_ERR_ARG;
   Dims d;
   MB_CHECK(mb::get_dims(params, d));
   MB_CHECK_CUDA(cudaSetDevice(ctx->device));
   MB_CHECK(mb::ctx_reserve_pipeline(ctx, mb::pipeline_bytes_mixed(d)));
-  if (a_lo2 && !a_lo) return MCNLA_B200_ERR_ARG;
-  return mb::run_isvd_mixed(ctx, d, integrator, former, A, a_layout, lda, a_hi, a_lo, a_lo2, lda16, seed,
-                            max_iteration, tolerance, S, U, V, iteration, static_cast<char*>(ctx->parena));
+  mb::AtParts at;
+  at.hi = at_hi;
+  at.lo = at_lo;
+  at.lo2 = at_lo2;
+  at.ld = ldat;
+  return mb::run_isvd_mixed(ctx, d, integrator, former, A, a_layout, lda, a_hi, a_lo, a_lo2, lda16,
+                            at_hi ? &at : nullptr, seed, max_iteration, tolerance, S, U, V, iteration,
+                            static_cast<char*>(ctx->parena));
 }
 
 int mcnla_b200_syev_batched(mcnla_b200_ctx* ctx, int n, int batch, const double* A, double* W, double* V,

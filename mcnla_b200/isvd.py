@@ -686,17 +686,39 @@ def gemm_bf16(a_hi, a_lo, lda, b, ldb, out_dtype=torch.float64, a_lo2=None):
     return d
 
 
+def form_bf16(at_split, qbar, k, p, N, former="svd", with_v=True):
+    """Precision-form former: Q' A on tcgen05 from the BF16 parts of A' (`at_split`, e.g.
+    split_bf16(a.t(), 3)) and a three-part split of Qbar, the rest in FP64.  Returns (S, U, V)."""
+    at_hi, at_lo, at_lo2, ldt = at_split
+    n, m = at_hi.shape[0], qbar.shape[0]
+    _check_dev(qbar, "Qbar")
+    if not qbar.is_contiguous():
+        raise ValueError("Qbar must be a contiguous row-major m x l matrix")
+    prm = _lib.Params(m, n, k, p, N)
+    dev = qbar.device
+    s = torch.empty(k, dtype=torch.float64, device=dev)
+    u = torch.empty(m, k, dtype=torch.float64, device=dev)
+    v = torch.empty(n, k, dtype=torch.float64, device=dev) if with_v else None
+    ctx = context(dev)
+    _lib.check(ctx.lib.mcnla_b200_form_bf16(ctx.bind(), ctypes.byref(prm), FORMERS[former], _ptr(at_hi), _ptr(at_lo),
+                                            _ptr(at_lo2), ldt, _ptr(qbar), _ptr(s), _ptr(u), _ptr(v)), "form_bf16")
+    return s, u, v
+
+
 def solve_mixed(a, k, p, N, seed=0, integrator="kn", former="svd", maxit=256, tol=1e-4, split=None, with_v=True,
-                parts=2):
-    """Whole iSVD with the BF16 tensor-core sketch (Omega drawn in BF16 from seed) and FP64
-    orthogonalizer / integrator / former.  `split` (a Split) reuses a resident BF16 copy of A;
-    otherwise A is split into `parts` BF16 parts.  Returns (S, U, V, iterations)."""
+                parts=2, former_split=None):
+    """Whole iSVD with the BF16 tensor-core sketch (Omega drawn in BF16 from seed), FP64
+    orthogonalizer / integrator steps, and the former in FP64 from A or, when `former_split`
+    (the BF16 parts of A', e.g. split_bf16(a.t(), 3)) is given, in the precision form.
+    `split` (a Split) reuses a resident BF16 copy of A; otherwise A is split into `parts` BF16
+    parts.  Returns (S, U, V, iterations)."""
     m, n = a.shape
     _check_dev(a, "A")
     layout, lda = _layout(a)
     if split is None:
         split = split_bf16(a, parts)
     hi, lo, lo2, ld16 = split
+    at_hi, at_lo, at_lo2, ldt = former_split if former_split is not None else (None, None, None, 0)
     prm = _lib.Params(m, n, k, p, N)
     dev = a.device
     s = torch.empty(k, dtype=torch.float64, device=dev)
@@ -706,7 +728,7 @@ def solve_mixed(a, k, p, N, seed=0, integrator="kn", former="svd", maxit=256, to
     it = ctypes.c_int()
     _lib.check(ctx.lib.mcnla_b200_isvd_mixed(ctx.bind(), ctypes.byref(prm), INTEGRATORS[integrator], FORMERS[former],
                                              _ptr(a), layout, lda, _ptr(hi), _ptr(lo), _ptr(lo2), ld16,
-                                             ctypes.c_uint64(seed),
+                                             _ptr(at_hi), _ptr(at_lo), _ptr(at_lo2), ldt, ctypes.c_uint64(seed),
                                              maxit, tol, _ptr(s), _ptr(u), _ptr(v), ctypes.byref(it)), "isvd_mixed")
     return s, u, v, it.value
 

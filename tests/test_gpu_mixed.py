@@ -112,3 +112,57 @@ def test_mixed_matches_fp64_isvd(cuda, case):
           "it %d/%d" % (case, rel, rel1, rel3, ang, orth, it, it64))
     assert rel1 <= 1e-2
     assert rel3 <= 1e-6, rel3
+
+
+@pytest.mark.parametrize("m,n,k,p", [(1000, 2000, 10, 10), (20011, 1537, 24, 8), (777, 3001, 64, 16)])
+@pytest.mark.parametrize("former", ["svd", "rb_gramian"])
+def test_form_bf16_matches_fp64_former(cuda, m, n, k, p, former):
+    """Precision-form former (Q' A on tcgen05 from three BF16 parts of A' and of Qbar, split over
+    K = m) against the FP64 former on the same A and Qbar: sigma to 1e-6 relative, U and V
+    subspaces, U orthonormal to FP64 rounding."""
+    from mcnla_b200 import isvd, synthetic
+    a = torch.as_tensor(synthetic.lowrank_np(m, n, 1.0 / np.arange(1, min(m, n, 300) + 1), seed=m + n), device=cuda)
+    g = torch.Generator(device=cuda).manual_seed(7)
+    qbar = torch.linalg.qr(a @ torch.randn(n, k + p, generator=g, dtype=torch.float64, device=cuda))[0].contiguous()
+    prm = isvd.Parameters(device=cuda).setSize(m, n).setRank(k).setOverRank(p).setNumSketch(1).sync()
+    stage = {"svd": isvd.SvdFormer, "rb_gramian": isvd.RowBlockGramianFormer}[former](prm)
+    stage.initialize()
+    stage(a, qbar)
+    s64, u64, v64 = (x.cpu().numpy() for x in (stage.vectorS(), stage.matrixU(), stage.matrixV()))
+    at = isvd.split_bf16(a.t(), 3)
+    assert at.hi.shape == (n, m)
+    s, u, v = isvd.form_bf16(at, qbar, k, p, 1, former=former)
+    rel, ang, orth = _metrics(*(x.cpu().numpy() for x in (s, u, v)), s64, u64, v64)
+    print("form_bf16 %s %dx%d l=%d: sigma rel %.2e, angle %.2e, ||U'U-I|| %.2e" % (former, m, n, k + p, rel, ang, orth))
+    assert rel <= 1e-6, rel
+    assert ang <= 1e-5, ang
+    assert orth <= 1e-10, orth
+    # deterministic: the same call gives the same bits
+    s2, u2, v2 = isvd.form_bf16(at, qbar, k, p, 1, former=former)
+    assert torch.equal(s, s2) and torch.equal(u, u2) and torch.equal(v, v2)
+
+
+@pytest.mark.parametrize("case", ["config1", "ill_conditioned"])
+def test_mixed_precision_former_solve(cuda, case):
+    """Whole mixed solve with the sketch and the former on tcgen05 (A' in three BF16 parts)
+    against plain FP64 iSVD on the same A and Omega."""
+    from mcnla_b200 import isvd, synthetic
+    if case == "config1":
+        m, n, k, p, N = 1000, 2000, 10, 10, 16
+        a = synthetic.lowrank_np(m, n, 1.0 / np.arange(1, 1001), seed=0)
+    else:
+        m, n, k, p, N = 1000, 2000, 64, 16, 32
+        a = synthetic.lowrank_np(m, n, synthetic.config3_sigma(), seed=0, noise=1e-8)
+    at = torch.as_tensor(a, device=cuda)
+    seed = 5
+    _, _, omega = isvd.gaussian_bf16(n, (k + p) * N, seed, cuda, with_fp64=True)
+    s64, u64, v64, it64 = isvd.solve(at, k, p, N, omega=omega, integrator="rb_gramian_kn", former="rb_gramian",
+                                     tol=1e-6)
+    fs = isvd.split_bf16(at.t(), 3)
+    for former in ("rb_gramian", "svd"):
+        s, u, v, it = isvd.solve_mixed(at, k, p, N, seed=seed, integrator="rb_gramian_kn", former=former, tol=1e-6,
+                                       parts=3, former_split=fs)
+        rel, ang, orth = _metrics(*(x.cpu().numpy() for x in (s, u, v, s64, u64, v64)))
+        print("%s %s: sigma rel %.2e, angle %.2e, ||U'U-I|| %.2e, it %d/%d" % (case, former, rel, ang, orth, it, it64))
+        assert rel <= 1e-6, rel
+        assert orth <= 1e-10, orth
