@@ -32,10 +32,13 @@ int bf16_gemm_split(Context* c, int64_t M, int64_t N, int64_t K, const uint16_t*
                     const uint16_t* a_lo2, int64_t lda, const uint16_t* b, int64_t ldb, void* D, int64_t ldd,
                     bool out_fp64, bool accumulate, bool lower, const Bf16Split& sp);
 Bf16Split plan_bf16_split(const Context* c, int64_t M, int64_t N, int64_t K, bool chunked, int max_splits);
-// D := sum over z of P + z stride (M x N, pitch ldp), added in order z = 0, 1, ...;
-// D is written N x M when transpose.
+// D := scale x the sum over z of P + z stride (M x N, pitch ldp), added in
+// order z = 0, 1, ...; with groups > 1 each slice contributes its column
+// blocks [g group_cols, g group_cols + N) for g = 0 .. groups-1 (in order).
+// D is written N x M when transpose.  Honours the context's iteration guard.
 int launch_sum_splits(Context* c, const double* P, int splits, int64_t stride, int64_t M, int64_t N, int64_t ldp,
-                      double* D, int64_t ldd, bool transpose);
+                      double* D, int64_t ldd, bool transpose, double scale = 1.0, int groups = 1,
+                      int64_t group_cols = 0);
 
 // hi := bf16(A), lo := bf16(A - hi), lo2 := bf16(A - hi - lo) (lo, lo2 may be
 // null), written row-major (K contiguous) with pitch ldo, from row-major

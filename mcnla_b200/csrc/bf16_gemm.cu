@@ -470,15 +470,21 @@ int bf16_gemm_split(Context* c, int64_t M, int64_t N, int64_t K, const uint16_t*
 
 namespace {
 
-// D := sum_z P_z (z = 0, 1, ... in order: deterministic), P_z = P + z stride,
-// each M x N row-major with pitch ldp; D is N x M (transpose) or M x N.
+// D := scale sum_z sum_g P_z(:, g group_cols + (0:N)) (z, then g, in order:
+// deterministic), P_z = P + z stride, row-major with pitch ldp; D is N x M
+// (transpose) or M x N.  Returns at once when guard_stop says the iteration
+// loop stopped before iteration guard_it.
 __global__ void k_sum_splits(const double* __restrict__ P, int splits, int64_t stride, int M, int N, int64_t ldp,
-                             double* __restrict__ D, int64_t ldd, int transpose) {
+                             int groups, int64_t group_cols, double scale, double* __restrict__ D, int64_t ldd,
+                             int transpose, const int* guard_stop, int guard_it) {
+  if (guard_stop && *guard_stop < guard_it) return;
   const int64_t total = int64_t(M) * N;
   for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x) {
     const int64_t i = e / N, j = e % N;
     double v = 0.0;
-    for (int z = 0; z < splits; ++z) v += P[z * stride + i * ldp + j];
+    for (int z = 0; z < splits; ++z)
+      for (int g = 0; g < groups; ++g) v += P[z * stride + i * ldp + g * group_cols + j];
+    v *= scale;
     if (transpose) D[j * ldd + i] = v; else D[i * ldd + j] = v;
   }
 }
@@ -486,11 +492,12 @@ __global__ void k_sum_splits(const double* __restrict__ P, int splits, int64_t s
 }  // namespace
 
 int launch_sum_splits(Context* c, const double* P, int splits, int64_t stride, int64_t M, int64_t N, int64_t ldp,
-                      double* D, int64_t ldd, bool transpose) {
-  if (M <= 0 || N <= 0 || splits < 1) return MCNLA_B200_ERR_SHAPE;
+                      double* D, int64_t ldd, bool transpose, double scale, int groups, int64_t group_cols) {
+  if (M <= 0 || N <= 0 || splits < 1 || groups < 1) return MCNLA_B200_ERR_SHAPE;
   const int64_t total = M * N;
   const int blocks = int(std::min<int64_t>(cdiv(total, 256), int64_t(c->num_sms) * 8));
-  k_sum_splits<<<blocks, 256, 0, c->stream>>>(P, splits, stride, int(M), int(N), ldp, D, ldd, transpose ? 1 : 0);
+  k_sum_splits<<<blocks, 256, 0, c->stream>>>(P, splits, stride, int(M), int(N), ldp, groups, group_cols, scale, D,
+                                              ldd, transpose ? 1 : 0, c->guard_stop, c->guard_it);
   c->kernels_launched++;
   MB_CHECK_CUDA(cudaGetLastError());
   return MCNLA_B200_OK;

@@ -328,8 +328,22 @@ int run_rb_gramian_kn(Context* c, const Dims& d, const double* Qs, int maxit, do
   pl.add(size_t(L) * l); pl.add(kn_series_work_doubles(l)); pl.add(wsb / 8 + 1);
   const size_t n16 = c->mixed_gramian ? gramian_bs16_count(d) : 0;
   pl.add(n16, sizeof(uint16_t));
+  // precision form of Bs Bc: three BF16 parts of Bs (L x L) and of Bc' (stacked 3l x L), split-K slices
+  const bool bf16_bgc = c->mixed_gramian;
+  const int64_t ldL = (L + 7) & ~int64_t(7);
+  Bf16Split spb;
+  if (bf16_bgc) {
+    spb = plan_bf16_split(c, L, 3 * l, L, true, 16);
+    spb.split_stride = L * 3 * l;
+  }
+  const size_t nbs = bf16_bgc ? 3 * size_t(L) * ldL : 0, nbc = bf16_bgc ? 3 * size_t(l) * ldL : 0;
+  const size_t nsl = bf16_bgc ? size_t(spb.splits) * L * 3 * l : 0;
+  pl.add(nbs, sizeof(uint16_t)); pl.add(nbc, sizeof(uint16_t)); pl.add(nsl);
   MB_CHECK(ctx_reserve(c, pl.bytes));
   uint16_t* bs16 = ctx_take<uint16_t>(c, n16);
+  uint16_t* bsp = ctx_take<uint16_t>(c, nbs);
+  uint16_t* bcp = ctx_take<uint16_t>(c, nbc);
+  double* slices = ctx_take<double>(c, nsl);
   double* Bs = ctx_take<double>(c, size_t(L) * L);
   double* EB[2] = {ctx_take<double>(c, size_t(L) * l3), ctx_take<double>(c, size_t(L) * l3)};
   double* DD = ctx_take<double>(c, size_t(l2) * l);
@@ -345,6 +359,8 @@ int run_rb_gramian_kn(Context* c, const Dims& d, const double* Qs, int maxit, do
   MB_CHECK(gramian_bs(c, d, Qs, Bs, EB[0] + l, l3, ws, bs16));
   MB_CHECK(launch_fill(c, L, l, 0.0, EB[0], l3));
   MB_CHECK(launch_set_identity(c, l, FF[0], l));
+  const size_t bpart = size_t(L) * ldL, cpart = size_t(l) * ldL;
+  if (bf16_bgc) MB_CHECK(launch_split_bf16(c, Bs, MCNLA_B200_ROW_MAJOR, L, L, L, bsp, bsp + bpart, bsp + 2 * bpart, ldL));
   MB_CHECK(ctx_toc(c));
   auto body = [&](int i, bool allow_series) -> int {
     const int cur = i & 1;
@@ -352,7 +368,16 @@ int run_rb_gramian_kn(Context* c, const Dims& d, const double* Qs, int maxit, do
     double* Bc = EB[cur] + l;
     double* Bgc = EB[cur] + l2;
     // Bgc := 1/N Bs Bc   (:152)
-    MB_CHECK(dgemm(c, L, l, L, inv_n, crow(Bs, L), crow(Bc, l3), 0.0, drow(Bgc, l3), GemmBatch(), ws));
+    if (bf16_bgc) {
+      // (Bs_hi + Bs_lo + Bs_lo2) [Bc_hi | Bc_lo | Bc_lo2] on tcgen05 (Bc' split from the column-major view
+      // of Bc), the three column groups and the K slices added in order, times 1/N
+      MB_CHECK(launch_split_bf16(c, Bc, MCNLA_B200_COL_MAJOR, l3, l, L, bcp, bcp + cpart, bcp + 2 * cpart, ldL));
+      MB_CHECK(bf16_gemm_split(c, L, 3 * l, L, bsp, bsp + bpart, bsp + 2 * bpart, ldL, bcp, ldL, slices, 3 * l, true,
+                               false, false, spb));
+      MB_CHECK(launch_sum_splits(c, slices, spb.splits, spb.split_stride, L, l, 3 * l, Bgc, l3, false, inv_n, 3, l));
+    } else {
+      MB_CHECK(dgemm(c, L, l, L, inv_n, crow(Bs, L), crow(Bc, l3), 0.0, drow(Bgc, l3), GemmBatch(), ws));
+    }
     // [Dc | Dgc] := 1/N Bc' [Bc | Bgc]   (:155-158)
     MB_CHECK(dgemm(c, l, l2, L, inv_n, cm(Bc, 1, l3), crow(Bc, l3), 0.0, drow(DD, l2), GemmBatch(), ws));
     // Z, eig, C, inv(C), Fc; F~+ := F~c Fc; convergence test   (:164-214)

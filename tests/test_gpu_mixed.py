@@ -166,3 +166,26 @@ def test_mixed_precision_former_solve(cuda, case):
         print("%s %s: sigma rel %.2e, angle %.2e, ||U'U-I|| %.2e, it %d/%d" % (case, former, rel, ang, orth, it, it64))
         assert rel <= 1e-6, rel
         assert orth <= 1e-10, orth
+
+
+def test_mixed_gramian_loop_bf16(cuda):
+    """N l > 1536: the mixed row-block Gramian KN loop runs Bs Bc on tcgen05 (three BF16 parts of
+    Bs and of Bc each iteration) instead of the persistent FP64 kernel; sigma against plain FP64
+    iSVD on the same A and Omega to 1e-6, U orthonormal to FP64 rounding."""
+    from mcnla_b200 import isvd, synthetic
+    m, n, k, p, N = 6000, 3000, 30, 10, 48
+    a = torch.as_tensor(synthetic.lowrank_np(m, n, np.exp(-np.arange(1, 201) / 30.0), seed=3, noise=1e-4),
+                        device=cuda)
+    seed = 9
+    _, _, omega = isvd.gaussian_bf16(n, (k + p) * N, seed, cuda, with_fp64=True)
+    s64, u64, v64, it64 = isvd.solve(a, k, p, N, omega=omega, integrator="rb_gramian_kn", former="rb_gramian",
+                                     tol=1e-6)
+    s, u, v, it = isvd.solve_mixed(a, k, p, N, seed=seed, integrator="rb_gramian_kn", former="rb_gramian", tol=1e-6,
+                                   parts=3)
+    rel, ang, orth = _metrics(*(x.cpu().numpy() for x in (s, u, v, s64, u64, v64)))
+    print("gramian loop bf16: sigma rel %.2e, angle %.2e, ||U'U-I|| %.2e, it %d/%d" % (rel, ang, orth, it, it64))
+    assert rel <= 1e-6, rel
+    assert orth <= 1e-10, orth
+    s2, u2, v2, it2 = isvd.solve_mixed(a, k, p, N, seed=seed, integrator="rb_gramian_kn", former="rb_gramian",
+                                       tol=1e-6, parts=3)
+    assert it2 == it and torch.equal(s2, s) and torch.equal(u2, u)
