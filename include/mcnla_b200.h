@@ -103,6 +103,8 @@ MCNLA_B200_API const char* mcnla_b200_status_string(int status);
 MCNLA_B200_API const char* mcnla_b200_last_error(void);
 /* Number of kernels this context has launched (for launch accounting). */
 MCNLA_B200_API int64_t mcnla_b200_kernels_launched(const mcnla_b200_ctx* ctx);
+/* Chunks of KN iterations this context ran as a replayed CUDA graph. */
+MCNLA_B200_API int64_t mcnla_b200_graph_replays(const mcnla_b200_ctx* ctx);
 
 /* Kolmogorov-Nagumo step method.  The reference forms C = f(Z) and inv(C)
  * from an eigendecomposition of Z (row_block_kolmogorov_nagumo_integrator.hpp:159-180).
@@ -120,6 +122,13 @@ MCNLA_B200_API int64_t mcnla_b200_kernels_launched(const mcnla_b200_ctx* ctx);
  * contexts, so a shape always runs the same configuration).  Other products,
  * and all products when off, use a fixed shape heuristic.                    */
 MCNLA_B200_API int mcnla_b200_set_autotune(mcnla_b200_ctx* ctx, int on);
+/* CUDA-graph iteration loops (on by default): the Kolmogorov-Nagumo
+ * integrators that launch their products per iteration (kolmogorov_nagumo_
+ * integrator.hpp:109-183 and the row-block forms) run the first chunk of 8
+ * iterations as ordinary launches, capture the next chunk once as a CUDA
+ * graph and replay it for every later full chunk; results are bit-identical
+ * either way.  Off: every iteration is launched.                             */
+MCNLA_B200_API int mcnla_b200_set_graph_loop(mcnla_b200_ctx* ctx, int on);
 
 #define MCNLA_B200_KN_AUTO  0
 #define MCNLA_B200_KN_EIGEN 1

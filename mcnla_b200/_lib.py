@@ -78,8 +78,10 @@ SIGNATURES = {
     "mcnla_b200_status_string": (ctypes.c_char_p, [_INT]),
     "mcnla_b200_last_error": (ctypes.c_char_p, []),
     "mcnla_b200_kernels_launched": (_I64, [_P]),
+    "mcnla_b200_graph_replays": (_I64, [_P]),
     "mcnla_b200_set_kn_method": (_INT, [_P, _INT]),
     "mcnla_b200_set_autotune": (_INT, [_P, _INT]),
+    "mcnla_b200_set_graph_loop": (_INT, [_P, _INT]),
     "mcnla_b200_last_times": (_INT, [_P, ctypes.POINTER(_D), _INT]),
     "mcnla_b200_initialize": (_INT, [_P, ctypes.POINTER(Params), _INT, _INT]),
     "mcnla_b200_sketch": (_INT, [_P, ctypes.POINTER(Params), _P, _INT, _I64, _P, _INT, _P]),

@@ -93,6 +93,8 @@ struct Context {
   // repeat for every iteration, are tuned
   bool autotune = true;
   bool tune_hot = false;
+  // KN iteration loops replay one captured CUDA graph per chunk of iterations
+  bool graph_loop = true;
   // precision form: the Gramian integrators form Bs = Qs' Qs from BF16 parts of Qs
   bool mixed_gramian = false;
   DevScalars* scal = nullptr;       // device scalars
@@ -104,6 +106,7 @@ struct Context {
   bool timing = true;
   // bookkeeping
   int64_t kernels_launched = 0;
+  int64_t graph_replays = 0;   // chunks of KN iterations run as a replayed CUDA graph
 };
 
 // Arena allocation: every call of a stage first computes the bytes it needs,

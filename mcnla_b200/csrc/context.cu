@@ -178,10 +178,17 @@ int mcnla_b200_set_stream(mcnla_b200_ctx* c, void* stream) {
 }
 
 int64_t mcnla_b200_kernels_launched(const mcnla_b200_ctx* c) { return c ? c->kernels_launched : 0; }
+int64_t mcnla_b200_graph_replays(const mcnla_b200_ctx* c) { return c ? c->graph_replays : 0; }
 
 int mcnla_b200_set_autotune(mcnla_b200_ctx* c, int on) {
   if (!c) return MCNLA_B200_ERR_ARG;
   c->autotune = on != 0;
+  return MCNLA_B200_OK;
+}
+
+int mcnla_b200_set_graph_loop(mcnla_b200_ctx* c, int on) {
+  if (!c) return MCNLA_B200_ERR_ARG;
+  c->graph_loop = on != 0;
   return MCNLA_B200_OK;
 }
 

@@ -152,25 +152,90 @@ struct HotLoop {
   ~HotLoop() { c->tune_hot = false; }
 };
 
+//
+// CUDA graph: the bodies of one chunk depend on the iteration only through
+// its parity (double buffers) and the guard index, so after the first chunk
+// (launched directly: it also tunes every product shape) the next full chunk
+// is captured once with guard indices relative to the chunk start, and every
+// later full chunk replays that graph.  Relative indices work because the KN
+// step records the converged iteration as the guard index it was given: the
+// host adds the chunk start.  A capture that fails (an operation the graph
+// cannot hold) is abandoned and the loop continues with direct launches.
+struct LoopGraph {
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t cap = nullptr;
+  ~LoopGraph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (cap) cudaStreamDestroy(cap);
+  }
+};
+
+template <class Body>
+int capture_chunk(Context* c, int it0, int chunk, Body& body, LoopGraph& g, uint64_t* kernels) {
+  if (cudaStreamCreateWithFlags(&g.cap, cudaStreamNonBlocking) != cudaSuccess) return MCNLA_B200_ERR_CUDA;
+  struct Swap { Context* c; cudaStream_t s; ~Swap() { c->stream = s; } } swap{c, c->stream};
+  const uint64_t k0 = c->kernels_launched;
+  if (cudaStreamBeginCapture(g.cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return MCNLA_B200_ERR_CUDA;
+  c->stream = g.cap;
+  int st = MCNLA_B200_OK;
+  for (int r = 0; r < chunk && st == MCNLA_B200_OK; ++r) {
+    c->guard_it = r;
+    st = body(it0 + r);
+  }
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ec = cudaStreamEndCapture(g.cap, &graph);
+  c->stream = swap.s;
+  *kernels = c->kernels_launched - k0;
+  c->kernels_launched = k0;            // nothing ran yet: replays count themselves
+  if (st == MCNLA_B200_OK && (ec != cudaSuccess || !graph)) st = MCNLA_B200_ERR_CUDA;
+  if (st == MCNLA_B200_OK && cudaGraphInstantiate(&g.exec, graph, 0) != cudaSuccess) {
+    g.exec = nullptr;
+    st = MCNLA_B200_ERR_CUDA;
+  }
+  if (graph) cudaGraphDestroy(graph);
+  if (st != MCNLA_B200_OK) cudaGetLastError();   // capture errors are not sticky: clear and go on eagerly
+  return st;
+}
+
 template <class Body>
 int kn_loop(Context* c, int maxit, Body body, int* iters) {
   MB_CHECK_CUDA(cudaMemsetAsync(&c->scal->stop_it, 0x7f, sizeof(int), c->stream));   // "not yet"
   struct Reset { Context* c; ~Reset() { c->guard_stop = nullptr; c->guard_it = 0; } } reset{c};
   HotLoop hot(c);
   c->guard_stop = &c->scal->stop_it;
-  const int chunk = 8;
+  const int chunk = 8;   // even: every chunk starts on the same buffer parity
   int launched = 0, done = -1;
+  LoopGraph graph;
+  bool use_graph = c->graph_loop;
+  uint64_t graph_kernels = 0;
   while (launched < maxit) {
     const int end = std::min(maxit, launched + chunk);
-    for (int it = launched; it < end; ++it) {
-      c->guard_it = it;
-      MB_CHECK(body(it));
+    // graph replays for full chunks after the first, when at least two remain
+    if (use_graph && launched > 0 && end - launched == chunk && !graph.exec && maxit - launched >= 2 * chunk) {
+      if (capture_chunk(c, launched, chunk, body, graph, &graph_kernels) != MCNLA_B200_OK) use_graph = false;
     }
+    if (use_graph && graph.exec && end - launched == chunk) {
+      MB_CHECK_CUDA(cudaGraphLaunch(graph.exec, c->stream));
+      c->kernels_launched += graph_kernels;
+      c->graph_replays++;
+    } else {
+      for (int it = launched; it < end; ++it) {
+        c->guard_it = it;
+        MB_CHECK(body(it));
+      }
+    }
+    const bool relative = use_graph && graph.exec && end - launched == chunk;
+    const int start = launched;
     launched = end;
     MB_CHECK(ctx_sync_scalars(c));
     if (c->scal_host->status) return c->scal_host->status;
     const int stop = c->scal_host->stop_it;
-    if (stop < launched) { done = stop + 1; break; }
+    if (relative) {
+      if (stop < chunk) { done = start + stop + 1; break; }
+    } else if (stop < launched) {
+      done = stop + 1;
+      break;
+    }
   }
   *iters = done < 0 ? launched : done;
   return MCNLA_B200_OK;

@@ -74,9 +74,16 @@ class Context:
     def kernels_launched(self):
         return int(self.lib.mcnla_b200_kernels_launched(self.handle))
 
+    def graph_replays(self):
+        return int(self.lib.mcnla_b200_graph_replays(self.handle))
+
     def set_autotune(self, on):
         """GEMM tile autotuner on (default) or off (fixed shape heuristic)."""
         _lib.check(self.lib.mcnla_b200_set_autotune(self.handle, 1 if on else 0), "set_autotune")
+
+    def set_graph_loop(self, on):
+        """KN iteration loops as replayed CUDA graphs (default on) or direct launches."""
+        _lib.check(self.lib.mcnla_b200_set_graph_loop(self.handle, 1 if on else 0), "set_graph_loop")
 
     def set_kn_method(self, method):
         """_lib.KN_AUTO (matrix functions, eigen fallback) or _lib.KN_EIGEN."""

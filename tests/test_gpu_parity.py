@@ -485,3 +485,29 @@ def test_dgemm_autotuned_matches_heuristic(cuda, M, N, K):
     for c in outs:
         assert (c - ref).abs().max().item() <= 1e-14 * scale * K ** 0.5
     assert torch.equal(outs[1], outs[2])
+
+
+@pytest.mark.parametrize("integrator,shape", [("kn", (1000, 2000, 10, 10, 16)), ("rb_kn", (1000, 2000, 10, 10, 16)),
+                                              ("rb_gramian_kn", (3000, 2000, 20, 12, 50))])
+def test_graph_loop_matches_direct(cuda, integrator, shape):
+    """The KN loop replayed as a captured CUDA graph gives the same bits and the same iteration
+    count as direct launches (the last shape has N l = 1600, past the persistent kernel)."""
+    from mcnla_b200 import isvd, synthetic
+    m, n, k, p, N = shape
+    a = torch.as_tensor(synthetic.lowrank_np(m, n, 1.0 / np.arange(1, min(m, n) + 1), seed=4), device=cuda)
+    ctx = isvd.context()
+    out = []
+    try:
+        for on in (False, True, True):
+            ctx.set_graph_loop(on)
+            r0 = ctx.graph_replays()
+            out.append(isvd.solve(a, k, p, N, seed=2, integrator=integrator, former="svd", tol=1e-5))
+            replays = ctx.graph_replays() - r0
+            assert (replays > 0) == on, replays
+    finally:
+        ctx.set_graph_loop(True)
+    (s0, u0, v0, it0) = out[0]
+    assert it0 > 24, it0          # several graph chunks ran
+    for s1, u1, v1, it1 in out[1:]:
+        assert it1 == it0
+        assert torch.equal(s1, s0) and torch.equal(u1, u0) and torch.equal(v1, v0)
