@@ -1,7 +1,8 @@
 // FP64 DMMA GEMM (see dgemm.cuh).
 //
 // Tiling: a CTA computes a BM x BN tile of C; its warps own WM x WN sub-tiles
-// made of 8x8 DMMA fragments.  K advances in steps of BK = 16 through a
+// made of 8x8 DMMA fragments.  K advances in steps of BK = 16 (32 for the
+// large 128x128 configuration: half the barriers per flop) through a
 // STAGES-deep cp.async ring.  Shared-memory rows are padded (K-contiguous
 // rows by 4 doubles, M/N-contiguous rows by 8) so every fragment load of a
 // warp touches each bank pair at most twice: the minimum two wavefronts for
@@ -52,17 +53,18 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
                : "d"(a), "d"(b));
 }
 
-template <int BM_, int BN_, int WM_, int WN_, bool AK_, bool BKM_, int VEC_, int STAGES_>
+template <int BM_, int BN_, int WM_, int WN_, bool AK_, bool BKM_, int VEC_, int STAGES_, int BK_ = BK>
 struct Cfg {
   static constexpr int BM = BM_, BN = BN_, WM = WM_, WN = WN_, VEC = VEC_, STAGES = STAGES_;
+  static constexpr int BKT = BK_;   // k-tile depth
   static constexpr bool AK = AK_, BKM = BKM_;
   static constexpr int WARPS_M = BM / WM, WARPS_N = BN / WN;
   static constexpr int THREADS = WARPS_M * WARPS_N * 32;
   static constexpr int MT = WM / 8, NT = WN / 8;
-  static constexpr int LDA = AK ? (BK + PAD_K) : (BM + PAD_MN);
-  static constexpr int LDB = BKM ? (BK + PAD_K) : (BN + PAD_MN);
-  static constexpr int A_ELEMS = AK ? BM * LDA : BK * LDA;
-  static constexpr int B_ELEMS = BKM ? BN * LDB : BK * LDB;
+  static constexpr int LDA = AK ? (BKT + PAD_K) : (BM + PAD_MN);
+  static constexpr int LDB = BKM ? (BKT + PAD_K) : (BN + PAD_MN);
+  static constexpr int A_ELEMS = AK ? BM * LDA : BKT * LDA;
+  static constexpr int B_ELEMS = BKM ? BN * LDB : BKT * LDB;
   static constexpr int STAGE_ELEMS = A_ELEMS + B_ELEMS;
   static constexpr size_t SMEM = size_t(STAGES) * STAGE_ELEMS * sizeof(double);
 };
@@ -72,10 +74,10 @@ struct Cfg {
 // computed once; each k-tile only adds k0 * (k stride) and re-checks the K end.
 //   KROWS: the tile's rows run along M (or N) and K is contiguous;
 //   otherwise the rows run along K and M (or N) is contiguous.
-template <int ROWS_MN, bool KCONTIG, int V, int THREADS, int LD>
+template <int ROWS_MN, bool KCONTIG, int V, int THREADS, int LD, int TK>
 struct TileLoader {
-  static constexpr int CPR = KCONTIG ? BK / V : ROWS_MN / V;        // chunks per smem row
-  static constexpr int TOTAL = KCONTIG ? ROWS_MN * CPR : BK * CPR;
+  static constexpr int CPR = KCONTIG ? TK / V : ROWS_MN / V;        // chunks per smem row
+  static constexpr int TOTAL = KCONTIG ? ROWS_MN * CPR : TK * CPR;
   static constexpr int PER = (TOTAL + THREADS - 1) / THREADS;
   const double* src[PER];
   int mn_valid[PER];   // KCONTIG: row in range; else valid elements along M/N (0..V)
@@ -147,7 +149,8 @@ __global__ void __launch_bounds__(C::THREADS) dgemm_kernel(KArgs g) {
   const double* B = g.B + bz * g.b_bs;
   const int64_t kbeg = split * g.kps;
   const int64_t kend = min(g.K, kbeg + g.kps);
-  const int KT = kend > kbeg ? int((kend - kbeg + BK - 1) / BK) : 0;
+  constexpr int TK = C::BKT;
+  const int KT = kend > kbeg ? int((kend - kbeg + TK - 1) / TK) : 0;
 
   double acc[C::MT][C::NT][2];
 #pragma unroll
@@ -157,8 +160,8 @@ __global__ void __launch_bounds__(C::THREADS) dgemm_kernel(KArgs g) {
 
   // A tile: BM rows along M (K contiguous) or BK rows along K (M contiguous);
   // B tile: BN rows along N (K contiguous) or BK rows along K (N contiguous).
-  TileLoader<C::BM, C::AK, C::VEC, C::THREADS, C::LDA> la;
-  TileLoader<C::BN, C::BKM, C::VEC, C::THREADS, C::LDB> lb;
+  TileLoader<C::BM, C::AK, C::VEC, C::THREADS, C::LDA, TK> la;
+  TileLoader<C::BN, C::BKM, C::VEC, C::THREADS, C::LDB, TK> lb;
   la.init(A, m0, g.M, C::AK ? g.a_rs : 1, C::AK ? 1 : g.a_cs, tid);
   lb.init(B, n0, g.N, C::BKM ? g.b_cs : 1, C::BKM ? 1 : g.b_rs, tid);
 
@@ -166,8 +169,8 @@ __global__ void __launch_bounds__(C::THREADS) dgemm_kernel(KArgs g) {
   for (int s = 0; s < C::STAGES - 1; ++s) {
     if (s < KT) {
       double* st = smem + s * C::STAGE_ELEMS;
-      la.load(st, kbeg + int64_t(s) * BK, kend);
-      lb.load(st + C::A_ELEMS, kbeg + int64_t(s) * BK, kend);
+      la.load(st, kbeg + int64_t(s) * TK, kend);
+      lb.load(st + C::A_ELEMS, kbeg + int64_t(s) * TK, kend);
     }
     cp_commit();
   }
@@ -179,15 +182,15 @@ __global__ void __launch_bounds__(C::THREADS) dgemm_kernel(KArgs g) {
       const int nt = kt + C::STAGES - 1;
       if (nt < KT) {
         double* st = smem + (nt % C::STAGES) * C::STAGE_ELEMS;
-        la.load(st, kbeg + int64_t(nt) * BK, kend);
-        lb.load(st + C::A_ELEMS, kbeg + int64_t(nt) * BK, kend);
+        la.load(st, kbeg + int64_t(nt) * TK, kend);
+        lb.load(st + C::A_ELEMS, kbeg + int64_t(nt) * TK, kend);
       }
       cp_commit();
     }
     const double* sA = smem + (kt % C::STAGES) * C::STAGE_ELEMS;
     const double* sB = sA + C::A_ELEMS;
 #pragma unroll
-    for (int kk = 0; kk < BK / 4; ++kk) {
+    for (int kk = 0; kk < TK / 4; ++kk) {
       const int k = kk * 4 + t4;
       double af[C::MT], bf[C::NT];
 #pragma unroll
@@ -273,13 +276,14 @@ int launch(Context* ctx, const KArgs& g, int batch) {
 }
 
 // Tile shape families, picked by the output shape.
-enum Shape { S128x128 = 0, S128x64 = 1, S64x64 = 2, S128x32 = 3, S64x32 = 4, S128x128w16 = 5 };
+enum Shape { S128x128 = 0, S128x64 = 1, S64x64 = 2, S128x32 = 3, S64x32 = 4, S128x128w16 = 5, S128x128k32 = 6 };
 
 template <bool AK, bool BKM, int VEC>
 int dispatch_shape(Context* ctx, const KArgs& g, int batch, Shape s) {
   switch (s) {
     case S128x128: return launch<Cfg<128, 128, 64, 32, AK, BKM, VEC, 4>>(ctx, g, batch);
     case S128x128w16: return launch<Cfg<128, 128, 32, 32, AK, BKM, VEC, 4>>(ctx, g, batch);
+    case S128x128k32: return launch<Cfg<128, 128, 32, 32, AK, BKM, VEC, 3, 32>>(ctx, g, batch);
     case S128x64: return launch<Cfg<128, 64, 32, 32, AK, BKM, VEC, 4>>(ctx, g, batch);
     case S64x64: return launch<Cfg<64, 64, 32, 32, AK, BKM, VEC, 4>>(ctx, g, batch);
     case S128x32: return launch<Cfg<128, 32, 32, 16, AK, BKM, VEC, 4>>(ctx, g, batch);
@@ -315,6 +319,8 @@ Plan make_plan(const Context* ctx, int64_t M, int64_t N, int64_t K, int batch, i
   splits = int(std::max<int64_t>(1, cdiv(K, kps)));
   p.splits = splits;
   p.kps = kps;
+  // long K per CTA: 32-deep k-tiles (half the barriers per flop)
+  if (p.shape == S128x128w16 && kps >= 512) p.shape = S128x128k32;
   return p;
 }
 
@@ -413,7 +419,7 @@ int tune(Context* ctx, const KArgs& g0, int batch, const Plan& heuristic, int ma
   int st = MCNLA_B200_OK;
   if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) st = MCNLA_B200_ERR_CUDA;
   float best_ms = 1e30f;
-  const Shape shapes[] = {S128x128w16, S128x128, S128x64, S64x64, S128x32, S64x32};
+  const Shape shapes[] = {S128x128k32, S128x128w16, S128x128, S128x64, S64x64, S128x32, S64x32};
   const int split_opts[] = {1, 2, 4, 8, 16, 32};
   for (Shape sh : shapes) {
     for (int so : split_opts) {
