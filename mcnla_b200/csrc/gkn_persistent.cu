@@ -29,6 +29,7 @@ namespace {
 
 constexpr int kGknThreads = 256;
 constexpr int kGknWarps = kGknThreads / 32;
+static_assert(kGknThreads == 256, "grid_tiles reduces a 16 x 16 tile with one thread per element");
 constexpr int64_t kGknMaxL = 1536;
 
 struct GknArgs {
@@ -48,32 +49,66 @@ struct GknArgs {
   int smax;                 // power slabs of the series step
 };
 
-// out(i, j) := sum_k A(i, k) B(k, j) for an M x N product over 8 x 8 tiles
+// out(i, j) := sum_k A(i, k) B(k, j) for an M x N product over 16 x 16 tiles
 // distributed round-robin over the grid's CTAs.  In a CTA, warp w sums k in
-// its eighth of K and the partial tiles are added in warp order through
-// shared memory (red: kGknWarps x 64 doubles), so the result does not depend
-// on the grid size.  fa(i, k), fb(k, j) load operands; fo(i, j, v) stores.
+// its eighth of K for all four 8 x 8 quarters of the tile (2 x 2 register
+// blocking: four DMMAs per pair of A and B fragment loads) and the partial
+// tiles are added in warp order through shared memory (red: kGknWarps x 256
+// doubles), so the result does not depend on the grid size; every element
+// sees the same sequence of DMMA steps as with one 8 x 8 tile per pass.
+// fa(i, k), fb(k, j) load operands; fo(i, j, v) stores.
 template <class FA, class FB, class FO>
 __device__ void grid_tiles(FA fa, FB fb, FO fo, int M, int N, int K, double* red) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane >> 2, t4 = lane & 3;
-  const int mt = (M + 7) >> 3, ntl = (N + 7) >> 3;
+  const int mt = (M + 15) >> 4, ntl = (N + 15) >> 4;
   const int chunk = ((K + kGknWarps - 1) / kGknWarps + 3) & ~3;
   const int kb = min(K, warp * chunk), ke = min(K, kb + chunk);
   for (int t = blockIdx.x; t < mt * ntl; t += gridDim.x) {
-    const int ti = (t / ntl) * 8, tj = (t % ntl) * 8;
-    const int i = ti + g, j = tj + g;
-    const bool iv = i < M, jv = j < N;
-    double c0 = 0.0, c1 = 0.0;
-    tile_acc([&](int k) { return iv ? fa(i, k) : 0.0; }, [&](int k) { return jv ? fb(k, j) : 0.0; }, kb, ke, c0,
-             c1);
-    red[warp * 64 + g * 8 + 2 * t4] = c0;
-    red[warp * 64 + g * 8 + 2 * t4 + 1] = c1;
+    const int ti = (t / ntl) * 16, tj = (t % ntl) * 16;
+    const int i0 = ti + g, i1 = i0 + 8, j0 = tj + g, j1 = j0 + 8;
+    const bool iv0 = i0 < M, iv1 = i1 < M, jv0 = j0 < N, jv1 = j1 < N;
+    double c[2][2][2], e[2][2][2];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      (&c[0][0][0])[q] = 0.0;
+      (&e[0][0][0])[q] = 0.0;
+    }
+    for (int k = kb; k < ke; k += 4 * kU) {
+      double a0[kU], a1[kU], b0[kU], b1[kU];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        const int kk = k + 4 * u + t4;
+        const bool kv = kk < ke;
+        a0[u] = kv && iv0 ? fa(i0, kk) : 0.0;
+        a1[u] = kv && iv1 ? fa(i1, kk) : 0.0;
+        b0[u] = kv && jv0 ? fb(kk, j0) : 0.0;
+        b1[u] = kv && jv1 ? fb(kk, j1) : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < kU; u += 2) {
+        dmma(c[0][0][0], c[0][0][1], a0[u], b0[u]);
+        dmma(c[0][1][0], c[0][1][1], a0[u], b1[u]);
+        dmma(c[1][0][0], c[1][0][1], a1[u], b0[u]);
+        dmma(c[1][1][0], c[1][1][1], a1[u], b1[u]);
+        dmma(e[0][0][0], e[0][0][1], a0[u + 1], b0[u + 1]);
+        dmma(e[0][1][0], e[0][1][1], a0[u + 1], b1[u + 1]);
+        dmma(e[1][0][0], e[1][0][1], a1[u + 1], b0[u + 1]);
+        dmma(e[1][1][0], e[1][1][1], a1[u + 1], b1[u + 1]);
+      }
+    }
+#pragma unroll
+    for (int ib = 0; ib < 2; ++ib)
+#pragma unroll
+      for (int jb = 0; jb < 2; ++jb)
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+          red[warp * 256 + (8 * ib + g) * 16 + 8 * jb + 2 * t4 + h] = c[ib][jb][h] + e[ib][jb][h];
     __syncthreads();
-    if (threadIdx.x < 64) {
-      const int r = threadIdx.x >> 3, cc = threadIdx.x & 7;
+    {
+      const int r = threadIdx.x >> 4, cc = threadIdx.x & 15;   // kGknThreads = 256 outputs
       double v = 0.0;
-      for (int w = 0; w < kGknWarps; ++w) v += red[w * 64 + threadIdx.x];
+      for (int w = 0; w < kGknWarps; ++w) v += red[w * 256 + threadIdx.x];
       if (ti + r < M && tj + cc < N) fo(ti + r, tj + cc, v);
     }
     __syncthreads();
@@ -84,7 +119,9 @@ __global__ void __launch_bounds__(kGknThreads, 1) k_gkn_persistent(GknArgs a) {
   extern __shared__ __align__(16) double sm[];
   __shared__ int s_flag;
   const int l = a.l, L = a.L, l3 = 3 * l;
-  double* red = sm + kn_series_smem_doubles(l, a.smax);   // kGknWarps x 64 doubles
+  // the products' reduction space (kGknWarps x 256 doubles) aliases the series step's
+  // shared memory: the step zeroes and reloads it on every call and ends on a grid barrier
+  double* red = sm;
   for (int it = a.it0; it < a.maxit; ++it) {
     const int cur = it & 1;
     double* E = cur ? a.eb1 : a.eb0;                   // [E~c | Bc | Bgc]
@@ -171,7 +208,8 @@ int launch_gkn_persistent(Context* c, int l, int64_t L, int N, double tol, int i
                           double* work) {
   if (!gkn_persistent_fits(c, l, L)) return MCNLA_B200_ERR_UNSUPPORTED;
   const int smax = kn_series_smax(l, c->smem_optin, kGknWarps * 64);
-  const size_t smem = (kn_series_smem_doubles(l, smax) + kGknWarps * 64) * sizeof(double);
+  const size_t smem =
+      std::max<size_t>(kn_series_smem_doubles(l, smax) + kGknWarps * 64, kGknWarps * 256) * sizeof(double);
   MB_CHECK(set_smem(c, reinterpret_cast<const void*>(k_gkn_persistent), smem));
   GknArgs a;
   a.l = l;
