@@ -62,10 +62,12 @@ def parse():
     ap.add_argument("--cpu-rows", type=int, default=0, help="row sample of the CPU baseline (0: auto)")
     ap.add_argument("--quick", action="store_true", help="small shape for a smoke run")
     ap.add_argument("--no-serving", action="store_true", help="skip the batched / served leg")
-    ap.add_argument("--kernel", choices=["sketch_bf16", "gkn"], default=None,
+    ap.add_argument("--kernel", choices=["sketch_bf16", "gkn", "trace"], default=None,
                     help="time one kernel alone (profiling case) instead of the benchmark: the BF16 sketch GEMM "
                          "on --m x --n x (--k + --p) --N with --parts parts, or the persistent row-block Gramian "
-                         "KN integrator on the sketches of a seeded --m x --n matrix (sigma_j = 1/j, tol 1e-5)")
+                         "KN integrator on the sketches of a seeded --m x --n matrix (sigma_j = 1/j, tol 1e-5); "
+                         "trace: per-kernel device time (CUPTI activity records, no replay) of one FP64 and one "
+                         "mixed solve of the workload, and the per-iteration share from maxit 65 vs 257")
     ap.add_argument("--only-serving", action="store_true", help="run the batched / served leg alone")
     ap.add_argument("--batch-count", type=int, default=1024, help="matrices in the uneven batch")
     ap.add_argument("--serve-workers", type=int, default=8, help="concurrent solves of the server")
@@ -655,6 +657,56 @@ def run_serving(args, dev):
 # ------------------------------------------------------------------------------------------------
 # single-kernel cases (profiling)
 # ------------------------------------------------------------------------------------------------
+def run_trace(args, dev):
+    """Device time per kernel (CUPTI activity records through torch.profiler: every launch's own
+    start and end on the GPU, no replay, the autotuner sees ordinary launches) for one FP64 and one
+    mixed solve of the workload after two warm-up solves each, and each kernel's time per
+    integrator iteration from the difference of solves capped at 257 and 65 iterations."""
+    import collections
+    import numpy as np
+    import torch
+    from torch.profiler import profile, ProfilerActivity
+    from mcnla_b200 import isvd, synthetic
+    m, n, k, p, N = args.m, args.n, args.k, args.p, args.N
+    a = synthetic.lowrank_torch(m, n, np.exp(-np.arange(1, args.rank_r + 1) / 30.0), seed=1, noise=1e-4, device=dev)
+    sp = isvd.split_bf16(a, args.parts)
+    fs = isvd.split_bf16(a.t(), args.former_parts) if args.former_parts else None
+
+    def solve(mixed, maxit):
+        kw = dict(seed=3, integrator=args.integrator, former=args.former, tol=args.tol, maxit=maxit)
+        if mixed:
+            return isvd.solve_mixed(a, k, p, N, split=sp, former_split=fs, **kw)
+        return isvd.solve(a, k, p, N, **kw)
+
+    def kernels(mixed, maxit):
+        solve(mixed, maxit)
+        solve(mixed, maxit)
+        torch.cuda.synchronize()
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            solve(mixed, maxit)
+            torch.cuda.synchronize()
+        agg = collections.defaultdict(lambda: [0, 0.0])
+        for e in prof.events():
+            if e.device_type.name == "CUDA" and e.time_range.end > e.time_range.start:
+                key = e.name.replace("(anonymous namespace)::", "").split("(")[0]
+                agg[key][0] += 1
+                agg[key][1] += (e.time_range.end - e.time_range.start) / 1e3   # ms
+        return agg
+
+    out = {"workload": workload(args)["workload"], "timing": "CUPTI activity records (device start/end per "
+           "launch), one solve after two warm-up solves"}
+    for name, mixed in (("fp64", False), ("mixed", True)):
+        full, short = kernels(mixed, args.maxit), kernels(mixed, 65)
+        rows = []
+        for key in sorted(full, key=lambda x: -full[x][1]):
+            c1, t1 = full[key]
+            c0, t0 = short.get(key, [0, 0.0])
+            rows.append({"kernel": key[-110:], "launches": c1, "ms": round(t1, 3),
+                         "us_per_iteration": round((t1 - t0) * 1e3 / max(1, args.maxit - 65), 2)})
+        out[name] = {"kernel_ms_total": round(sum(r["ms"] for r in rows), 3), "kernels": rows[:20]}
+    return out
+
+
 def run_kernel_case(args, dev):
     import numpy as np
     import torch
@@ -662,6 +714,8 @@ def run_kernel_case(args, dev):
     m, n, k, p, N = args.m, args.n, args.k, args.p, args.N
     L = (k + p) * N
     ctx = isvd.context(dev)
+    if args.kernel == "trace":
+        return run_trace(args, dev)
     if args.kernel == "sketch_bf16":
         a = torch.randn(m, n, dtype=torch.float64, device=dev)
         sp = isvd.split_bf16(a, args.parts)

@@ -922,6 +922,10 @@ int run_isvd(Context* c, const Dims& d, int integrator, int former, const double
   return MCNLA_B200_OK;
 }
 
+// FP64 flops of the lower-triangle Bs = Qs' Qs (L^2 m) from which the mixed
+// solve forms it from BF16 parts instead.
+constexpr double kMixedGramianMinFlops = 1e11;
+
 // Mixed solve: Omega drawn in BF16, sketch on tcgen05, FP64 afterwards.
 int run_isvd_mixed(Context* c, const Dims& d, int integrator, int former, const double* A, int layout, int64_t lda,
                    const uint16_t* a_hi, const uint16_t* a_lo, const uint16_t* a_lo2, int64_t lda16,
@@ -943,14 +947,19 @@ int run_isvd_mixed(Context* c, const Dims& d, int integrator, int former, const 
   MB_CHECK(bf16_gemm(c, d.m, d.L, d.n, a_hi, a_lo, a_lo2, lda16, omega_t, ldo, Q, d.L, true));
   MB_CHECK(ctx_toc(c));
   MB_CHECK(run_orthogonalize(c, d, Q));
+  // The Gramian integrators' Bs (and the loop's Bs Bc) from BF16 parts (the
+  // precision form) only where the FP64 product is long: below ~1e11 flops it
+  // takes a few milliseconds at most, less than the split and the FP64
+  // re-orthonormalization the BF16 form needs afterwards.
+  const bool gramian = integrator == MCNLA_B200_ROW_BLOCK_GRAMIAN_KOLMOGOROV_NAGUMO ||
+                       integrator == MCNLA_B200_ROW_BLOCK_GRAMIAN_WEN_YIN;
+  const bool bf16_gramian = gramian && double(d.L) * double(d.L) * double(d.m) >= kMixedGramianMinFlops;
   {
-    // the Gramian integrators' Bs from BF16 parts of Qs (the precision form)
-    struct Mixed { Context* c; explicit Mixed(Context* x) : c(x) { c->mixed_gramian = true; }
-                   ~Mixed() { c->mixed_gramian = false; } } mixed(c);
+    struct Mixed { Context* c; Mixed(Context* x, bool on) : c(x) { c->mixed_gramian = on; }
+                   ~Mixed() { c->mixed_gramian = false; } } mixed(c, bf16_gramian);
     MB_CHECK(run_integrate(c, d, integrator, Q, maxit, tol, Qbar, iters));
   }
-  if (integrator == MCNLA_B200_ROW_BLOCK_GRAMIAN_KOLMOGOROV_NAGUMO ||
-      integrator == MCNLA_B200_ROW_BLOCK_GRAMIAN_WEN_YIN) {
+  if (bf16_gramian) {
     // Bs carried the BF16 rounding of Qs into the iterates: one FP64 Gramian
     // pass (Qbar := Qbar V S^(-1/2), an orthonormal basis of the same span)
     // brings ||Qbar' Qbar - I|| back to FP64 rounding

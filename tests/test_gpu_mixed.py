@@ -169,11 +169,12 @@ def test_mixed_precision_former_solve(cuda, case):
 
 
 def test_mixed_gramian_loop_bf16(cuda):
-    """N l > 1536: the mixed row-block Gramian KN loop runs Bs Bc on tcgen05 (three BF16 parts of
-    Bs and of Bc each iteration) instead of the persistent FP64 kernel; sigma against plain FP64
-    iSVD on the same A and Omega to 1e-6, U orthonormal to FP64 rounding."""
+    """N l > 1536 and (N l)^2 m >= 1e11: the mixed solve forms Bs from BF16 parts of Qs and its
+    row-block Gramian KN loop runs Bs Bc on tcgen05 (three BF16 parts of Bs and of Bc each
+    iteration), then re-orthonormalizes Qbar in FP64; sigma against plain FP64 iSVD on the same A
+    and Omega to 1e-6, U orthonormal to FP64 rounding."""
     from mcnla_b200 import isvd, synthetic
-    m, n, k, p, N = 6000, 3000, 30, 10, 48
+    m, n, k, p, N = 30000, 3000, 30, 10, 48
     a = torch.as_tensor(synthetic.lowrank_np(m, n, np.exp(-np.arange(1, 201) / 30.0), seed=3, noise=1e-4),
                         device=cuda)
     seed = 9
