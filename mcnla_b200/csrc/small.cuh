@@ -90,7 +90,10 @@ __device__ inline int cta_jacobi_eig(double* a, int lda, double* v, int ldv, int
   const double eps = 2.220446049250313e-16;
   const double eps2 = eps * eps;
   const double abs_floor = eps2 * fro2;
-  const int items = npairs * n;
+  // items (pair k, element j) of a round, k-major: thread tid takes e = tid, tid + nt, ...,
+  // walked as (k, j) with a fixed increment instead of dividing e by n for every item
+  const int k_start = tid / n, j_start = tid - k_start * n;
+  const int k_step = nt / n, j_step = nt - k_step * n;
   int sweep = 0;
   for (; sweep < max_sweeps; ++sweep) {
     int rotated = 0;
@@ -125,21 +128,23 @@ __device__ inline int cta_jacobi_eig(double* a, int lda, double* v, int ldv, int
       if (cnt == 0) continue;
       rotated += cnt;
       // 2. rows: a <- J' a   (item (k, j): element j of rows p, q of pair k)
-      for (int e = tid; e < items; e += nt) {
-        const int k = e / n, j = e - k * n;
+      for (int k = k_start, j = j_start; k < npairs;) {
         const double s = js.s[k];
-        if (s == 0.0) continue;
-        const double c = js.c[k];
-        const int p = js.p[k], q = js.q[k];
-        const double x = a[p * lda + j], y = a[q * lda + j];
-        a[p * lda + j] = c * x - s * y;
-        a[q * lda + j] = s * x + c * y;
+        if (s != 0.0) {
+          const double c = js.c[k];
+          const int p = js.p[k], q = js.q[k];
+          const double x = a[p * lda + j], y = a[q * lda + j];
+          a[p * lda + j] = c * x - s * y;
+          a[q * lda + j] = s * x + c * y;
+        }
+        k += k_step;
+        j += j_step;
+        if (j >= n) { j -= n; ++k; }
       }
       __syncthreads();
       // 3. columns: a <- a J (the 2x2 block of each pair written exactly:
       //    J' B J = diag(app - t apq, aqq + t apq)), and rows p, q of v
-      for (int e = tid; e < items; e += nt) {
-        const int k = e / n, i = e - k * n;
+      for (int k = k_start, i = j_start; k < npairs; k += k_step, i += j_step, (i >= n ? (i -= n, ++k) : 0)) {
         const double s = js.s[k];
         if (s == 0.0) continue;
         const double c = js.c[k];
