@@ -171,10 +171,10 @@ struct LoopGraph {
 };
 
 template <class Body>
-int capture_chunk(Context* c, int it0, int chunk, Body& body, LoopGraph& g, uint64_t* kernels) {
+int capture_chunk(Context* c, int it0, int chunk, Body& body, LoopGraph& g, int64_t* kernels) {
   if (cudaStreamCreateWithFlags(&g.cap, cudaStreamNonBlocking) != cudaSuccess) return MCNLA_B200_ERR_CUDA;
   struct Swap { Context* c; cudaStream_t s; ~Swap() { c->stream = s; } } swap{c, c->stream};
-  const uint64_t k0 = c->kernels_launched;
+  const int64_t k0 = c->kernels_launched;
   if (cudaStreamBeginCapture(g.cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return MCNLA_B200_ERR_CUDA;
   c->stream = g.cap;
   int st = MCNLA_B200_OK;
@@ -207,7 +207,7 @@ int kn_loop(Context* c, int maxit, Body body, int* iters) {
   int launched = 0, done = -1;
   LoopGraph graph;
   bool use_graph = c->graph_loop;
-  uint64_t graph_kernels = 0;
+  int64_t graph_kernels = 0;
   while (launched < maxit) {
     const int end = std::min(maxit, launched + chunk);
     // graph replays for full chunks after the first, when at least two remain
