@@ -63,6 +63,7 @@ struct DevScalars {
 struct Context {
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t copy_stream = nullptr;   // host-to-device copies overlapped with compute (created on first use)
   bool own_stream = false;
   int num_sms = 148;
   size_t smem_optin = 0;

@@ -153,12 +153,14 @@ int mcnla_b200_destroy(mcnla_b200_ctx* c) {
   if (!c) return MCNLA_B200_OK;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
+  if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);   // copies land in the arenas freed below
   for (auto ev : c->events) cudaEventDestroy(ev);
   if (c->arena) cudaFree(c->arena);
   if (c->parena) cudaFree(c->parena);
   if (c->scal) cudaFree(c->scal);
   if (c->scal_host) cudaFreeHost(c->scal_host);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
   delete c;
   return MCNLA_B200_OK;
 }

@@ -326,6 +326,10 @@ Plan make_plan(const Context* ctx, int64_t M, int64_t N, int64_t K, int batch, i
 
 }  // namespace
 
+int dgemm_heuristic_splits(const Context* c, int64_t M, int64_t N, int64_t K, int batch) {
+  return (M <= 0 || N <= 0) ? 1 : make_plan(c, M, N, K, batch, 0).splits;
+}
+
 size_t dgemm_workspace_bytes(const Context* c, int64_t M, int64_t N, int64_t K, int batch) {
   if (M <= 0 || N <= 0) return 0;
   Plan p = make_plan(c, M, N, K, batch, 0);

@@ -23,6 +23,10 @@ struct GemmBatch {
 
 // Bytes of workspace dgemm() needs for this shape (0 when no split-K is used).
 size_t dgemm_workspace_bytes(const Context* c, int64_t M, int64_t N, int64_t K, int batch);
+// The split-K count the shape heuristic picks for this product (1: none).  Every
+// element's sum depends only on K and this count, not on M, so row blocks of a
+// product computed with the same count equal the rows of the whole product.
+int dgemm_heuristic_splits(const Context* c, int64_t M, int64_t N, int64_t K, int batch);
 
 // Launches C := alpha*A*B + beta*C on ctx->stream.  ws may be null when
 // dgemm_workspace_bytes() is 0.  force_splits > 0 overrides the split choice

@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <vector>
 
 namespace mb {
 namespace {
@@ -922,6 +923,55 @@ int run_isvd(Context* c, const Dims& d, int integrator, int former, const double
   return MCNLA_B200_OK;
 }
 
+// Host-buffer solve with A streamed in: the row-major host A is copied to the
+// device in row blocks on the context's copy stream, and the sketch GEMM of
+// each block (Q rows := A rows * Omega, gaussian_projection_sketcher.hpp:96)
+// starts as soon as its block has landed, so the copy of A hides behind the
+// sketch.  Each block's GEMM uses the split-K count of the whole product, so
+// every element of Q equals the whole-product GEMM's.
+int run_sketch_streamed(Context* c, const Dims& d, const double* A_host, double* A, const double* omega_host,
+                        double* omega, double* Q) {
+  const size_t row_bytes = size_t(d.n) * sizeof(double);
+  const int64_t rows_per = std::max<int64_t>(
+      128, std::min<int64_t>(int64_t((size_t(1) << 30) / row_bytes), cdiv(d.m, 4)));
+  const int nblocks = int(cdiv(d.m, rows_per));
+  const int splits = dgemm_heuristic_splits(c, d.m, d.L, d.n, 1);
+  const size_t wsb = splits > 1 ? size_t(splits) * rows_per * d.L * sizeof(double) : 0;
+  Plan pl;
+  pl.add(wsb / 8 + 1);
+  MB_CHECK(ctx_reserve(c, pl.bytes));
+  double* ws = take_ws(c, wsb);
+  MB_CHECK(check_arena(c));
+  if (!c->copy_stream) MB_CHECK_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+  std::vector<cudaEvent_t> ev(size_t(nblocks) + 1, nullptr);
+  struct Events {
+    std::vector<cudaEvent_t>& v;
+    ~Events() { for (auto e : v) if (e) cudaEventDestroy(e); }
+  } release{ev};
+  for (auto& e : ev) MB_CHECK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  // the copies start after the work already queued on the compute stream (which may still use the buffers)
+  MB_CHECK_CUDA(cudaEventRecord(ev[nblocks], c->stream));
+  MB_CHECK_CUDA(cudaStreamWaitEvent(c->copy_stream, ev[nblocks], 0));
+  MB_CHECK_CUDA(cudaMemcpyAsync(omega, omega_host, size_t(d.n) * d.L * sizeof(double), cudaMemcpyHostToDevice,
+                                c->copy_stream));
+  for (int b = 0; b < nblocks; ++b) {
+    const int64_t r0 = b * rows_per, rows = std::min<int64_t>(rows_per, d.m - r0);
+    MB_CHECK_CUDA(cudaMemcpyAsync(A + r0 * d.n, A_host + r0 * d.n, size_t(rows) * row_bytes, cudaMemcpyHostToDevice,
+                                  c->copy_stream));
+    MB_CHECK_CUDA(cudaEventRecord(ev[b], c->copy_stream));
+  }
+  MB_CHECK(ctx_tic(c));
+  MB_CHECK(ctx_toc(c));   // "random generating" part: Omega is given
+  for (int b = 0; b < nblocks; ++b) {
+    const int64_t r0 = b * rows_per, rows = std::min<int64_t>(rows_per, d.m - r0);
+    MB_CHECK_CUDA(cudaStreamWaitEvent(c->stream, ev[b], 0));
+    MB_CHECK(dgemm(c, rows, d.L, d.n, 1.0, crow(A + r0 * d.n, d.n), crow(omega, d.L), 0.0, drow(Q + r0 * d.L, d.L),
+                   GemmBatch(), ws, splits));
+  }
+  MB_CHECK(ctx_toc(c));
+  return MCNLA_B200_OK;
+}
+
 // FP64 flops of the lower-triangle Bs = Qs' Qs (L^2 m) from which the mixed
 // solve forms it from BF16 parts instead.
 constexpr double kMixedGramianMinFlops = 1e11;
@@ -1088,15 +1138,25 @@ int mcnla_b200_isvd_host(mcnla_b200_ctx* ctx, const mcnla_b200_params* params, i
   double* V = reinterpret_cast<double*>(base);
   base += mb::arena_bytes_for(size_t(d.n) * d.k, 8);
   // omega goes straight into its pipeline slot
-  MB_CHECK_CUDA(cudaMemcpyAsync(A, A_host, a_elems * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   char* pbase = base;
+  double* Q = reinterpret_cast<double*>(pbase);
+  double* Qbar = reinterpret_cast<double*>(pbase + mb::arena_bytes_for(size_t(d.m) * d.L, 8));
   double* omega_dev = reinterpret_cast<double*>(pbase + mb::arena_bytes_for(size_t(d.m) * d.L, 8) +
                                                 mb::arena_bytes_for(size_t(d.m) * d.l, 8));
-  MB_CHECK_CUDA(cudaMemcpyAsync(omega_dev, omega_host, size_t(d.n) * d.L * sizeof(double), cudaMemcpyHostToDevice,
-                                ctx->stream));
   const int64_t lda = a_layout == MCNLA_B200_ROW_MAJOR ? d.n : d.m;
-  MB_CHECK(mb::run_isvd(ctx, d, integrator, former, A, a_layout, lda, omega_dev, 0, max_iteration, tolerance, S, U,
-                        V, iteration, pbase));
+  if (a_layout == MCNLA_B200_ROW_MAJOR && a_elems * sizeof(double) >= (size_t(64) << 20)) {
+    // large row-major A: copied in row blocks behind the sketch
+    MB_CHECK(mb::run_sketch_streamed(ctx, d, A_host, A, omega_host, omega_dev, Q));
+    MB_CHECK(mb::run_orthogonalize(ctx, d, Q));
+    MB_CHECK(mb::run_integrate(ctx, d, integrator, Q, max_iteration, tolerance, Qbar, iteration));
+    MB_CHECK(mb::run_form(ctx, d, former, A, a_layout, lda, Qbar, S, U, V));
+  } else {
+    MB_CHECK_CUDA(cudaMemcpyAsync(A, A_host, a_elems * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    MB_CHECK_CUDA(cudaMemcpyAsync(omega_dev, omega_host, size_t(d.n) * d.L * sizeof(double),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    MB_CHECK(mb::run_isvd(ctx, d, integrator, former, A, a_layout, lda, omega_dev, 0, max_iteration, tolerance, S,
+                          U, V, iteration, pbase));
+  }
   MB_CHECK_CUDA(cudaMemcpyAsync(S_host, S, size_t(d.k) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   if (U_host)
     MB_CHECK_CUDA(cudaMemcpyAsync(U_host, U, size_t(d.m) * d.k * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));

@@ -381,6 +381,24 @@ def test_host_entry_point_matches_device(cuda):
     np.testing.assert_allclose(s3.numpy(), s2.numpy(), rtol=1e-12)
 
 
+@pytest.mark.parametrize("m,n", [(6000, 2000), (1100, 8000)])
+def test_host_entry_point_streams_large_a(cuda, m, n):
+    """Row-major host A of 64 MB or more is copied in row blocks behind the sketch; the result is
+    bit for bit the device-resident solve's (the second shape's whole sketch GEMM uses split-K,
+    which every row block repeats)."""
+    from mcnla_b200 import isvd, synthetic
+    a, omega = synthetic.config1_numpy(m=m, n=n, k=8, p=8, N=4, seed=6)
+    assert a.nbytes >= 64 << 20
+    s1, u1, v1, it1 = isvd.solve(dev(a, cuda), 8, 8, 4, omega=dev(omega, cuda), integrator="rb_gramian_kn",
+                                 former="rb_gramian")
+    a_h = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    o_h = torch.from_numpy(np.ascontiguousarray(omega)).pin_memory()
+    for _ in range(2):
+        s2, u2, v2, it2 = isvd.solve_host(a_h, o_h, 8, 8, 4, integrator="rb_gramian_kn", former="rb_gramian")
+        assert it1 == it2
+        assert torch.equal(s1.cpu(), s2) and torch.equal(u1.cpu(), u2) and torch.equal(v1.cpu(), v2)
+
+
 def test_stage_api_pipeline_with_device_omega(cuda):
     """Stages chained as the reference's driver does, Omega drawn on the device."""
     from mcnla_b200 import isvd, synthetic
