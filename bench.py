@@ -34,10 +34,10 @@ sys.path.insert(0, ROOT)
 METRIC = "iSVD/s & A-read GB/s, mixed vs FP64 plain on B200 at σ err≤1e-6; p50/p99 ms"
 
 # dram bytes (read + write) per row of A for one launch of the sketch GEMM, from
-# one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum: 24.97 GB +
-# 0.53 GB) of the 16384 x 20000 x 4096 case with the 128 x 128 x 32 tile; scaled
-# by rows to the benchmark's m (A is re-read ~9.5x through L2 either way)
-SKETCH_TRAFFIC_PER_ROW = (24.968428e9 + 0.532365e9) / 16384
+# one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum: 22.48 GB +
+# 0.53 GB) of the 16384 x 20000 x 4096 case with the 64 x 128 two-CTA tile;
+# scaled by rows to the benchmark's m (A is re-read ~8.6x through L2)
+SKETCH_TRAFFIC_PER_ROW = (22.475526e9 + 0.534837e9) / 16384
 
 
 def parse():
