@@ -53,6 +53,7 @@ extern "C" {
 #define MCNLA_B200_ERR_UNSUPPORTED     7  /* shape beyond a kernel's stated limit (e.g. l > 160) */
 #define MCNLA_B200_ERR_SINGULAR        8  /* exact zero pivot in a small inverse */
 #define MCNLA_B200_ERR_DEVICE_TIMEOUT  9  /* a bounded device-side wait ran out (results invalid) */
+#define MCNLA_B200_ERR_IO             10  /* a file is missing, unreadable, or not in the expected format */
 
 /* ---- enumerators -------------------------------------------------------- */
 #define MCNLA_B200_ROW_MAJOR 0
@@ -204,6 +205,43 @@ MCNLA_B200_API int mcnla_b200_isvd(mcnla_b200_ctx* ctx, const mcnla_b200_params*
 MCNLA_B200_API int mcnla_b200_isvd_host(mcnla_b200_ctx* ctx, const mcnla_b200_params* params, int integrator, int former,
                          const double* A_host, int a_layout, const double* omega_host, int max_iteration,
                          double tolerance, double* S_host, double* U_host, double* V_host, int* iteration);
+
+/* ---- files (the reference's io module; host only, no device work) -----------
+ * Dense MatrixMarket "array" text (include/mcnla/core/io/matrix_market/
+ * dense_load.hpp:70-251, dense_load_block.hpp, dense_save.hpp): '%' lines,
+ * then "m n" (a matrix) or "m n l" (a 3-D collection of l m x n matrices),
+ * then the values column-major, matrix after matrix.  A collection is read
+ * and written as its unfolded m x (n l) matrix (matrix k = columns
+ * [k n, (k + 1) n)), the layout of mcnla_b200_sketch's Q.                      */
+/* dims[0..2] := m, n, l (l = 1 for a matrix); *ndim := 2 or 3.               */
+MCNLA_B200_API int mcnla_b200_mm_size(const char* path, int64_t* dims, int* ndim);
+/* Rows [row0, row0 + rows) x columns [col0, col0 + cols) of the (unfolded)
+ * matrix into out, row-major (layout 0) or column-major (1) with leading
+ * dimension ldo: the whole matrix, a row block (loadMatrixMarketRowBlock,
+ * dense_load_block.hpp:86-130) or a column block (loadMatrixMarketColBlock,
+ * :31-74).                                                                   */
+MCNLA_B200_API int mcnla_b200_mm_load(const char* path, int64_t row0, int64_t rows, int64_t col0, int64_t cols,
+                                      double* out, int64_t ldo, int layout);
+/* Writes the unfolded m x (n nmat) matrix a (row- or column-major, leading
+ * dimension lda) as a matrix (nmat = 1) or a 3-D collection, values as the
+ * reference writes them (scientific, 16 digits after the point: exact for
+ * doubles); comment (optional, one line) follows the banner.                  */
+MCNLA_B200_API int mcnla_b200_mm_save(const char* path, const double* a, int64_t m, int64_t n, int64_t nmat,
+                                      int64_t lda, int layout, const char* comment);
+/* MCNLA dense binary files (include/mcnla/core/io/binary/dense_load.hpp:70-141,
+ * dense_save.hpp; format in doxygen/tutorial/io/binary.dox:17-30): a 128-byte
+ * header, int64 ndim, int64 dims[ndim], the values contiguous along dims[0]
+ * (a column-major matrix has dims {m, n}; the reference's row-major matrix
+ * {n, m}).  Size and value type ("R8", "R4", ...; 9 bytes with the NUL).      */
+MCNLA_B200_API int mcnla_b200_binary_size(const char* path, int64_t* dims, int* ndim, char* val_type);
+/* Slices [first, first + count) along the last dimension (each the product of
+ * the other dims), converted to double (R8 or R4 files): a row block of a
+ * row-major matrix, a column block of a column-major one
+ * (loadBinaryRowBlock / ColBlock, binary/dense_load_block.hpp).              */
+MCNLA_B200_API int mcnla_b200_binary_load(const char* path, int64_t first, int64_t count, double* out);
+/* Writes a (dims[0] fastest) as an R8 dense binary file.                     */
+MCNLA_B200_API int mcnla_b200_binary_save(const char* path, const double* a, int ndim, const int64_t* dims,
+                                          const char* comment);
 
 /* ---- mixed precision (BF16 tensor cores, tcgen05) ---------------------------
  * The sketch A * Omega is where the plain FP64 path spends most of its time.

@@ -13,7 +13,7 @@ HEADER_PATH = os.path.join(os.path.dirname(HERE), "include", "mcnla_b200.h")
 
 OK = 0
 ERR_SHAPE, ERR_LAYOUT, ERR_WORKSPACE, ERR_CUDA, ERR_NOMEM, ERR_ARG, ERR_UNSUPPORTED, ERR_SINGULAR, \
-    ERR_DEVICE_TIMEOUT = range(1, 10)
+    ERR_DEVICE_TIMEOUT, ERR_IO = range(1, 11)
 
 ROW_MAJOR, COL_MAJOR = 0, 1
 
@@ -76,6 +76,12 @@ SIGNATURES = {
     "mcnla_b200_destroy": (_INT, [_P]),
     "mcnla_b200_set_stream": (_INT, [_P, _P]),
     "mcnla_b200_status_string": (ctypes.c_char_p, [_INT]),
+    "mcnla_b200_mm_size": (_INT, [ctypes.c_char_p, ctypes.POINTER(_I64), ctypes.POINTER(_INT)]),
+    "mcnla_b200_mm_load": (_INT, [ctypes.c_char_p, _I64, _I64, _I64, _I64, _P, _I64, _INT]),
+    "mcnla_b200_mm_save": (_INT, [ctypes.c_char_p, _P, _I64, _I64, _I64, _I64, _INT, ctypes.c_char_p]),
+    "mcnla_b200_binary_size": (_INT, [ctypes.c_char_p, ctypes.POINTER(_I64), ctypes.POINTER(_INT), ctypes.c_char_p]),
+    "mcnla_b200_binary_load": (_INT, [ctypes.c_char_p, _I64, _I64, _P]),
+    "mcnla_b200_binary_save": (_INT, [ctypes.c_char_p, _P, _INT, ctypes.POINTER(_I64), ctypes.c_char_p]),
     "mcnla_b200_last_error": (ctypes.c_char_p, []),
     "mcnla_b200_kernels_launched": (_I64, [_P]),
     "mcnla_b200_graph_replays": (_I64, [_P]),

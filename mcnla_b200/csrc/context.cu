@@ -117,6 +117,7 @@ const char* mcnla_b200_status_string(int status) {
     case MCNLA_B200_ERR_UNSUPPORTED: return "shape beyond a kernel limit";
     case MCNLA_B200_ERR_SINGULAR: return "singular matrix in a small inverse";
     case MCNLA_B200_ERR_DEVICE_TIMEOUT: return "a bounded device-side wait ran out";
+    case MCNLA_B200_ERR_IO: return "a file is missing, unreadable, or not in the expected format";
     default: return "unknown status";
   }
 }
