@@ -287,6 +287,85 @@ using GramianFormer = FormerStage<MCNLA_B200_GRAMIAN_FORMER>;
 using RowBlockGramianFormer = FormerStage<MCNLA_B200_ROW_BLOCK_GRAMIAN_FORMER>;
 using ColBlockGramianFormer = FormerStage<MCNLA_B200_COL_BLOCK_GRAMIAN_FORMER>;
 
+// Dense files with the reference's names (include/mcnla/core/io/): host
+// matrices as std::vector<double> in the requested layout; a 3-D MatrixMarket
+// collection is its unfolded m x (n l) matrix.
+namespace io {
+
+struct HostMatrix {
+  std::vector<double> val;
+  int64_t nrow = 0, ncol = 0;
+  int layout = MCNLA_B200_ROW_MAJOR;   // leading dimension ncol (row-major) or nrow (column-major)
+};
+
+// (m, n, l) of a dense MatrixMarket file (matrix_market/dense_load_block.hpp:13-29)
+inline std::vector<int64_t> loadMatrixMarketSize(const char* file) {
+  std::vector<int64_t> dims(3);
+  int nd = 0;
+  check(mcnla_b200_mm_size(file, dims.data(), &nd), "loadMatrixMarketSize");
+  return dims;
+}
+
+// rows [row0, row0 + rows) x columns [col0, col0 + cols); rows < 0 / cols < 0: to the end
+inline HostMatrix loadMatrixMarketBlock(const char* file, int64_t row0, int64_t rows, int64_t col0, int64_t cols,
+                                        int layout = MCNLA_B200_ROW_MAJOR) {
+  const std::vector<int64_t> d = loadMatrixMarketSize(file);
+  HostMatrix a;
+  a.nrow = rows < 0 ? d[0] - row0 : rows;
+  a.ncol = cols < 0 ? d[1] * d[2] - col0 : cols;
+  a.layout = layout;
+  a.val.resize(size_t(a.nrow * a.ncol));
+  const int64_t ld = layout == MCNLA_B200_ROW_MAJOR ? a.ncol : a.nrow;
+  check(mcnla_b200_mm_load(file, row0, a.nrow, col0, a.ncol, a.val.data(), ld > 0 ? ld : 1, layout),
+        "loadMatrixMarket");
+  return a;
+}
+
+// matrix_market/dense_load.hpp:70-251
+inline HostMatrix loadMatrixMarket(const char* file, int layout = MCNLA_B200_ROW_MAJOR) {
+  return loadMatrixMarketBlock(file, 0, -1, 0, -1, layout);
+}
+// matrix_market/dense_load_block.hpp:86-130 (row-major rows) and :31-74 (column-major columns)
+inline HostMatrix loadMatrixMarketRowBlock(const char* file, int64_t row0, int64_t rows) {
+  return loadMatrixMarketBlock(file, row0, rows, 0, -1, MCNLA_B200_ROW_MAJOR);
+}
+inline HostMatrix loadMatrixMarketColBlock(const char* file, int64_t col0, int64_t cols) {
+  return loadMatrixMarketBlock(file, 0, -1, col0, cols, MCNLA_B200_COL_MAJOR);
+}
+
+// matrix_market/dense_save.hpp (nmat > 1: a 3-D collection)
+inline void saveMatrixMarket(const HostMatrix& a, const char* file, int64_t nmat = 1, const char* comment = nullptr) {
+  const int64_t ld = a.layout == MCNLA_B200_ROW_MAJOR ? a.ncol : a.nrow;
+  check(mcnla_b200_mm_save(file, a.val.data(), a.nrow, a.ncol / nmat, nmat, ld > 0 ? ld : 1, a.layout, comment),
+        "saveMatrixMarket");
+}
+
+// binary/dense_load.hpp:52-86 for a matrix: dims {ncol, nrow} hold a row-major
+// matrix, {nrow, ncol} a column-major one (layout says which the file is)
+inline HostMatrix loadBinary(const char* file, int layout = MCNLA_B200_ROW_MAJOR) {
+  int64_t dims[3];
+  int nd = 0;
+  char vt[9];
+  check(mcnla_b200_binary_size(file, dims, &nd, vt), "loadBinary");
+  if (nd != 2) throw Error(MCNLA_B200_ERR_SHAPE, "loadBinary: not a matrix");
+  HostMatrix a;
+  a.layout = layout;
+  a.nrow = layout == MCNLA_B200_ROW_MAJOR ? dims[1] : dims[0];
+  a.ncol = layout == MCNLA_B200_ROW_MAJOR ? dims[0] : dims[1];
+  a.val.resize(size_t(dims[0] * dims[1]));
+  check(mcnla_b200_binary_load(file, 0, dims[1], a.val.data()), "loadBinary");
+  return a;
+}
+
+// binary/dense_save.hpp:60-100
+inline void saveBinary(const HostMatrix& a, const char* file, const char* comment = nullptr) {
+  const int64_t dims[2] = {a.layout == MCNLA_B200_ROW_MAJOR ? a.ncol : a.nrow,
+                           a.layout == MCNLA_B200_ROW_MAJOR ? a.nrow : a.ncol};
+  check(mcnla_b200_binary_save(file, a.val.data(), 2, dims, comment), "saveBinary");
+}
+
+}  // namespace io
+
 }  // namespace mcnla_b200
 
 #endif  // MCNLA_B200_ISVD_HPP_

@@ -12,11 +12,11 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 
 
-def build(out_dir):
-    exe = os.path.join(out_dir, "check_isvd")
+def build(out_dir, name="check_isvd"):
+    exe = os.path.join(out_dir, name)
     lib_dir = os.path.join(ROOT, "mcnla_b200")
     cmd = ["g++", "-std=c++14", "-O2", "-I", os.path.join(ROOT, "include"), "-I", os.path.join(CUDA, "include"),
-           os.path.join(ROOT, "tests", "cpp", "check_isvd.cpp"), "-o", exe,
+           os.path.join(ROOT, "tests", "cpp", name + ".cpp"), "-o", exe,
            "-L", lib_dir, "-lmcnla_b200", "-Wl,-rpath," + lib_dir,
            "-L", os.path.join(CUDA, "lib64"), "-lcudart", "-Wl,-rpath," + os.path.join(CUDA, "lib64")]
     subprocess.run(cmd, check=True, capture_output=True, text=True)
@@ -27,6 +27,16 @@ def test_cpp_api_compiles(tmp_path):
     if shutil.which("g++") is None:
         pytest.skip("no g++")
     assert os.path.exists(build(str(tmp_path)))
+
+
+def test_cpp_io_round_trips(tmp_path):
+    """The C++ file API (mcnla_b200::io): host only, so it runs here."""
+    if shutil.which("g++") is None:
+        pytest.skip("no g++")
+    exe = build(str(tmp_path), "check_io")
+    r = subprocess.run([exe, str(tmp_path)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.strip().endswith("OK")
 
 
 @pytest.mark.gpu
