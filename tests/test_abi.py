@@ -72,3 +72,30 @@ def test_create_without_gpu_fails_cleanly():
     assert st == _lib.ERR_CUDA
     assert not h.value
     assert lib.mcnla_b200_last_error()
+
+
+def test_header_is_plain_c(tmp_path):
+    """include/mcnla_b200.h is a C header (C99, no warnings under -Wall -Wextra -pedantic) and
+    a C program links the library and calls it (host-only entry points: no GPU needed)."""
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("no gcc")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / "abi_check.c"
+    src.write_text(
+        "#include <mcnla_b200.h>\n#include <stdio.h>\n"
+        "int main(void) {\n"
+        "  int64_t dims[3]; int nd = 0;\n"
+        "  printf(\"%s\\n\", mcnla_b200_status_string(MCNLA_B200_ERR_IO));\n"
+        "  return mcnla_b200_mm_size(\"/nonexistent/x.mtx\", dims, &nd) == MCNLA_B200_ERR_IO ? 0 : 1;\n"
+        "}\n")
+    exe = tmp_path / "abi_check"
+    lib_dir = os.path.join(root, "mcnla_b200")
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I",
+                        os.path.join(root, "include"), str(src), "-o", str(exe), "-L", lib_dir, "-lmcnla_b200",
+                        "-Wl,-rpath," + lib_dir], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "file" in r.stdout
