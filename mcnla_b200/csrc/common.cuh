@@ -135,6 +135,10 @@ int ctx_sync_scalars(Context* c);   // copies DevScalars to the pinned mirror an
 
 inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+// FP64 flops of the lower-triangle Bs = Qs' Qs ((N l)^2 m) from which a mixed
+// solve forms Bs (and its Gramian loop's Bs Bc) from BF16 parts instead.
+constexpr double kMixedGramianMinFlops = 1e11;
+
 }  // namespace mb
 
 // The opaque handle of the C ABI is the context itself.

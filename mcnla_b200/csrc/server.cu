@@ -54,6 +54,12 @@ int64_t problem_bytes(const mcnla_b200_problem& p) {
   if (!p.A && p.A32) bytes += m * n * 8;                                        // FP64 copy of an FP32 A
   if (p.precision == MCNLA_B200_PRECISION_MIXED) bytes += 2 * m * round8(n) * 2 + L * round8(n) * 2;
   if (p.precision == MCNLA_B200_PRECISION_MIXED3) bytes += 3 * m * round8(n) * 2 + L * round8(n) * 2;
+  const bool gramian = p.integrator == MCNLA_B200_ROW_BLOCK_GRAMIAN_KOLMOGOROV_NAGUMO ||
+                       p.integrator == MCNLA_B200_ROW_BLOCK_GRAMIAN_WEN_YIN;
+  if (p.precision != MCNLA_B200_PRECISION_FP64 && gramian && double(L) * double(L) * double(m) >= kMixedGramianMinFlops) {
+    // the BF16 Gramian's scratch: three parts of Qs', of Bs and of Bc', and the loop's split-K slices
+    bytes += 3 * L * round8(m) * 2 + 3 * L * round8(L) * 2 + 3 * l * round8(L) * 2 + 16 * L * 3 * l * 8;
+  }
   return bytes;
 }
 

@@ -972,10 +972,6 @@ int run_sketch_streamed(Context* c, const Dims& d, const double* A_host, double*
   return MCNLA_B200_OK;
 }
 
-// FP64 flops of the lower-triangle Bs = Qs' Qs (L^2 m) from which the mixed
-// solve forms it from BF16 parts instead.
-constexpr double kMixedGramianMinFlops = 1e11;
-
 // Mixed solve: Omega drawn in BF16, sketch on tcgen05, FP64 afterwards.
 int run_isvd_mixed(Context* c, const Dims& d, int integrator, int former, const double* A, int layout, int64_t lda,
                    const uint16_t* a_hi, const uint16_t* a_lo, const uint16_t* a_lo2, int64_t lda16,
