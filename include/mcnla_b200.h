@@ -248,9 +248,10 @@ MCNLA_B200_API int mcnla_b200_binary_save(const char* path, const double* a, int
  * The mixed path keeps A as two or three BF16 parts, A = A_hi + A_lo (+
  * A_lo2): 16 or 24 bits of mantissa (three parts hold an FP32 A exactly),
  * draws Omega directly in BF16, and runs the sketch on the tcgen05 tensor
- * cores with FP32 accumulation; the orthogonalizer, integrator and former
- * stay FP64.  BF16 buffers are uint16_t bit patterns, K-major (row pitch a
- * multiple of 8 elements, 16-byte aligned base).                            */
+ * cores with FP32 accumulation; large Gramian-integrator products and, when
+ * BF16 parts of A' are given, the former's product run there too, and every
+ * small factorization stays FP64.  BF16 buffers are uint16_t bit patterns,
+ * K-major (row pitch a multiple of 8 elements, 16-byte aligned base).        */
 
 /* hi := bf16(A), lo := bf16(A - hi), lo2 := bf16(A - hi - lo) (lo, lo2 may be
  * NULL), row-major m x n with pitch ldo, from FP64 A (row- or column-major). */
