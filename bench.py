@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--cpu-rows", type=int, default=0, help="row sample of the CPU baseline (0: auto)")
+    ap.add_argument("--ref-budget", type=float, default=1200.0,
+                    help="reference arm: seconds of timed full solves; no step starts that would end past it")
     ap.add_argument("--quick", action="store_true", help="small shape for a smoke run")
     ap.add_argument("--no-serving", action="store_true", help="skip the batched / served leg")
     ap.add_argument("--kernel", choices=["sketch_bf16", "gkn", "trace"], default=None,
@@ -263,6 +265,47 @@ def stage_rooflines(m, n, k, l, N, integrator, former, stages, peak_tflops, hbm_
     out["peaks"] = {"fp64_tflops": round(peak_tflops, 3), "hbm_gbs": hbm_gbs,
                     "source": "FP64: cuBLAS DGEMM measured in this run; HBM: MEASURED_PEAKS.json hbm_gbs of measured"}
     return out
+
+
+def run_config1_b200(args, dev):
+    """Configuration 1 in full on this build: device-resident A and Omega (value), and the same
+    through mcnla_b200_isvd_host with pinned host A and Omega in and S/U/V out (e2e)."""
+    import torch
+    from mcnla_b200 import isvd
+    a_np, om_np = config1_inputs()
+    a = torch.as_tensor(a_np, device=dev)
+    om = torch.as_tensor(om_np, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    kw = dict(integrator="kn", former="svd", maxit=256, tol=1e-4)
+    for _ in range(max(1, args.warmup)):
+        s, u, v, it = isvd.solve(a, 10, 10, 16, omega=om, **kw)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        s, u, v, it = isvd.solve(a, 10, 10, 16, omega=om, **kw)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3 / args.steps
+    a_h = torch.from_numpy(a_np).pin_memory()
+    om_h = torch.from_numpy(om_np).pin_memory()
+    out = (torch.empty(10, dtype=torch.float64, pin_memory=True),
+           torch.empty(1000, 10, dtype=torch.float64, pin_memory=True),
+           torch.empty(2000, 10, dtype=torch.float64, pin_memory=True))
+    isvd.solve_host(a_h, om_h, 10, 10, 16, out=out, device=dev, **kw)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        isvd.solve_host(a_h, om_h, 10, 10, 16, out=out, device=dev, **kw)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_e2e = e0.elapsed_time(e1) / 1e3 / args.steps
+    return {**CONFIG1, "value": round(1.0 / t, 3), "unit": "iSVD/s", "ms_per_step": round(t * 1e3, 4),
+            "steps": args.steps, "iterations": it,
+            "e2e": {"value": round(1.0 / t_e2e, 3), "unit": "iSVD/s", "h2d_bytes_per_step": int((a_np.size + om_np.size) * 8),
+                    "d2h_bytes_per_step": int((10 + 1000 * 10 + 2000 * 10) * 8)},
+            "reconstruction_rel_err": reconstruction_error_torch(a, s, u, v),
+            "sigma": [float(x) for x in s[:3].tolist()]}
 
 
 def run_b200(args, world, rank, local):
@@ -473,6 +516,8 @@ def run_b200(args, world, rank, local):
                "path": "mcnla_b200_isvd_host (pinned host A and Omega in, S/U/V out)"}
         del a_host, om_host
 
+    recon = reconstruction_error_torch(a, s, u, v)
+    c1 = run_config1_b200(args, dev) if world == 1 and not args.quick else None
     result = {
         "metric": METRIC, "value": round(value, 5), "unit": "iSVD/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(total / args.steps * 1e3, 3), "higher_is_better": True,
@@ -484,6 +529,7 @@ def run_b200(args, world, rank, local):
         "iterations": iters[-1], "stages": stages, "integrators": variants, "mixed": mixed, "roofline": roofline,
         "stage_roofline": stage_roof, "e2e": e2e,
         "gpu_launches": int(launches), "clocks": clk,
+        "reconstruction_rel_err": recon, "config1": c1,
     }
     return result
 
@@ -509,7 +555,7 @@ def run_serving(args, dev):
     from mcnla_b200 import isvd, synthetic
 
     W = args.serve_workers
-    budget = 150 << 30
+    budget = int(150e9)   # the configuration's 150 GB admission cap
     shapes = synthetic.batch_shapes(args.batch_count, seed=4)
     pool = [synthetic.lowrank_torch(sh["m"], sh["n"], sh["sigma"], seed=sh["seed"], device=dev, dtype=torch.float32)
             for sh in shapes]
@@ -640,7 +686,7 @@ def run_serving(args, dev):
     torch.cuda.empty_cache()
     return {
         "workload": "%d uneven FP32 matrices (m~U[512,16384], n~U[256,4096], k in {8,16,32,64}, p=k/2, N=8, "
-                    "sigma_j=j^-alpha, alpha~U[0.5,2], spectrum cut at 256), %s tol 1e-5, %s former"
+                    "sigma_j=j^-alpha over j=1..min(m,n), alpha~U[0.5,2]), %s tol 1e-5, %s former"
                     % (len(shapes), args.serve_integrator, args.serve_former),
         "timing": "host wall clock, device synchronized on both sides; solves on the workers' own streams",
         "per_request_fp64": serial64, "batched_fp64": batched64, "batched_mixed": batched_mx,
@@ -804,29 +850,161 @@ def cpu_sample(args, rows=None):
         detail = {"integrate_iterations": r["iterations"], "sample_wall_s": wall}
     sample = ("first %d of %d rows (same n, k, p, N, spectrum); row-proportional stage times scaled by %.1f"
               % (rows, m, scale))
-    return est, {"cores": cores, "kind": kind, "sample": sample, "detail": detail}
+    return est, {"cores": cores, "kind": kind, "sample": sample, "detail": detail,
+                 "sample_iterations": detail.get("integrate_iterations")}
+
+
+def workload_matrix(args, rank=0, device=None):
+    """The workload's A: U_r diag(exp(-j/30)) V_r' + 1e-4 G from the seeded generator of this
+    build's arm (rank r uses seed 1000 + r).  Built on `device` (the GPU when given)."""
+    import numpy as np
+    from mcnla_b200 import synthetic
+    sigma = np.exp(-np.arange(1, args.rank_r + 1) / 30.0)
+    return synthetic.lowrank_torch(args.m, args.n, sigma, seed=1000 + rank, noise=1e-4,
+                                   device=device or "cpu", colmajor=args.colmajor)
+
+
+def reconstruction_error_np(a, s, u, v, chunk=8192):
+    """||A - U diag(S) V'||_F / ||A||_F, the reference drivers' check (src/isvd_dense_rb.cpp:291-315),
+    in row chunks of A."""
+    import numpy as np
+    num = den = 0.0
+    us = u * s
+    for r0 in range(0, a.shape[0], chunk):
+        blk = np.asarray(a[r0:r0 + chunk])
+        num += float(np.sum((blk - us[r0:r0 + chunk] @ v.T) ** 2))
+        den += float(np.sum(blk * blk))
+    return (num / den) ** 0.5
+
+
+def reconstruction_error_torch(a, s, u, v, chunk=8192):
+    """The same check on the device (a may be a column-major view)."""
+    num = den = 0.0
+    us = u * s
+    for r0 in range(0, a.shape[0], chunk):
+        blk = a[r0:r0 + chunk]
+        num += float(((blk - us[r0:r0 + chunk] @ v.t()) ** 2).sum().item())
+        den += float((blk * blk).sum().item())
+    return (num / den) ** 0.5
+
+
+REF_KINDS = {"kn": 0, "rb_kn": 1, "rb_gramian_kn": 2, "rb_wy": 3, "rb_gramian_wy": 4}
+REF_FORMERS = {"svd": 0, "gramian": 1, "rb_gramian": 2, "cb_gramian": 3}
+
+
+def ref_solver(lib, a, omega, k, p, N, integrator, former, maxit, tol, colmajor=False, row_block=True):
+    """The reference's own stages (oracle/_ref) set up for repeated whole solves: A and Omega
+    loaded and the stages initialized once (the reference drivers' order, src/isvd_dense_rb.cpp:
+    118-221); each run() reports the stages' own timers (report/include/stage.hpp pattern)."""
+    from oracle import ref_lib
+    return ref_lib.Solver(lib, a, omega, k, p, N, REF_KINDS[integrator], REF_FORMERS[former], maxit, tol,
+                          colmajor=colmajor, row_block=row_block)
+
+
+def config1_inputs():
+    """Configuration 1: A = U diag(1/j) V' (1000 x 2000, U and V the Q factors of seeded
+    Gaussians), Omega 2000 x 320 N(0,1) from seed 0; k = 10, p = 10, N = 16."""
+    from mcnla_b200 import synthetic
+    return synthetic.config1_numpy(m=1000, n=2000, k=10, p=10, N=16, seed=0)
+
+
+CONFIG1 = {"workload": "plain iSVD, A = U diag(1/j) V', m=1000 n=2000, k=10 p=10 N=16, Omega N(0,1) seed 0",
+           "stages": "Gramian / KolmogorovNagumo (tol 1e-4, maxit 256) / Svd"}
+
+
+def run_reference_config1(lib, steps, warmup):
+    """Configuration 1 in full through the reference's stages: `steps` timed solves, each the
+    sum of the stages' own timers (the reference driver's "total computing time")."""
+    a, omega = config1_inputs()
+    sol = ref_solver(lib, a, omega, 10, 10, 16, "kn", "svd", 256, 1e-4, row_block=False)
+    for _ in range(max(1, warmup)):
+        sol.run()
+    totals, it = [], None
+    for _ in range(steps):
+        it, t = sol.run()
+        totals.append(float(t.sum()))
+    s, u, v = sol.result()
+    sol.close()
+    mean = sum(totals) / len(totals)
+    return {**CONFIG1, "value": round(1.0 / mean, 4), "unit": "iSVD/s", "ms_per_step": round(mean * 1e3, 3),
+            "steps": steps, "iterations": it, "reconstruction_rel_err": reconstruction_error_np(a, s, u, v),
+            "sigma": [float(x) for x in s[:3]]}
 
 
 def run_reference(args, world, rank):
+    """The reference's own CPU stages (oracle/_ref, OpenBLAS on all host threads) on the full
+    workload: the same A as this build's arm (its generator and seed; built on the GPU when
+    there is one, then copied to host memory) and a seeded N(0,1) Omega.  Each timed step is
+    one whole solve on the full matrix.  Warm-up steps run the stages on a 1024-row sample
+    (they only warm the BLAS threads and caches).  Timed steps stop early, before a step that
+    would end past --ref-budget seconds, and `steps` reports how many ran."""
     if rank != 0:
         return None
-    steps = []
-    info = None
-    for i in range(args.warmup + args.steps):
-        est, info = cpu_sample(args)
-        if i >= args.warmup:
-            steps.append(est)
-    mean = sum(steps) / len(steps)
+    import numpy as np
+    from oracle import ref_lib
+    from mcnla_b200 import synthetic
+    if not ref_lib.available():
+        return {"metric": METRIC, "impl": "reference", "unavailable": "oracle/_ref (the reference compiled here) is missing"}
+    lib = ref_lib.load()
+    cores = os.cpu_count() or 1
+    lib.mref_set_threads(cores)
+    k, p, N = args.k, args.p, args.N
+    L = (k + p) * N
+    gpu = False
+    try:
+        import torch
+        gpu = torch.cuda.is_available()
+    except Exception:
+        pass
+    t_setup = time.perf_counter()
+    at = workload_matrix(args, 0, device="cuda" if gpu else None)
+    a = (at.t() if args.colmajor else at).contiguous().cpu().numpy()
+    a = a.T if args.colmajor else a           # column-major A is the transpose of a C-ordered n x m buffer
+    del at
+    if gpu:
+        torch.cuda.empty_cache()
+    omega = synthetic.omega_np(args.n, L, seed=5)
+    setup_s = time.perf_counter() - t_setup
+    t_init = time.perf_counter()
+    sol = ref_solver(lib, a, omega, k, p, N, args.integrator, args.former, args.maxit, args.tol,
+                     colmajor=args.colmajor)
+    init_s = time.perf_counter() - t_init
+    for _ in range(args.warmup):
+        cpu_sample(args)
+    totals, stage_times, iters = [], [], []
+    t_begin = time.perf_counter()
+    while len(totals) < args.steps:
+        if totals and (time.perf_counter() - t_begin) + 1.1 * max(totals) > args.ref_budget:
+            break
+        it, t = sol.run()
+        totals.append(float(t.sum()))
+        stage_times.append(t)
+        iters.append(it)
+    timed_wall = time.perf_counter() - t_begin
+    s, u, v = sol.result()
+    sol.close()
+    mean = sum(totals) / len(totals)
     value = 1.0 / mean
+    names = ("sketch_s", "orthogonalize_s", "integrate_s", "form_s")
+    detail = {nm: round(float(sum(t[i] for t in stage_times)) / len(stage_times), 4) for i, nm in enumerate(names)}
+    c1 = run_reference_config1(lib, args.steps, args.warmup) if not args.quick else None
     return {
-        "metric": METRIC, "value": round(value, 6), "unit": "iSVD/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round(mean * 1e3, 3), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
+        "metric": METRIC, "value": round(value, 6), "unit": "iSVD/s", "n_gpus": world, "steps": len(totals),
+        "steps_requested": args.steps, "warmup": args.warmup, "ms_per_step": round(mean * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded)", "impl": "reference",
         "config": dict(workload(args), parallelism="host CPU"),
-        "cpu_baseline": {"value": round(value, 6), "unit": "iSVD/s", "cores": info["cores"], "kind": info["kind"],
-                         "sample": info["sample"]},
+        "cpu_baseline": {"value": round(value, 6), "unit": "iSVD/s", "cores": cores, "kind": "reference",
+                         "sample": "none: every timed step is one whole solve of the full %d x %d matrix "
+                                   "(warm-ups on a 1024-row sample)" % (args.m, args.n)},
         "e2e": {"value": round(value, 6), "unit": "iSVD/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "detail": info["detail"],
+        "timing": "per step the sum of the four stages' own timers (the reference driver's total computing "
+                  "time; A and Omega loaded and the stages initialized once before, as its drivers do)",
+        "a_read_gbs": round(2 * args.m * args.n * 8 / mean / 1e9, 3),
+        "iterations": iters[-1], "iterations_all": iters, "stage_s": detail, "setup_s": round(setup_s, 1),
+        "budget_s": args.ref_budget, "timed_wall_s": round(timed_wall, 1), "init_s": round(init_s, 1),
+        "reconstruction_rel_err": reconstruction_error_np(a, s, u, v),
+        "config1": c1,
     }
 
 
@@ -852,7 +1030,9 @@ def main():
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             est, info = cpu_sample(args)
             res["cpu_baseline"] = {"value": round(1.0 / est, 6), "unit": "iSVD/s", "cores": info["cores"],
-                                   "kind": info["kind"], "sample": info["sample"]}
+                                   "kind": info["kind"], "sample": info["sample"], "estimated": True,
+                                   "sample_iterations": info["sample_iterations"],
+                                   "full_run_iterations": res.get("iterations")}
     if rank == 0 and res is not None:
         print(json.dumps(res), flush=True)
     if world > 1:

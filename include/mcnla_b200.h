@@ -382,8 +382,11 @@ MCNLA_B200_API int mcnla_b200_inverse_batched(mcnla_b200_ctx* ctx, int n, int ba
  * context: it runs on `stream` (NULL: the default stream) on the current
  * device, and keeps the split-K partial sums in a 16 MiB device array that
  * the library defines (held on every GPU that loads the library until the
- * process exits).  The first call on each device looks that array's address
- * up (cudaGetSymbolAddress); make that first call before any stream capture.
+ * process exits).  Every call looks that array's address up
+ * (cudaGetSymbolAddress), so the entry point stays valid across a
+ * cudaDeviceReset; the first call on each device may load the library's
+ * module for that lookup, so make it before any stream capture (calls on a
+ * capturing stream reuse the device's last looked-up address).
  * Shapes whose partial sums need more than MCNLA_B200_NOALLOC_SCRATCH_BYTES
  * are rejected with MCNLA_B200_ERR_SHAPE (mcnla_b200_last_error names the
  * size).  All calls on a device share the array: calls that overlap on the

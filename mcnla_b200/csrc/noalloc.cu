@@ -25,24 +25,35 @@ constexpr size_t kScratchBytes = size_t(16) << 20;   // MCNLA_B200_NOALLOC_SCRAT
 static __device__ __align__(256) double g_splitk_scratch[kScratchBytes / sizeof(double)];
 
 // In host code g_splitk_scratch names a host-side shadow, not device memory:
-// the device address is looked up once per device (with that device current)
-// and cached here.
+// the device address is looked up with the device current.  It is looked up
+// again on every call, because a cudaDeviceReset recreates the device's
+// primary context and the library's module with it, which may move the
+// array; the last address seen on each device is kept only for calls made
+// while their stream is being captured into a CUDA graph (a lookup that has
+// to load the module is not allowed then).
 constexpr int kMaxDevices = 64;
 double* g_scratch_addr[kMaxDevices] = {};
 std::mutex g_scratch_mutex;
 
-int scratch_address(int device, double** out) {
+int scratch_address(int device, cudaStream_t stream, double** out) {
   if (device < 0 || device >= kMaxDevices) return MCNLA_B200_ERR_ARG;
   std::lock_guard<std::mutex> lock(g_scratch_mutex);
-  if (!g_scratch_addr[device]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_splitk_scratch);
-    if (e != cudaSuccess) {
-      mb::set_last_cuda_error(e, "cudaGetSymbolAddress(g_splitk_scratch)", __FILE__, __LINE__);
-      return MCNLA_B200_ERR_CUDA;
-    }
-    g_scratch_addr[device] = static_cast<double*>(p);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(stream, &cap) != cudaSuccess) {
+    (void)cudaGetLastError();
+    cap = cudaStreamCaptureStatusNone;
   }
+  if (cap != cudaStreamCaptureStatusNone && g_scratch_addr[device]) {
+    *out = g_scratch_addr[device];
+    return MCNLA_B200_OK;
+  }
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_splitk_scratch);
+  if (e != cudaSuccess) {
+    mb::set_last_cuda_error(e, "cudaGetSymbolAddress(g_splitk_scratch)", __FILE__, __LINE__);
+    return MCNLA_B200_ERR_CUDA;
+  }
+  g_scratch_addr[device] = static_cast<double*>(p);
   *out = g_scratch_addr[device];
   return MCNLA_B200_OK;
 }
@@ -58,7 +69,7 @@ extern "C" int mcnla_b200_dgemm_noalloc(void* stream, int64_t M, int64_t N, int6
   int device = 0;
   MB_CHECK_CUDA(cudaGetDevice(&device));
   double* scratch = nullptr;
-  MB_CHECK(scratch_address(device, &scratch));
+  MB_CHECK(scratch_address(device, static_cast<cudaStream_t>(stream), &scratch));
   int sms = 0;
   MB_CHECK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
   // A context on the stack: stream, SM count and the static scratch as the

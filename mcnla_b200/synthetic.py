@@ -98,10 +98,10 @@ def omega_torch(n, L, seed=0, device="cuda"):
 # ----------------------------------------------------------------------------------------------
 # uneven batches and served requests
 # ----------------------------------------------------------------------------------------------
-def batch_shapes(count, seed=0, r_max=256):
+def batch_shapes(count, seed=0, r_max=None):
     """`count` uneven problems: m ~ U[512, 16384], n ~ U[256, 4096], k in {8, 16, 32, 64},
-    p = k / 2, N = 8, sigma_j = j^-alpha with alpha ~ U[0.5, 2] (j = 1 .. min(m, n, r_max);
-    the spectrum is cut at r_max so the generator's QR stays cheap)."""
+    p = k / 2, N = 8, sigma_j = j^-alpha with alpha ~ U[0.5, 2] over the whole spectrum,
+    j = 1 .. min(m, n) (r_max, when given, cuts it shorter)."""
     rng = np.random.default_rng(seed)
     out = []
     for i in range(count):
@@ -109,15 +109,17 @@ def batch_shapes(count, seed=0, r_max=256):
         n = int(rng.integers(256, 4097))
         k = int(rng.choice([8, 16, 32, 64]))
         alpha = float(rng.uniform(0.5, 2.0))
-        r = min(m, n, r_max)
+        r = min(m, n) if r_max is None else min(m, n, r_max)
         out.append({"m": m, "n": n, "k": k, "p": k // 2, "N": 8, "alpha": alpha,
                     "sigma": np.arange(1, r + 1, dtype=np.float64) ** -alpha, "seed": int(seed) * 100003 + i})
     return out
 
 
-def large_shape(seed=0, r_max=256):
-    """The large served request: m = 65536, n = 8192, k = 128, p = 32, N = 16."""
+def large_shape(seed=0, r_max=None):
+    """The large served request: m = 65536, n = 8192, k = 128, p = 32, N = 16, sigma_j = j^-alpha
+    over the whole spectrum (j = 1 .. 8192; r_max, when given, cuts it shorter)."""
     rng = np.random.default_rng(seed)
     alpha = float(rng.uniform(0.5, 2.0))
+    r = 8192 if r_max is None else min(8192, r_max)
     return {"m": 65536, "n": 8192, "k": 128, "p": 32, "N": 16, "alpha": alpha,
-            "sigma": np.arange(1, r_max + 1, dtype=np.float64) ** -alpha, "seed": int(seed) * 100003 + 99991}
+            "sigma": np.arange(1, r + 1, dtype=np.float64) ** -alpha, "seed": int(seed) * 100003 + 99991}

@@ -176,10 +176,11 @@ def _gramian_bs(qs, l):
     return bs, bc
 
 
-def integrate_rb_gramian_kn(qs, l, N, maxit=256, tol=1e-4):
+def integrate_rb_gramian_kn(qs, l, N, maxit=256, tol=1e-4, history=None):
     """Row-block Gramian Kolmogorov-Nagumo integrator (iterates on Bs only).
 
     include/mcnla/isvd/integrator/row_block_gramian_kolmogorov_nagumo_integrator.hpp:112-226.
+    history: an optional list that receives the stopping quantity ||s - 1||_2 of every iteration.
     """
     L = qs.shape[1]
     bs, bc = _gramian_bs(qs, l)                             # :112-125
@@ -200,6 +201,8 @@ def integrate_rb_gramian_kn(qs, l, N, maxit=256, tol=1e-4):
         ff = ff_new
         bc = bc @ fc + bgc @ cinv                           # :203-204
         converged = _nrm2_converged(s - 1.0, tol)           # :207-214
+        if history is not None:
+            history.append(float(np.linalg.norm(s - 1.0)))
         it += 1
     qbar = qs[:, :l] @ ff + qs @ ee                         # :225-226
     return qbar, it

@@ -20,6 +20,8 @@
 
 #include <limits>
 #include <cstring>
+#include <functional>
+#include <memory>
 #include <mcnla/isvd.hpp>
 
 extern "C" void openblas_set_num_threads(int);
@@ -183,5 +185,118 @@ int mref_form(const Val* A, int a_colmajor, int m, int n, const Val* Qbar, int k
   }
   return 0;
 }
+
+
+// ---- a whole solve held between calls, the way the reference's drivers run it
+// (src/isvd_dense_rb.cpp:118-221, src/isvd_dense_cb.cpp): Parameters, the four
+// stages constructed and initialize()d once, A and Omega loaded into the
+// reference's own matrices once (the drivers read A from a file before
+// timing), then each mref_solver_run executes sketch -> orthogonalize ->
+// integrate -> form and reports every stage's own time() (the drivers' and
+// report/'s StageWrapper timers).  The sketch is the sketcher's projection
+// GEMM with the explicit Omega (gaussian_projection_sketcher.hpp:96), timed
+// around that GEMM alone.
+//   integrator: as mref_integrate; former: as mref_form (3 needs a_colmajor);
+//   row_block: RowBlockGramianOrthogonalizer instead of GramianOrthogonalizer.
+struct MrefSolver {
+  Params params;
+  int colmajor = 0, kind = 0, fkind = 0, k = 0;
+  mcnla::matrix::DenseMatrixRowMajor<Val> arm, om;
+  mcnla::matrix::DenseMatrixColMajor<Val> acm;
+  mcnla::matrix::DenseMatrixCollectionColBlockRowMajor<Val> q;
+  mcnla::matrix::DenseMatrixRowMajor<Val> qbar;
+  std::function<double()> orth, form;
+  std::function<double(int*)> integ;
+  std::function<void(Val*, Val*, Val*)> result;
+  explicit MrefSolver(Params p) : params(std::move(p)) {}
+};
+
+void* mref_solver_create(const Val* A, int a_colmajor, int m, int n, int k, int p, int N, int row_block, int kind,
+                         int fkind, int maxit, double tol, const Val* omega) {
+  auto* s = new MrefSolver(make_params(m, n, k, p, N));
+  s->colmajor = a_colmajor; s->kind = kind; s->fkind = fkind; s->k = k;
+  const int L = (k + p) * N;
+  if (a_colmajor) { s->acm.reconstruct(m, n); load_colmajor(s->acm, A, m, n); }
+  else { s->arm.reconstruct(m, n); load_rowmajor(s->arm, A, m, n); }
+  s->om.reconstruct(n, L);
+  load_rowmajor(s->om, omega, n, L);
+  s->q = kind == 0 ? s->params.createCollectionQ() : s->params.createCollectionQj();
+  s->qbar = kind == 0 ? s->params.createMatrixQbar() : s->params.createMatrixQbarj();
+  Params& prm = s->params;
+  if (row_block) {
+    auto o = std::make_shared<mcnla::isvd::RowBlockGramianOrthogonalizer<Val>>(prm);
+    o->initialize();
+    s->orth = [s, o] { (*o)(s->q); return o->time(); };
+  } else {
+    auto o = std::make_shared<mcnla::isvd::GramianOrthogonalizer<Val>>(prm);
+    o->initialize();
+    s->orth = [s, o] { (*o)(s->q); return o->time(); };
+  }
+  auto set_integ = [&](auto o) {
+    o->initialize();
+    s->integ = [s, o](int* it) { (*o)(s->q, s->qbar); *it = o->iteration(); return o->time(); };
+  };
+  switch (kind) {
+    case 0: set_integ(std::make_shared<mcnla::isvd::KolmogorovNagumoIntegrator<Val>>(prm, maxit, tol)); break;
+    case 1: set_integ(std::make_shared<mcnla::isvd::RowBlockKolmogorovNagumoIntegrator<Val>>(prm, maxit, tol)); break;
+    case 2: set_integ(std::make_shared<mcnla::isvd::RowBlockGramianKolmogorovNagumoIntegrator<Val>>(prm, maxit, tol)); break;
+    case 3: set_integ(std::make_shared<mcnla::isvd::RowBlockWenYinIntegrator<Val>>(prm, maxit, tol)); break;
+    case 4: set_integ(std::make_shared<mcnla::isvd::RowBlockGramianWenYinIntegrator<Val>>(prm, maxit, tol)); break;
+    default: delete s; return nullptr;
+  }
+  // U and V read from matrixU/matrixV (plain formers) or matrixUj/matrixVj (row-block former)
+  auto uv = [s](const auto& u, const auto& v, Val* U, Val* V) {
+    store_rowmajor(u, U, s->params.nrow(), s->k);
+    store_rowmajor(v, V, s->params.ncol(), s->k);
+  };
+  auto set_form = [&](auto f, auto& a, auto store) {
+    f->initialize();
+    s->form = [s, f, &a] { (*f)(a, s->qbar); return f->time(); };
+    s->result = [s, f, store](Val* S, Val* U, Val* V) {
+      const auto& sv = f->vectorS();
+      for (int i = 0; i < s->k; ++i) S[i] = sv(i);
+      store(*f, U, V);
+    };
+  };
+  auto plain = [uv](const auto& f, Val* U, Val* V) { uv(f.matrixU(), f.matrixV(), U, V); };
+  auto rowblk = [uv](const auto& f, Val* U, Val* V) { uv(f.matrixUj(), f.matrixVj(), U, V); };
+  auto colblk = [uv](const auto& f, Val* U, Val* V) { uv(f.matrixU(), f.matrixVj(), U, V); };
+  if (a_colmajor) {
+    if (fkind == 0) set_form(std::make_shared<mcnla::isvd::SvdFormer<Val, true>>(prm), s->acm, plain);
+    else if (fkind == 1) set_form(std::make_shared<mcnla::isvd::GramianFormer<Val, true>>(prm), s->acm, plain);
+    else if (fkind == 3) set_form(std::make_shared<mcnla::isvd::ColBlockGramianFormer<Val, true>>(prm), s->acm, colblk);
+    else { delete s; return nullptr; }
+  } else {
+    if (fkind == 0) set_form(std::make_shared<mcnla::isvd::SvdFormer<Val, true>>(prm), s->arm, plain);
+    else if (fkind == 1) set_form(std::make_shared<mcnla::isvd::GramianFormer<Val, true>>(prm), s->arm, plain);
+    else if (fkind == 2) set_form(std::make_shared<mcnla::isvd::RowBlockGramianFormer<Val, true>>(prm), s->arm, rowblk);
+    else { delete s; return nullptr; }
+  }
+  return s;
+}
+
+// t[0..3]: sketch, orthogonalize, integrate, form seconds (each stage's own timer).
+int mref_solver_run(void* h, double* t, int* iters) {
+  auto* s = static_cast<MrefSolver*>(h);
+  if (!s) return -1;
+  auto qu = s->q.unfold();
+  double t0 = mcnla::utility::getTime();
+  if (s->colmajor) mcnla::la::mm(s->acm, s->om, qu);
+  else mcnla::la::mm(s->arm, s->om, qu);
+  t[0] = mcnla::utility::getTime() - t0;
+  t[1] = s->orth();
+  t[2] = s->integ(iters);
+  t[3] = s->form();
+  return 0;
+}
+
+int mref_solver_result(void* h, Val* S, Val* U, Val* V) {
+  auto* s = static_cast<MrefSolver*>(h);
+  if (!s) return -1;
+  s->result(S, U, V);
+  return 0;
+}
+
+void mref_solver_destroy(void* h) { delete static_cast<MrefSolver*>(h); }
 
 }  // extern "C"

@@ -30,6 +30,13 @@ def load():
                                    ctypes.c_double, _D, _I, _D]
     lib.mref_form.argtypes = [_D, ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, ctypes.c_int, ctypes.c_int,
                               ctypes.c_int, _D, _D, _D, _D]
+    lib.mref_solver_create.restype = ctypes.c_void_p
+    lib.mref_solver_create.argtypes = [_D, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_double, _D]
+    lib.mref_solver_run.argtypes = [ctypes.c_void_p, _D, _I]
+    lib.mref_solver_result.argtypes = [ctypes.c_void_p, _D, _D, _D]
+    lib.mref_solver_destroy.argtypes = [ctypes.c_void_p]
     lib.mref_set_threads.argtypes = [ctypes.c_int]
     lib.mref_get_threads.restype = ctypes.c_int
     return lib
@@ -59,9 +66,10 @@ def sketch(lib, a, omega, colmajor=False):
     return y, t[0]
 
 
-def orthogonalize(lib, y, l, N, row_block=False, timing=False):
-    """timing=True also returns [time(), parts...]."""
-    q = _c(y).copy()
+def orthogonalize(lib, y, l, N, row_block=False, timing=False, inplace=False):
+    """timing=True also returns [time(), parts...].  inplace=True orthogonalizes y
+    itself (a C-contiguous float64 array) instead of a copy."""
+    q = y if inplace and y.flags.c_contiguous and y.dtype == np.float64 else _c(y).copy()
     m = q.shape[0]
     t = _times()
     lib.mref_orthogonalize(_p(q), m, l, N, int(row_block), _p(t))
@@ -90,3 +98,40 @@ def form(lib, a, qbar, k, p, kind, colmajor=False, timing=False):
     rc = lib.mref_form(_p(ab), int(colmajor or kind == 3), m, n, _p(qb), k, p, kind, _p(s), _p(u), _p(v), _p(t))
     assert rc == 0
     return (s, u, v, t) if timing else (s, u, v)
+
+
+class Solver:
+    """A whole reference solve held between runs (mref_solver_*): A and Omega are loaded into
+    the reference's own matrices and the four stages constructed and initialized once, as the
+    reference's drivers do before they time anything; run() executes sketch -> orthogonalize ->
+    integrate -> form and returns (iterations, [sketch, orthogonalize, integrate, form] seconds
+    from the stages' own timers).  kind / fkind: as integrate() / form()."""
+
+    def __init__(self, lib, a, omega, k, p, N, kind, fkind, maxit, tol, colmajor=False, row_block=True):
+        m, n = a.shape
+        self.lib, self.k, self.m, self.n = lib, k, m, n
+        ab = _c(a.T if colmajor else a)
+        om = _c(omega)
+        self.h = lib.mref_solver_create(_p(ab), int(colmajor), m, n, k, p, N, int(row_block), kind, fkind, maxit,
+                                        tol, _p(om))
+        if not self.h:
+            raise ValueError("unsupported integrator / former / layout combination")
+
+    def run(self):
+        t = np.zeros(4)
+        it = ctypes.c_int()
+        assert self.lib.mref_solver_run(self.h, _p(t), ctypes.byref(it)) == 0
+        return it.value, t
+
+    def result(self):
+        s, u, v = np.empty(self.k), np.empty((self.m, self.k)), np.empty((self.n, self.k))
+        assert self.lib.mref_solver_result(self.h, _p(s), _p(u), _p(v)) == 0
+        return s, u, v
+
+    def close(self):
+        if self.h:
+            self.lib.mref_solver_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()

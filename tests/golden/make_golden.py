@@ -26,6 +26,7 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 
 def read_mtx_array(path):
@@ -54,7 +55,10 @@ def read_mtx_array(path):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    from oracle.refpath import reference_root
+    ref = sys.argv[1] if len(sys.argv) > 1 else reference_root()
+    if not ref:
+        sys.exit("the reference checkout was not found: pass its path or set MCNLA_REFERENCE")
     data = os.path.join(ref, "data")
     out = {}
     for name in ["a", "q", "u", "yi", "qi", "qb_kn", "qb_wy"]:

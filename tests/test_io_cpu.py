@@ -8,7 +8,10 @@ import pytest
 
 from mcnla_b200 import _lib, io
 
-REF_DATA = "/root/reference/data"
+from oracle.refpath import reference_root
+
+_REF = reference_root()
+REF_DATA = os.path.join(_REF, "data") if _REF else None
 
 
 def test_matrix_market_round_trip_and_blocks(tmp_path):
@@ -47,7 +50,7 @@ def test_matrix_market_collection(tmp_path):
     assert np.array_equal(io.load_matrix_market(p), unfolded)
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_DATA), reason="the reference's data directory is not here")
+@pytest.mark.skipif(not REF_DATA or not os.path.isdir(REF_DATA), reason="the reference's data directory is not here")
 def test_reference_fixtures_parse_like_the_golden_conversion():
     golden = np.load(os.path.join(os.path.dirname(__file__), "golden", "mcnla_data.npz"))
     a = io.load_matrix_market(os.path.join(REF_DATA, "a.mtx"))

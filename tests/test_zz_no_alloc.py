@@ -78,3 +78,66 @@ def test_noalloc_rejects_partials_beyond_the_scratch():
     assert b"static scratch" in lib.mcnla_b200_last_error()
     torch.cuda.synchronize()
     assert torch.equal(c, before)
+
+
+def test_noalloc_leaves_device_free_memory_unchanged():
+    """The property the entry point exists for: after the first call (which may load the
+    library's module), a call takes no device memory, and neither does a second one."""
+    from mcnla_b200 import _lib
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    lib = _lib.load()
+    stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    M, N, K = 128, 128, 60000      # split-K: the partial sums go to the static scratch
+    a, b, c = _operands(M, N, K, False, False, dev, 11)
+
+    def call():
+        _lib.check(lib.mcnla_b200_dgemm_noalloc(stream, M, N, K, 1.0, _p(a), K, 1, _p(b), N, 1, 0.0, _p(c), N, 1),
+                   "dgemm_noalloc")
+        torch.cuda.synchronize()
+
+    call()
+    free0, _ = torch.cuda.mem_get_info(dev)
+    call()
+    free1, _ = torch.cuda.mem_get_info(dev)
+    call()
+    free2, _ = torch.cuda.mem_get_info(dev)
+    assert free0 == free1 == free2, (free0, free1, free2)
+    assert (c - a @ b).abs().max().item() <= 1e-14 * (a.abs() @ b.abs()).max().item() * K ** 0.5
+
+
+_FRESH = r"""
+import ctypes, sys, torch
+sys.path.insert(0, sys.argv[1])
+from mcnla_b200 import _lib
+lib = _lib.load()
+dev = torch.device("cuda", 0)
+g = torch.Generator(device=dev).manual_seed(5)
+M, N, K = 96, 80, 50000
+a = torch.randn(M, K, generator=g, dtype=torch.float64, device=dev)
+b = torch.randn(K, N, generator=g, dtype=torch.float64, device=dev)
+c = torch.empty(M, N, dtype=torch.float64, device=dev)
+torch.cuda.synchronize()
+P = lambda t: ctypes.c_void_p(t.data_ptr())
+for call in range(2):
+    c.zero_()
+    torch.cuda.synchronize()
+    st = lib.mcnla_b200_dgemm_noalloc(None, M, N, K, 1.0, P(a), K, 1, P(b), N, 1, 0.0, P(c), N, 1)
+    assert st == 0, (st, lib.mcnla_b200_last_error())
+    torch.cuda.synchronize()
+    tol = 1e-14 * (a.abs() @ b.abs()).max().item() * K ** 0.5
+    err = (c - a @ b).abs().max().item()
+    assert err <= tol, (call, err, tol)
+print("fresh ok")
+"""
+
+
+def test_noalloc_first_call_in_a_fresh_process_on_the_null_stream():
+    """The documented use: a caller that never creates a library context makes its first call
+    on a device with the NULL (default) stream; checked against torch's a @ b."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", _FRESH, root], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and "fresh ok" in r.stdout, r.stdout[-2000:] + r.stderr[-2000:]
