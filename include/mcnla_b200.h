@@ -351,6 +351,49 @@ MCNLA_B200_API int mcnla_b200_server_destroy(mcnla_b200_server* server);
 MCNLA_B200_API int mcnla_b200_isvd_batched(int device, mcnla_b200_problem* problems, int count, int workers,
                                            int64_t budget_bytes);
 
+/* ---- row-block decomposition over several GPUs -------------------------------
+ * The reference's MPI decomposition of one solve (src/isvd_dense_rb.cpp:118-221
+ * with the row-block stages): every rank holds a block of rows of A, sketches
+ * them with the same Omega, and keeps its rows of Q, Qbar and U; the stages
+ * sum their row-dependent partial products over the ranks where the
+ * reference calls MPI:
+ *   orthogonalizer  W_i = sum_r Y_ir' Y_ir  (row_block_gramian_orthogonalizer.hpp:86)
+ *   integrators     row-block KN: Bc once and Bgc per iteration
+ *                   (row_block_kolmogorov_nagumo_integrator.hpp:115, :143);
+ *                   Gramian KN / WY: Bs once (row_block_gramian_kolmogorov_
+ *                   nagumo_integrator.hpp:117, row_block_gramian_wen_yin_
+ *                   integrator.hpp:126); row-block WY: Bc, Bgc and per
+ *                   iteration Bgc and the three step-size inner products
+ *                   (row_block_wen_yin_integrator.hpp:117, :129, :229, :269);
+ *                   plain KN: B = Qs' Qc and Z = X' X per iteration (the
+ *                   reference distributes that integrator over sketches
+ *                   instead, kolmogorov_nagumo_integrator.hpp:109-136)
+ *   formers         Z = A' Qbar (Gramian) or Q' A (SVD former): the reference
+ *                   reduce-scatters Z over column blocks and all-reduces W
+ *                   (row_block_gramian_former.hpp:111, :121); here every rank
+ *                   receives all of Z and returns all of V
+ * Once a context has a communicator, every stage and whole-solve entry point
+ * above runs on the rank's rows: params->nrow is the number of LOCAL rows,
+ * A, Q, Qbar and U are the rank's row blocks, and S, V (and the iteration
+ * count) come out the same on every rank.  All ranks must call the same
+ * entry points with the same parameters (apart from nrow) in the same order.
+ * The iteration loops run without CUDA-graph replay on such a context.
+ *
+ * mcnla_b200_allreduce_fn: sum `count` doubles at the DEVICE pointer buf over
+ * the ranks, in place, ordered on `stream` (a cudaStream_t) like a kernel
+ * launched there; return 0 on success.  NULL fn detaches.                    */
+typedef int (*mcnla_b200_allreduce_fn)(void* user, double* buf, int64_t count, void* stream);
+MCNLA_B200_API int mcnla_b200_set_allreduce(mcnla_b200_ctx* ctx, mcnla_b200_allreduce_fn fn, void* user);
+/* The library's own NCCL communicator (NCCL over NVLink / NVSwitch; libnccl.so.2
+ * is loaded on first use).  mcnla_b200_nccl_unique_id writes the 128-byte id
+ * that rank 0 creates and every rank then passes to mcnla_b200_set_nccl, with
+ * the context's device current (one GPU per rank).                           */
+#define MCNLA_B200_NCCL_ID_BYTES 128
+MCNLA_B200_API int mcnla_b200_nccl_unique_id(unsigned char* id);
+MCNLA_B200_API int mcnla_b200_set_nccl(mcnla_b200_ctx* ctx, const unsigned char* id, int nranks, int rank);
+/* Number of all-reduces this context has issued. */
+MCNLA_B200_API int64_t mcnla_b200_allreduces(const mcnla_b200_ctx* ctx);
+
 /* ---- building blocks (exposed for tests) ----------------------------------
  * FP64 GEMM C := alpha*A*B + beta*C on strided device matrices (element (i,j)
  * of X at X[i*x_rs + j*x_cs]); the reference's la::mm

@@ -70,8 +70,16 @@ _I64 = ctypes.c_int64
 _D = ctypes.c_double
 _INT = ctypes.c_int
 
+# mcnla_b200_allreduce_fn: int (*)(void* user, double* buf, int64_t count, void* stream)
+ALLREDUCE_FN = ctypes.CFUNCTYPE(_INT, _P, _P, _I64, _P)
+NCCL_ID_BYTES = 128
+
 # name -> (restype, argtypes), one line per entry point of the header
 SIGNATURES = {
+    "mcnla_b200_set_allreduce": (_INT, [_P, ALLREDUCE_FN, _P]),
+    "mcnla_b200_nccl_unique_id": (_INT, [_P]),
+    "mcnla_b200_set_nccl": (_INT, [_P, _P, _INT, _INT]),
+    "mcnla_b200_allreduces": (_I64, [_P]),
     "mcnla_b200_create": (_INT, [ctypes.POINTER(_P), _INT, _P]),
     "mcnla_b200_destroy": (_INT, [_P]),
     "mcnla_b200_set_stream": (_INT, [_P, _P]),

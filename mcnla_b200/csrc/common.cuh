@@ -98,6 +98,17 @@ struct Context {
   bool graph_loop = true;
   // precision form: the Gramian integrators form Bs = Qs' Qs from BF16 parts of Qs
   bool mixed_gramian = false;
+  // row-block decomposition over several GPUs: the stages sum their row-dependent
+  // partial products over the ranks at the reference's MPI reduction points, through a
+  // caller-supplied all-reduce or the library's own NCCL communicator (comm.cu)
+  mcnla_b200_allreduce_fn allreduce_fn = nullptr;
+  void* allreduce_user = nullptr;
+  void* nccl_comm = nullptr;
+  int comm_size = 1;
+  int comm_rank = 0;
+  int64_t allreduces = 0;
+  double* comm_tmp = nullptr;     // contiguous staging of strided blocks for the all-reduce
+  size_t comm_tmp_bytes = 0;
   DevScalars* scal = nullptr;       // device scalars
   DevScalars* scal_host = nullptr;  // pinned mirror
   // stage part timers (CUDA events), filled by the last stage call
@@ -132,6 +143,19 @@ int ctx_toc(Context* c);
 int ctx_collect_times(Context* c);
 
 int ctx_sync_scalars(Context* c);   // copies DevScalars to the pinned mirror and waits
+
+// Sums `count` doubles at the device pointer buf over the ranks of the context's
+// row-block decomposition, in place, ordered on the context's stream (comm.cu).  A
+// no-op without one.  Every rank must make the same calls in the same order.
+int ctx_allreduce(Context* c, double* buf, int64_t count);
+inline bool ctx_distributed(const Context* c) { return c->allreduce_fn != nullptr || c->nccl_comm != nullptr; }
+// The same for a rows x cols block with row stride ld (staged through a
+// contiguous buffer of the context when ld != cols).
+int ctx_allreduce2d(Context* c, double* p, int64_t ld, int64_t rows, int64_t cols);
+// Sum over the ranks of a host value (1 without a communicator: the value itself).
+int ctx_sum_host(Context* c, double v, double* out);
+// Frees the communicator and the staging buffer (mcnla_b200_destroy).
+void ctx_release_comm(Context* c);
 
 inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 

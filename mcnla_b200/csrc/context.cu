@@ -155,6 +155,8 @@ int mcnla_b200_destroy(mcnla_b200_ctx* c) {
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
   if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);   // copies land in the arenas freed below
+  mb::ctx_release_comm(c);
+  cudaStreamSynchronize(c->stream);
   for (auto ev : c->events) cudaEventDestroy(ev);
   if (c->arena) cudaFree(c->arena);
   if (c->parena) cudaFree(c->parena);

@@ -124,6 +124,7 @@ int run_orthogonalize(Context* c, const Dims& d, double* Q) {
   MB_CHECK(ctx_tic(c));
   // W_i := Q_i' Q_i   (:84-86)
   MB_CHECK(dgemm(c, l, l, m, 1.0, cm(Q, 1, L), cm(Q, L, 1), 0.0, drow(W, l), GemmBatch{N, l, l, int64_t(ll)}, ws));
+  MB_CHECK(ctx_allreduce(c, W, int64_t(ll) * N));   // row blocks over ranks (row_block_gramian_orthogonalizer.hpp:86)
   // eig(W_i) = V_i S_i V_i', descending (gesvd<'N','O'> of an SPD matrix, :89-91)
   MB_CHECK(launch_syev(c, l, N, W, l, int64_t(ll), S, V, 1));
   // T_i := V_i diag(S_i)^(-1/2)   (:94-99)
@@ -207,7 +208,7 @@ int kn_loop(Context* c, int maxit, Body body, int* iters) {
   const int chunk = 8;   // even: every chunk starts on the same buffer parity
   int launched = 0, done = -1;
   LoopGraph graph;
-  bool use_graph = c->graph_loop;
+  bool use_graph = c->graph_loop && !ctx_distributed(c);   // a caller's all-reduce may not be capturable
   int64_t graph_kernels = 0;
   while (launched < maxit) {
     const int end = std::min(maxit, launched + chunk);
@@ -272,6 +273,7 @@ int run_kn(Context* c, const Dims& d, const double* Qs, int maxit, double tol, d
     double* X = QX[cur] + l;
     // B := Qs' Qc   (:117)
     MB_CHECK(dgemm(c, L, l, m, 1.0, cm(Qs, 1, L), crow(Qc, lq), 0.0, drow(B, l), GemmBatch(), ws));
+    MB_CHECK(ctx_allreduce(c, B, L * l));   // row blocks over ranks
     // D := B' B   (:123)
     MB_CHECK(dgemm(c, l, l, L, 1.0, cm(B, 1, l), crow(B, l), 0.0, drow(D, l), GemmBatch(), ws));
     // X := Qs B / N;  X -= Qc D / N   (:126-129)
@@ -279,6 +281,7 @@ int run_kn(Context* c, const Dims& d, const double* Qs, int maxit, double tol, d
     MB_CHECK(dgemm(c, m, l, l, -inv_n, crow(Qc, lq), crow(D, l), 1.0, drow(X, lq), GemmBatch(), ws));
     // Z := X' X   (:143)
     MB_CHECK(dgemm(c, l, l, m, 1.0, cm(X, 1, lq), crow(X, lq), 0.0, drow(Z, l), GemmBatch(), ws));
+    MB_CHECK(ctx_allreduce(c, Z, int64_t(l) * l));
     // eig(Z); C, inv(C); convergence test   (:146-164, :174-181)
     MB_CHECK(launch_kn_step(c, l, Z, nullptr, inv_n, CC, nullptr, nullptr, nullptr, vwork, tol));
     // Qc := Qc C + X inv(C) = [Qc X] [C; inv(C)]   (:170-171)
@@ -314,6 +317,7 @@ int run_rb_kn(Context* c, const Dims& d, const double* Qs, int maxit, double tol
   // Qc := Q0; Bc := Qs' Qc   (:110-113)
   MB_CHECK(copy2d(c, QG[0], l2, Qs, L, m, l));
   MB_CHECK(dgemm(c, L, l, m, 1.0, cm(Qs, 1, L), crow(QG[0], l2), 0.0, drow(BB[0], l2), GemmBatch(), ws));
+  MB_CHECK(ctx_allreduce2d(c, BB[0], l2, L, l));   // (:115)
   MB_CHECK(ctx_toc(c));
   int it = 0;
   MB_CHECK(kn_loop(c, maxit, [&](int i) -> int {
@@ -322,6 +326,7 @@ int run_rb_kn(Context* c, const Dims& d, const double* Qs, int maxit, double tol
     MB_CHECK(dgemm(c, m, l, L, inv_n, crow(Qs, L), crow(BB[cur], l2), 0.0, drow(QG[cur] + l, l2), GemmBatch(), ws));
     // Bgc := Qs' Gc   (:141)
     MB_CHECK(dgemm(c, L, l, m, 1.0, cm(Qs, 1, L), crow(QG[cur] + l, l2), 0.0, drow(BB[cur] + l, l2), GemmBatch(), ws));
+    MB_CHECK(ctx_allreduce2d(c, BB[cur] + l, l2, L, l));   // (:143)
     // [Dc | Dgc] := 1/N Bc' [Bc | Bgc]   (:147-150)
     MB_CHECK(dgemm(c, l, l2, L, inv_n, cm(BB[cur], 1, l2), crow(BB[cur], l2), 0.0, drow(DD, l2), GemmBatch(), ws));
     // Z := Dgc - Dc^2; eig; C, inv(C); Fc := C - Dc inv(C); convergence test   (:156-201)
@@ -366,6 +371,9 @@ int gramian_bs(Context* c, const Dims& d, const double* Qs, double* Bs, double* 
   if (c->mixed_gramian) MB_CHECK(gramian_bs_bf16(c, d, Qs, Bs, x));
   else MB_CHECK(dgemm(c, d.L, d.L, d.m, 1.0, cm(Qs, 1, d.L), crow(Qs, d.L), 0.0, drow(Bs, d.L), GemmBatch(), ws, 0,
                       true));
+  // row blocks over ranks (row_block_gramian_kolmogorov_nagumo_integrator.hpp:117,
+  // row_block_gramian_wen_yin_integrator.hpp:126): the lower triangles are summed
+  MB_CHECK(ctx_allreduce(c, Bs, d.L * d.L));
   MB_CHECK(launch_gramian_prepare(c, d.L, d.l, Bs, Bc, ldbc));
   return MCNLA_B200_OK;
 }
@@ -538,8 +546,10 @@ int run_rb_wy(Context* c, const Dims& d, const double* Qs, int maxit, double tol
   // Initializing (:112-143)
   MB_CHECK(copy2d(c, QG[0], l2, Qs, L, m, l));                                                        // Qc := Q0
   MB_CHECK(dgemm(c, L, l, m, 1.0, cm(Qs, 1, L), crow(QG[0], l2), 0.0, drow(BB[0], l2), GemmBatch(), ws));  // Bc
+  MB_CHECK(ctx_allreduce2d(c, BB[0], l2, L, l));   // (:117)
   MB_CHECK(dgemm(c, m, l, L, inv_n, crow(Qs, L), crow(BB[0], l2), 0.0, drow(QG[0] + l, l2), GemmBatch(), ws));  // Gc
   MB_CHECK(dgemm(c, L, l, m, 1.0, cm(Qs, 1, L), crow(QG[0] + l, l2), 0.0, drow(BB[0] + l, l2), GemmBatch(), ws));  // Bgc
+  MB_CHECK(ctx_allreduce2d(c, BB[0] + l, l2, L, l));   // (:129)
   MB_CHECK(dgemm(c, l, l2, L, inv_n, cm(BB[0], 1, l2), crow(BB[0], l2), 0.0, drow(DD, l2), GemmBatch(), ws));  // Dc|Dgc
   // Xc := Gc - Qc Dc
   MB_CHECK(copy2d(c, X[0], l, QG[0] + l, l2, m, l));
@@ -566,6 +576,7 @@ int run_rb_wy(Context* c, const Dims& d, const double* Qs, int maxit, double tol
     // G+ := 1/N Qs B+; Bg+ := Qs' G+; [D+ | Dg+] := 1/N B+' [B+ | Bg+]   (:224-236)
     MB_CHECK(dgemm(c, m, l, L, inv_n, crow(Qs, L), crow(BB[nx], l2), 0.0, drow(QG[nx] + l, l2), GemmBatch(), ws));
     MB_CHECK(dgemm(c, L, l, m, 1.0, cm(Qs, 1, L), crow(QG[nx] + l, l2), 0.0, drow(BB[nx] + l, l2), GemmBatch(), ws));
+    MB_CHECK(ctx_allreduce2d(c, BB[nx] + l, l2, L, l));   // (:229)
     MB_CHECK(dgemm(c, l, l2, L, inv_n, cm(BB[nx], 1, l2), crow(BB[nx], l2), 0.0, drow(DD, l2), GemmBatch(), ws));
     // mu := tr(Dg+) - ||D+||_F^2   (:240)
     MB_CHECK(launch_wy_mu(c, l, DD, &c->scal->mu));
@@ -581,6 +592,7 @@ int run_rb_wy(Context* c, const Dims& d, const double* Qs, int maxit, double tol
     MB_CHECK(dgemm(c, m, l, l, -1.0, crow(QG[nx], l2), crow(DD, l2), 1.0, drow(X[nx], l), GemmBatch(), ws));
     // Delta1 := Qc - Q+, Delta2 := Xc - X+ and their inner products   (:261-274)
     MB_CHECK(launch_wy_delta_dots(c, QG[cur], QG[nx], l2, X[cur], X[nx], l, m, l, partials, &c->scal->dot[0]));
+    MB_CHECK(ctx_allreduce(c, &c->scal->dot[0], 3));   // (:269)
     MB_CHECK(ctx_sync_scalars(c));
     const double d11 = c->scal_host->dot[0], d12 = c->scal_host->dot[1], d22 = c->scal_host->dot[2];
     const double t1 = is_odd ? d11 : d12, t2 = is_odd ? d12 : d22;
@@ -813,6 +825,7 @@ int run_form_svd(Context* c, const Dims& d, const CMat& Am, const double* Qbar, 
   // Vt := Q' A   (:99)
   if (at) MB_CHECK(form_product_bf16(c, d, *at, Qbar, Vt, n, false, q16, slices));
   else MB_CHECK(dgemm(c, l, n, m, 1.0, cm(Qbar, 1, l), Am, 0.0, drow(Vt, n), GemmBatch(), ws));
+  MB_CHECK(ctx_allreduce(c, Vt, int64_t(l) * n));   // row blocks over ranks
   MB_CHECK(ctx_toc(c));
   // svd(Vt)   (:106)
   const double* Yin = Vt;
@@ -865,6 +878,7 @@ int run_form_gramian(Context* c, const Dims& d, const CMat& Am, const double* Qb
   // Z := A' Q   (gramian_former.hpp:101)
   if (at) MB_CHECK(form_product_bf16(c, d, *at, Qbar, Z, l, true, q16, slices));
   else MB_CHECK(dgemm(c, n, l, m, 1.0, ctr(Am), crow(Qbar, l), 0.0, drow(Z, l), GemmBatch(), ws));
+  MB_CHECK(ctx_allreduce(c, Z, n * l));   // row blocks over ranks (row_block_gramian_former.hpp:111)
   MB_CHECK(ctx_toc(c));
   // W := Z' Z; eig(W) = W S W' (descending); S := sqrt(S)   (:108-115)
   MB_CHECK(dgemm(c, l, l, n, 1.0, cm(Z, 1, l), crow(Z, l), 0.0, drow(W, l), GemmBatch(), ws));
@@ -999,7 +1013,9 @@ int run_isvd_mixed(Context* c, const Dims& d, int integrator, int former, const 
   // re-orthonormalization the BF16 form needs afterwards.
   const bool gramian = integrator == MCNLA_B200_ROW_BLOCK_GRAMIAN_KOLMOGOROV_NAGUMO ||
                        integrator == MCNLA_B200_ROW_BLOCK_GRAMIAN_WEN_YIN;
-  const bool bf16_gramian = gramian && double(d.L) * double(d.L) * double(d.m) >= kMixedGramianMinFlops;
+  double m_all = 0.0;   // the rows of all ranks: every rank takes the same path
+  MB_CHECK(ctx_sum_host(c, double(d.m), &m_all));
+  const bool bf16_gramian = gramian && double(d.L) * double(d.L) * m_all >= kMixedGramianMinFlops;
   {
     struct Mixed { Context* c; Mixed(Context* x, bool on) : c(x) { c->mixed_gramian = on; }
                    ~Mixed() { c->mixed_gramian = false; } } mixed(c, bf16_gramian);
