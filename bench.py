@@ -60,12 +60,13 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-row-block", action="store_true", help="N > 1: skip the row-block (one matrix over all ranks) leg")
     ap.add_argument("--cpu-rows", type=int, default=0, help="row sample of the CPU baseline (0: auto)")
     ap.add_argument("--ref-budget", type=float, default=1200.0,
                     help="reference arm: seconds of timed full solves; no step starts that would end past it")
     ap.add_argument("--quick", action="store_true", help="small shape for a smoke run")
     ap.add_argument("--no-serving", action="store_true", help="skip the batched / served leg")
-    ap.add_argument("--kernel", choices=["sketch_bf16", "gkn", "trace"], default=None,
+    ap.add_argument("--kernel", choices=["sketch_bf16", "gkn", "trace", "grouped"], default=None,
                     help="time one kernel alone (profiling case) instead of the benchmark: the BF16 sketch GEMM "
                          "on --m x --n x (--k + --p) --N with --parts parts, or the persistent row-block Gramian "
                          "KN integrator on the sketches of a seeded --m x --n matrix (sigma_j = 1/j, tol 1e-5); "
@@ -308,6 +309,48 @@ def run_config1_b200(args, dev):
             "sigma": [float(x) for x in s[:3].tolist()]}
 
 
+def run_row_block_b200(args, world, rank, local):
+    """One matrix of the workload split by rows over the ranks (the reference's row-block
+    decomposition): every rank sketches its rows with the same Omega and the stages sum their
+    partial products through the library's NCCL communicator (NVLink / NVSwitch).  K timed
+    solves, CUDA events on each rank, the max over ranks."""
+    import torch
+    from mcnla_b200 import isvd, rowblock
+    dev = torch.device("cuda", local)
+    full = workload_matrix(args, 0, device=dev)
+    r0, r1 = rowblock.row_range(args.m, world, rank)
+    a = full[r0:r1].contiguous() if not args.colmajor else full[r0:r1].t().contiguous().t()
+    del full
+    torch.cuda.empty_cache()
+    ctx = isvd.context(dev)
+    rowblock.attach_nccl(ctx, rank=rank, world=world)
+    stream = torch.cuda.current_stream(dev)
+    try:
+        def solve(seed):
+            return rowblock.solve_row_block(a, args.k, args.p, args.N, seed=seed, integrator=args.integrator,
+                                            former=args.former, maxit=args.maxit, tol=args.tol)
+        for w in range(max(1, args.warmup)):
+            solve(w)
+        torch.cuda.synchronize()
+        barrier(world)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for step in range(args.steps):
+            s, u, v, it = solve(100 + step)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = max_over_ranks(e0.elapsed_time(e1) / 1e3, world)
+        n_ar = rowblock.allreduces(ctx)
+    finally:
+        rowblock.detach(ctx)
+    del a
+    torch.cuda.empty_cache()
+    return {"value": round(args.steps / t, 5), "unit": "iSVD/s (one matrix over all ranks)",
+            "ms_per_step": round(t / args.steps * 1e3, 3), "rows_per_rank": [r1 - r0], "iterations": it,
+            "collective": "the library's NCCL communicator: all-reduce of W, Bs and Z per solve",
+            "allreduces_per_rank": int(n_ar), "scaling": "strong"}
+
+
 def run_b200(args, world, rank, local):
     import numpy as np
     import torch
@@ -518,6 +561,11 @@ def run_b200(args, world, rank, local):
 
     recon = reconstruction_error_torch(a, s, u, v)
     c1 = run_config1_b200(args, dev) if world == 1 and not args.quick else None
+    row_block = None
+    if world > 1 and not args.no_row_block:
+        del a
+        torch.cuda.empty_cache()
+        row_block = run_row_block_b200(args, world, rank, local)
     result = {
         "metric": METRIC, "value": round(value, 5), "unit": "iSVD/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(total / args.steps * 1e3, 3), "higher_is_better": True,
@@ -529,7 +577,7 @@ def run_b200(args, world, rank, local):
         "iterations": iters[-1], "stages": stages, "integrators": variants, "mixed": mixed, "roofline": roofline,
         "stage_roofline": stage_roof, "e2e": e2e,
         "gpu_launches": int(launches), "clocks": clk,
-        "reconstruction_rel_err": recon, "config1": c1,
+        "reconstruction_rel_err": recon, "config1": c1, "row_block": row_block,
     }
     return result
 
@@ -763,6 +811,25 @@ def run_kernel_case(args, dev):
     ctx = isvd.context(dev)
     if args.kernel == "trace":
         return run_trace(args, dev)
+    if args.kernel == "grouped":
+        # the grouped batch integrator on --batch-count copies of one shape (m x n, k, p = k/2, N = 8)
+        shapes = [dict(sh, k=k, p=k // 2) for sh in synthetic.batch_shapes(args.batch_count, seed=4)]
+        pool = [synthetic.lowrank_torch(m, n, np.arange(1, min(m, n) + 1) ** -1.0, seed=i, device=dev)
+                for i in range(min(8, args.batch_count))]
+        def reqs():
+            return [isvd.Request(pool[i % len(pool)], k, k // 2, 8, seed=i, integrator="rb_gramian_kn",
+                                 former="rb_gramian", maxit=args.maxit, tol=1e-5) for i in range(args.batch_count)]
+        isvd.solve_batched(reqs(), workers=args.serve_workers)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rs = isvd.solve_batched(reqs(), workers=args.serve_workers)
+        torch.cuda.synchronize()
+        t = time.perf_counter() - t0
+        its = [r.result.iteration for r in rs]
+        del shapes
+        return {"kernel": "k_gkn_grouped (grouped batch)", "m": m, "n": n, "k": k, "count": args.batch_count,
+                "s": round(t, 4), "solves_per_s": round(args.batch_count / t, 2), "iterations_mean": float(np.mean(its)),
+                "iterations_max": int(max(its))}
     if args.kernel == "sketch_bf16":
         a = torch.randn(m, n, dtype=torch.float64, device=dev)
         sp = isvd.split_bf16(a, args.parts)

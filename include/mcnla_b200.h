@@ -297,16 +297,31 @@ MCNLA_B200_API int mcnla_b200_isvd_mixed(mcnla_b200_ctx* ctx, const mcnla_b200_p
                                          double* U, double* V, int* iteration);
 
 /* ---- batched and served solves ----------------------------------------------
- * Many independent solves of uneven sizes share the GPU: a pool of workers,
- * each with its own stream and workspaces, takes problems from a FIFO queue
- * and runs them concurrently, so small problems fill the SMs together.  A
- * problem is admitted when a worker is free and the estimated device bytes of
- * the problems in flight stay within the budget (A itself is the caller's and
- * is not counted).  Every solve is deterministic, so a problem gives the same
- * result alone and in a mix.  (The reference runs one problem per MPI job;
- * this has no counterpart there.)                                            */
+ * Many independent solves of uneven sizes share the GPU.  (The reference runs
+ * one problem per MPI job; this has no counterpart there.)
+ *   mcnla_b200_isvd_batched runs a batch in waves that fit the budget.  The
+ *   problems that use the row-block Gramian Kolmogorov-Nagumo integrator with
+ *   N l <= 1536 go through three phases: a pool of workers (each with its own
+ *   stream and workspaces) sketches and orthogonalizes them and forms their
+ *   Gramians; one grouped persistent kernel then runs every problem's
+ *   iterations, one problem per CTA from a device work queue, with per-problem
+ *   iteration counts; the workers finish Qbar and the formers.  Other problems
+ *   run whole solves on the workers.
+ *   mcnla_b200_server_* keeps a worker pool for requests that arrive over
+ *   time: a request is admitted when a worker is free and the estimated device
+ *   bytes of the requests in flight stay within the budget.
+ * A itself is the caller's and is not counted.  Every solve is deterministic
+ * and a problem takes the same operations on every path, so it gives the same
+ * result alone, in a batch and in a served mix.
+ * Precisions: FP64 runs the plain path (an FP32 A is converted to FP64 on the
+ * device for the sketch and the former).  The mixed precisions run the
+ * precision form: the sketch on tcgen05 from BF16 parts of A, Omega drawn in
+ * BF16, the orthogonalizer and the integrator's small factorizations in FP64,
+ * and the former's product Q' A on tcgen05 from three BF16 parts of A'.  The
+ * parts are split from A (FP32 or FP64) per solve, or read from the caller's
+ * resident copies when a_hi / at_hi are given (mcnla_b200_split_bf16).     */
 #define MCNLA_B200_PRECISION_FP64  0   /* FP64 sketch (plain path) */
-#define MCNLA_B200_PRECISION_MIXED 1   /* BF16 hi+lo tcgen05 sketch, FP64 elsewhere */
+#define MCNLA_B200_PRECISION_MIXED 1   /* BF16 hi+lo tcgen05 sketch, precision former */
 #define MCNLA_B200_PRECISION_MIXED3 2  /* BF16 hi+lo+lo2 (24 bits: exact for FP32 A) */
 
 typedef struct mcnla_b200_problem {
@@ -325,7 +340,18 @@ typedef struct mcnla_b200_problem {
   int iteration;          /* out */
   int status;             /* out */
   double seconds;         /* out: device time of the solve */
-  double latency;         /* out: host seconds from submit to completion (server) */
+  double latency;         /* out: host seconds from submit (or the batch's start) to completion */
+  /* mixed precisions, optional: the caller's resident BF16 parts of A
+   * (row-major m x n, pitch lda16; a_lo2 for MIXED3) and of A' (n x m, pitch
+   * ldat16, three parts); NULL a_hi / at_hi: split from A per solve.          */
+  const uint16_t* a_hi;
+  const uint16_t* a_lo;
+  const uint16_t* a_lo2;
+  int64_t lda16;
+  const uint16_t* at_hi;
+  const uint16_t* at_lo;
+  const uint16_t* at_lo2;
+  int64_t ldat16;
 } mcnla_b200_problem;
 
 typedef struct mcnla_b200_server mcnla_b200_server;

@@ -50,7 +50,9 @@ class Problem(ctypes.Structure):
                 ("former", ctypes.c_int), ("max_iteration", ctypes.c_int), ("tolerance", ctypes.c_double),
                 ("precision", ctypes.c_int), ("S", ctypes.c_void_p), ("U", ctypes.c_void_p), ("V", ctypes.c_void_p),
                 ("iteration", ctypes.c_int), ("status", ctypes.c_int), ("seconds", ctypes.c_double),
-                ("latency", ctypes.c_double)]
+                ("latency", ctypes.c_double), ("a_hi", ctypes.c_void_p), ("a_lo", ctypes.c_void_p),
+                ("a_lo2", ctypes.c_void_p), ("lda16", ctypes.c_int64), ("at_hi", ctypes.c_void_p),
+                ("at_lo", ctypes.c_void_p), ("at_lo2", ctypes.c_void_p), ("ldat16", ctypes.c_int64)]
 
 
 class McnlaError(RuntimeError):

@@ -45,6 +45,9 @@ int launch_sum_splits(Context* c, const double* P, int splits, int64_t stride, i
 // (layout 0) or column-major (layout 1) FP64 A.
 int launch_split_bf16(Context* c, const double* A, int layout, int64_t lda, int64_t m, int64_t n, uint16_t* hi,
                       uint16_t* lo, uint16_t* lo2, int64_t ldo);
+// The same from FP32 A (the parts of its exact FP64 copy).
+int launch_split_bf16_f32(Context* c, const float* A, int layout, int64_t lda, int64_t m, int64_t n, uint16_t* hi,
+                          uint16_t* lo, uint16_t* lo2, int64_t ldo);
 
 // Omega' in BF16 (L x n, pitch ldo) from the same Philox stream as the FP64
 // generator (element (i, j) of the n x L Omega is sample i L + j), rounded to

@@ -22,13 +22,15 @@ __device__ __forceinline__ void split(double x, uint16_t& hi, uint16_t& lo, uint
   lo2 = bf16_bits(__double2bfloat16(r - double(__bfloat162float(l))));
 }
 
-__global__ void k_split_rowmajor(const double* A, int64_t lda, int64_t m, int64_t n, uint16_t* hi, uint16_t* lo,
+// T: double, or float (an FP32 A splits to the same parts as its exact FP64 copy)
+template <class T>
+__global__ void k_split_rowmajor(const T* A, int64_t lda, int64_t m, int64_t n, uint16_t* hi, uint16_t* lo,
                                  uint16_t* lo2, int64_t ldo) {
   const int64_t total = m * n;
   for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x) {
     const int64_t i = e / n, j = e % n;
     uint16_t h, l, l2;
-    split(A[i * lda + j], h, l, l2);
+    split(double(A[i * lda + j]), h, l, l2);
     hi[i * ldo + j] = h;
     if (lo) lo[i * ldo + j] = l;
     if (lo2) lo2[i * ldo + j] = l2;
@@ -37,14 +39,15 @@ __global__ void k_split_rowmajor(const double* A, int64_t lda, int64_t m, int64_
 
 // column-major A (element (i, j) at A[i + j lda]) to row-major hi/lo through
 // 32 x 32 shared-memory tiles (coalesced on both sides)
-__global__ void k_split_colmajor(const double* A, int64_t lda, int64_t m, int64_t n, uint16_t* hi, uint16_t* lo,
+template <class T>
+__global__ void k_split_colmajor(const T* A, int64_t lda, int64_t m, int64_t n, uint16_t* hi, uint16_t* lo,
                                  uint16_t* lo2, int64_t ldo) {
   __shared__ double tile[32][33];
   const int64_t i0 = int64_t(blockIdx.x) * 32, j0 = int64_t(blockIdx.y) * 32;
   const int tx = threadIdx.x, ty = threadIdx.y;   // 32 x 8
   for (int r = ty; r < 32; r += 8) {
     const int64_t i = i0 + tx, j = j0 + r;
-    tile[r][tx] = (i < m && j < n) ? A[i + j * lda] : 0.0;
+    tile[r][tx] = (i < m && j < n) ? double(A[i + j * lda]) : 0.0;
   }
   __syncthreads();
   for (int r = ty; r < 32; r += 8) {
@@ -88,21 +91,32 @@ __global__ void k_gaussian_bf16(uint64_t seed, int64_t n, int64_t L, uint16_t* o
 
 }  // namespace
 
-int launch_split_bf16(Context* c, const double* A, int layout, int64_t lda, int64_t m, int64_t n, uint16_t* hi,
-                      uint16_t* lo, uint16_t* lo2, int64_t ldo) {
+template <class T>
+int split_bf16_any(Context* c, const T* A, int layout, int64_t lda, int64_t m, int64_t n, uint16_t* hi,
+                   uint16_t* lo, uint16_t* lo2, int64_t ldo) {
   if (m <= 0 || n <= 0) return MCNLA_B200_OK;
   if (layout == MCNLA_B200_ROW_MAJOR) {
     const int64_t total = m * n;
     const int blocks = int(std::min<int64_t>(cdiv(total, 256), int64_t(c->num_sms) * 32));
-    k_split_rowmajor<<<blocks, 256, 0, c->stream>>>(A, lda, m, n, hi, lo, lo2, ldo);
+    k_split_rowmajor<T><<<blocks, 256, 0, c->stream>>>(A, lda, m, n, hi, lo, lo2, ldo);
   } else {
     dim3 grid(unsigned(cdiv(m, 32)), unsigned(cdiv(n, 32)));
     if (grid.y > 65535) return MCNLA_B200_ERR_SHAPE;
-    k_split_colmajor<<<grid, dim3(32, 8), 0, c->stream>>>(A, lda, m, n, hi, lo, lo2, ldo);
+    k_split_colmajor<T><<<grid, dim3(32, 8), 0, c->stream>>>(A, lda, m, n, hi, lo, lo2, ldo);
   }
   c->kernels_launched++;
   MB_CHECK_CUDA(cudaGetLastError());
   return MCNLA_B200_OK;
+}
+
+int launch_split_bf16(Context* c, const double* A, int layout, int64_t lda, int64_t m, int64_t n, uint16_t* hi,
+                      uint16_t* lo, uint16_t* lo2, int64_t ldo) {
+  return split_bf16_any(c, A, layout, lda, m, n, hi, lo, lo2, ldo);
+}
+
+int launch_split_bf16_f32(Context* c, const float* A, int layout, int64_t lda, int64_t m, int64_t n, uint16_t* hi,
+                          uint16_t* lo, uint16_t* lo2, int64_t ldo) {
+  return split_bf16_any(c, A, layout, lda, m, n, hi, lo, lo2, ldo);
 }
 
 int launch_gaussian_bf16(Context* c, uint64_t seed, int64_t n, int64_t L, uint16_t* omega_t, int64_t ldo,

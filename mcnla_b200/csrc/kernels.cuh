@@ -42,16 +42,37 @@ size_t kn_series_work_doubles(int l);
 // large for the series; the launcher then runs the other form after it.
 int launch_kn_series(Context* c, int l, const double* z, const double* dd, double inv_n, double* out, double* outn,
                      const double* ff, double* ffn, double* work, double tol);
-// Persistent row-block Gramian KN integrator (gkn_persistent.cu): runs
-// iterations [it0, maxit) on one cooperative grid.  On return (after a
-// stream sync) scal->stop_it is the converged iteration, or scal->resume_it
-// the iteration whose KN step the series declined (to be run by the caller
-// with allow_series = false), or neither (maxit reached).  EB, FF, DD, FC,
-// FCN, work: the buffers of the launch-per-product loop.
-bool gkn_persistent_fits(const Context* c, int l, int64_t L);
-int launch_gkn_persistent(Context* c, int l, int64_t L, int N, double tol, int it0, int maxit, const double* Bs,
-                          double* const EB[2], double* const FF[2], double* DD, double* FC, double* FCN,
-                          double* work);
+// Grouped row-block Gramian KN integrator (gkn_grouped.cu): the iterations of
+// one or many problems, a cluster of CTAs per problem from a device work
+// queue.  A job's fields above stop_it are inputs (the buffers of the
+// launch-per-product loop, plus cbuf: l x l doubles and ddp:
+// gkn_grouped_ddp_doubles of scratch); after the launch stop_it is the
+// converged iteration (INT_MAX: not converged), resume_it the iteration whose
+// KN step the series declined (-1: none; the caller runs it on the
+// launch-per-product path), else maxit was reached.
+struct GknJob {
+  int l, L, it0, maxit, smax, pad0;
+  double inv_n, tol;
+  const double* bs;
+  double *eb0, *eb1, *ff0, *ff1, *dd, *fc, *fcn, *work, *cbuf, *ddp;
+  int stop_it, resume_it;
+  double norm;
+  int degree, pad1;
+  long long ns;     // out: nanoseconds the cluster spent on the job (device global timer)
+};
+// Largest N l the grouped kernel takes (beyond it the launch-per-product loop's
+// shared-memory-pipelined GEMMs are faster).
+constexpr int64_t kGknGroupedMaxL = 1536;
+bool gkn_grouped_fits(const Context* c, int l, int64_t L);
+// Dynamic shared memory of a job with this l (0: l unsupported) and its power slabs.
+size_t gkn_grouped_smem(const Context* c, int l);
+int gkn_grouped_smax(const Context* c, int l);
+size_t gkn_grouped_ddp_doubles(int l, int64_t L);
+// Runs jobs_dev[0 .. njobs) (device memory) on clusters of `cluster` CTAs with
+// `smem` bytes each (at least gkn_grouped_smem of every job's l); next_dev: one
+// device int of scratch.
+int launch_gkn_grouped(Context* c, GknJob* jobs_dev, int njobs, int* next_dev, size_t smem, int cluster);
+
 // Opts a kernel in to the device's whole dynamic shared memory (once per
 // device and kernel); fails when `bytes` exceeds it.
 int set_smem(const Context* c, const void* fn, size_t bytes);

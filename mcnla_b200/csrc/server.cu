@@ -1,11 +1,13 @@
-// Batched and served solves: a pool of host workers, each owning a context
-// (its own stream and workspaces), takes problems from a FIFO queue and runs
-// whole solves concurrently on the device.  Admission: the queue head is
+// Served solves: a pool of host workers, each owning a context (its own
+// stream and workspaces), takes problems from a FIFO queue and runs whole
+// solves concurrently on the device (the batch entry point, which groups the
+// integrator iterations of a whole batch, is in stages.cu).  Admission: the queue head is
 // started when a worker is free and the estimated bytes of the problems in
 // flight, plus its own, stay within the budget (a problem larger than the
 // budget runs alone).  Results do not depend on what else is in flight:
 // every kernel reduces in a fixed order.
 #include "common.cuh"
+#include "solve.cuh"
 
 #include <algorithm>
 #include <atomic>
@@ -20,14 +22,6 @@
 
 namespace mb {
 namespace {
-
-__global__ void k_f32_to_f64(const float* src, int64_t rows, int64_t cols, int64_t lds, double* dst, int64_t ldd) {
-  const int64_t total = rows * cols;
-  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x) {
-    const int64_t r = e / cols, c = e % cols;
-    dst[r * ldd + c] = double(src[r * lds + c]);
-  }
-}
 
 using Clock = std::chrono::steady_clock;
 
@@ -46,19 +40,22 @@ int64_t round8(int64_t x) { return (x + 7) & ~int64_t(7); }
 int64_t problem_bytes(const mcnla_b200_problem& p) {
   const int64_t m = p.params.nrow, n = p.params.ncol, l = p.params.rank + p.params.over_rank;
   const int64_t L = l * p.params.num_sketch;
-  int64_t bytes = (m * L + m * l + n * L) * 8;                                  // Q, Qbar, Omega
+  const bool mixed = p.precision == MCNLA_B200_PRECISION_MIXED || p.precision == MCNLA_B200_PRECISION_MIXED3;
+  int64_t bytes = (m * L + m * l) * 8 + (mixed ? L * round8(n) * 2 : n * L * 8);  // Q, Qbar, Omega
   int64_t stage = m * L * 8 + 5 * l * l * p.params.num_sketch * 8;              // orthogonalizer
   stage = std::max(stage, L * L * 8 + 8 * L * 3 * l * 8 + 4 * m * 2 * l * 8);   // integrators
   stage = std::max(stage, 4 * l * n * 8 + n * l * 8);                           // formers
+  if (mixed) stage = std::max(stage, 3 * l * round8(m) * 2 + 16 * l * n * 8);   // precision former
   bytes += stage + (int64_t(64) << 20);                                         // + split-K partials, small terms
-  if (!p.A && p.A32) bytes += m * n * 8;                                        // FP64 copy of an FP32 A
-  if (p.precision == MCNLA_B200_PRECISION_MIXED) bytes += 2 * m * round8(n) * 2 + L * round8(n) * 2;
-  if (p.precision == MCNLA_B200_PRECISION_MIXED3) bytes += 3 * m * round8(n) * 2 + L * round8(n) * 2;
+  bytes += int64_t(mb::problem_scratch_bytes(p));                               // FP64 copy or BF16 parts of A, A'
   const bool gramian = p.integrator == MCNLA_B200_ROW_BLOCK_GRAMIAN_KOLMOGOROV_NAGUMO ||
                        p.integrator == MCNLA_B200_ROW_BLOCK_GRAMIAN_WEN_YIN;
-  if (p.precision != MCNLA_B200_PRECISION_FP64 && gramian && double(L) * double(L) * double(m) >= kMixedGramianMinFlops) {
-    // the BF16 Gramian's scratch: three parts of Qs', of Bs and of Bc', and the loop's split-K slices
-    bytes += 3 * L * round8(m) * 2 + 3 * L * round8(L) * 2 + 3 * l * round8(L) * 2 + 16 * L * 3 * l * 8;
+  if (mixed && gramian && double(L) * double(L) * double(m) >= kMixedGramianMinFlops) {
+    // the BF16 Gramian's scratch: three parts of Qs' and, for the KN integrator, of Bs and of Bc'
+    // and the loop's split-K slices
+    bytes += 3 * L * round8(m) * 2;
+    if (p.integrator == MCNLA_B200_ROW_BLOCK_GRAMIAN_KOLMOGOROV_NAGUMO)
+      bytes += 3 * L * round8(L) * 2 + 3 * l * round8(L) * 2 + 16 * L * 3 * l * 8;
   }
   return bytes;
 }
@@ -80,57 +77,7 @@ struct mcnla_b200_server {
   std::atomic<int> init_failures{0};
 
   void worker();
-  int run(mcnla_b200_ctx* ctx, mcnla_b200_problem& p, double*& a64, size_t& a64_bytes, uint16_t*& split,
-          size_t& split_bytes);
 };
-
-int mcnla_b200_server::run(mcnla_b200_ctx* ctx, mcnla_b200_problem& p, double*& a64, size_t& a64_bytes,
-                           uint16_t*& split, size_t& split_bytes) {
-  const int64_t m = p.params.nrow, n = p.params.ncol;
-  if (m <= 0 || n <= 0) return MCNLA_B200_ERR_SHAPE;
-  if (p.precision < MCNLA_B200_PRECISION_FP64 || p.precision > MCNLA_B200_PRECISION_MIXED3) return MCNLA_B200_ERR_ARG;
-  const double* A = p.A;
-  int layout = p.a_layout;
-  int64_t lda = p.lda;
-  if (!A) {
-    if (!p.A32) return MCNLA_B200_ERR_ARG;
-    const size_t need = size_t(m) * n * sizeof(double);
-    if (need > a64_bytes) {
-      if (a64) MB_CHECK_CUDA(cudaFreeAsync(a64, ctx->stream));
-      a64 = nullptr;
-      a64_bytes = 0;
-      MB_CHECK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&a64), need, ctx->stream));
-      a64_bytes = need;
-    }
-    const int64_t rows = layout == MCNLA_B200_ROW_MAJOR ? m : n, cols = layout == MCNLA_B200_ROW_MAJOR ? n : m;
-    const int blocks = int(std::min<int64_t>(mb::cdiv(rows * cols, 256), int64_t(ctx->num_sms) * 16));
-    mb::k_f32_to_f64<<<blocks, 256, 0, ctx->stream>>>(p.A32, rows, cols, lda, a64, cols);
-    MB_CHECK_CUDA(cudaGetLastError());
-    A = a64;
-    lda = cols;
-  }
-  if (p.precision == MCNLA_B200_PRECISION_MIXED || p.precision == MCNLA_B200_PRECISION_MIXED3) {
-    const int nparts = p.precision == MCNLA_B200_PRECISION_MIXED3 ? 3 : 2;
-    const int64_t ldo = (n + 7) & ~int64_t(7);
-    const size_t need = nparts * size_t(m) * ldo * sizeof(uint16_t);
-    if (need > split_bytes) {
-      if (split) MB_CHECK_CUDA(cudaFreeAsync(split, ctx->stream));
-      split = nullptr;
-      split_bytes = 0;
-      MB_CHECK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&split), need, ctx->stream));
-      split_bytes = need;
-    }
-    uint16_t* hi = split;
-    uint16_t* lo = split + size_t(m) * ldo;
-    uint16_t* lo2 = nparts == 3 ? split + 2 * size_t(m) * ldo : nullptr;
-    MB_CHECK(mcnla_b200_split_bf16(ctx, A, layout, lda, m, n, hi, lo, lo2, ldo));
-    return mcnla_b200_isvd_mixed(ctx, &p.params, p.integrator, p.former, A, layout, lda, hi, lo, lo2, ldo, nullptr,
-                                 nullptr, nullptr, 0, p.seed,
-                                 p.max_iteration, p.tolerance, p.S, p.U, p.V, &p.iteration);
-  }
-  return mcnla_b200_isvd(ctx, &p.params, p.integrator, p.former, A, layout, lda, nullptr, p.seed, p.max_iteration,
-                         p.tolerance, p.S, p.U, p.V, &p.iteration);
-}
 
 void mcnla_b200_server::worker() {
   cudaSetDevice(device);
@@ -144,10 +91,7 @@ void mcnla_b200_server::worker() {
   // workers' integrations (latency-bound chains of small products) run side by side
   if (ok) ctx->coop_cta_limit = std::max(1, ctx->num_sms / nworkers);
   if (!ok) init_failures++;
-  double* a64 = nullptr;
-  size_t a64_bytes = 0;
-  uint16_t* split = nullptr;
-  size_t split_bytes = 0;
+  mb::SolveScratch scratch;
   while (true) {
     int64_t ticket = 0;
     mcnla_b200_problem p;
@@ -172,7 +116,7 @@ void mcnla_b200_server::worker() {
     float ms = 0.f;
     if (ok) {
       cudaEventRecord(e0, stream);
-      st = run(ctx, p, a64, a64_bytes, split, split_bytes);
+      st = mb::solve_problem(ctx, p, scratch);
       cudaEventRecord(e1, stream);
       if (cudaStreamSynchronize(stream) != cudaSuccess && st == MCNLA_B200_OK) st = MCNLA_B200_ERR_CUDA;
       cudaEventElapsedTime(&ms, e0, e1);
@@ -195,8 +139,7 @@ void mcnla_b200_server::worker() {
     cv_done.notify_all();
     cv_work.notify_all();
   }
-  if (a64) cudaFreeAsync(a64, stream);
-  if (split) cudaFreeAsync(split, stream);
+  if (ctx) mb::solve_scratch_free(ctx, scratch);
   if (stream) cudaStreamSynchronize(stream);
   if (e0) cudaEventDestroy(e0);
   if (e1) cudaEventDestroy(e1);
@@ -278,25 +221,7 @@ int mcnla_b200_server_destroy(mcnla_b200_server* s) {
 }
 
 int mcnla_b200_isvd_batched(int device, mcnla_b200_problem* problems, int count, int workers, int64_t budget_bytes) {
-  if (count < 0 || (count > 0 && !problems)) return MCNLA_B200_ERR_ARG;
-  mcnla_b200_server* s = nullptr;
-  MB_CHECK(mcnla_b200_server_create(&s, device, workers, budget_bytes));
-  std::vector<int64_t> tickets(static_cast<size_t>(count));
-  int first = MCNLA_B200_OK;
-  for (int i = 0; i < count; ++i) {
-    const int st = mcnla_b200_server_submit(s, &problems[i], &tickets[size_t(i)]);
-    if (st != MCNLA_B200_OK) { first = st; tickets[size_t(i)] = 0; }
-  }
-  for (int i = 0; i < count; ++i) {
-    if (!tickets[size_t(i)]) continue;
-    const int st = mcnla_b200_server_wait(s, tickets[size_t(i)], &problems[i]);
-    if (st != MCNLA_B200_OK && first == MCNLA_B200_OK) first = st;
-  }
-  int64_t inflight = 0, peak = 0, done = 0;
-  const int sst = mcnla_b200_server_stats(s, &inflight, &peak, &done);
-  mcnla_b200_server_destroy(s);
-  if (first == MCNLA_B200_OK && sst != MCNLA_B200_OK) first = sst;
-  return first;
+  return mb::batched_solve(device, problems, count, workers, budget_bytes);
 }
 
 }  // extern "C"

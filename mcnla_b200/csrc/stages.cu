@@ -12,9 +12,14 @@
 #include "dgemm.cuh"
 #include "kernels.cuh"
 #include "bf16.cuh"
+#include "solve.cuh"
 #include <algorithm>
 #include <array>
+#include <atomic>
+#include <chrono>
+#include <climits>
 #include <cmath>
+#include <thread>
 #include <vector>
 
 namespace mb {
@@ -378,6 +383,28 @@ int gramian_bs(Context* c, const Dims& d, const double* Qs, double* Bs, double* 
   return MCNLA_B200_OK;
 }
 
+// Buffers of the row-block Gramian Kolmogorov-Nagumo integrator for one problem
+// (carved by gkn_carve below).
+struct GknBufs {
+  uint16_t* bs16 = nullptr;   // precision form: BF16 parts of Qs', of Bs and of Bc', split-K slices
+  uint16_t* bsp = nullptr;
+  uint16_t* bcp = nullptr;
+  double* slices = nullptr;
+  double* Bs = nullptr;       // L x L
+  double* EB[2] = {nullptr, nullptr};   // [E~ | Bc | Bgc] (L x 3l), current / next
+  double* DD = nullptr;       // [Dc | Dgc] (l x 2l)
+  double* FC = nullptr;       // [Fc; inv(C)] (2l x l)
+  double* FCN = nullptr;      // [Fc; inv(C)/N]
+  double* FF[2] = {nullptr, nullptr};   // F~ (l x l)
+  double* Ebar = nullptr;     // L x l
+  double* vwork = nullptr;    // KN step scratch
+  double* cbuf = nullptr;     // l x l scratch of the grouped kernel's step
+  double* ddp = nullptr;      // the grouped kernel's K-slice partials of [Dc | Dgc]
+  double* job = nullptr;      // device GknJob and work-queue counter of a single solve
+  Bf16Split spb;
+  bool bf16_bgc = false;
+};
+
 // Qbar := Q0 F~ + Qs E~ = Qs (E~ + [F~; 0])
 int gramian_form_qbar(Context* c, const Dims& d, const double* Qs, const double* E, int64_t lde, const double* F,
                       double* Ebar, double* Qbar, double* ws) {
@@ -389,20 +416,22 @@ int gramian_form_qbar(Context* c, const Dims& d, const double* Qs, const double*
 }
 
 // RowBlockGramianKolmogorovNagumoIntegrator
-// (row_block_gramian_kolmogorov_nagumo_integrator.hpp:79-229)
-int run_rb_gramian_kn(Context* c, const Dims& d, const double* Qs, int maxit, double tol, double* Qbar, int* iters) {
-  const int l = d.l;
-  const int64_t m = d.m, L = d.L;
-  const double inv_n = 1.0 / d.N;
+// (row_block_gramian_kolmogorov_nagumo_integrator.hpp:79-229), in pieces that
+// the single solve below and the grouped batch (batch.cu) share: the
+// buffers, the preparation (Bs, Bc, F~, E~), one launch-per-product
+// iteration and the final Qbar.  Both run the same operations on the same
+// shapes, so a problem gives the same bits either way.
+size_t gkn_ws_bytes(const Context* c, const Dims& d) {
+  const int64_t L = d.L, l = d.l, m = d.m;
+  return gemm_ws(c, {{L, L, m, 1}, {L, l, L, 1}, {l, 2 * l, L, 1}, {L, l, 2 * l, 1}, {m, l, L, 1}});
+}
+
+// Visits the buffers in carve order: fn(count, element bytes).
+template <class Fn>
+void gkn_layout(const Context* c, const Dims& d, Fn fn, Bf16Split* spb_out = nullptr) {
+  const int64_t L = d.L, l = d.l;
   const int64_t l3 = 3 * l, l2 = 2 * l;
-  const size_t wsb = gemm_ws(c, {{L, L, m, 1}, {L, l, L, 1}, {l, l2, L, 1}, {L, l, l2, 1}, {m, l, L, 1}});
-  Plan pl;
-  pl.add(size_t(L) * L); pl.add(size_t(L) * l3); pl.add(size_t(L) * l3); pl.add(size_t(l2) * l);
-  pl.add(size_t(l2) * l); pl.add(size_t(l2) * l); pl.add(size_t(l) * l); pl.add(size_t(l) * l);
-  pl.add(size_t(L) * l); pl.add(kn_series_work_doubles(l)); pl.add(wsb / 8 + 1);
   const size_t n16 = c->mixed_gramian ? gramian_bs16_count(d) : 0;
-  pl.add(n16, sizeof(uint16_t));
-  // precision form of Bs Bc: three BF16 parts of Bs (L x L) and of Bc' (stacked 3l x L), split-K slices
   const bool bf16_bgc = c->mixed_gramian;
   const int64_t ldL = (L + 7) & ~int64_t(7);
   Bf16Split spb;
@@ -410,71 +439,173 @@ int run_rb_gramian_kn(Context* c, const Dims& d, const double* Qs, int maxit, do
     spb = plan_bf16_split(c, L, 3 * l, L, true, 16);
     spb.split_stride = L * 3 * l;
   }
+  if (spb_out) *spb_out = spb;
   const size_t nbs = bf16_bgc ? 3 * size_t(L) * ldL : 0, nbc = bf16_bgc ? 3 * size_t(l) * ldL : 0;
   const size_t nsl = bf16_bgc ? size_t(spb.splits) * L * 3 * l : 0;
-  pl.add(nbs, sizeof(uint16_t)); pl.add(nbc, sizeof(uint16_t)); pl.add(nsl);
+  fn(n16, 2); fn(nbs, 2); fn(nbc, 2); fn(nsl, 8);
+  fn(size_t(L) * L, 8); fn(size_t(L) * l3, 8); fn(size_t(L) * l3, 8); fn(size_t(l2) * l, 8);
+  fn(size_t(l2) * l, 8); fn(size_t(l2) * l, 8); fn(size_t(l) * l, 8); fn(size_t(l) * l, 8);
+  fn(size_t(L) * l, 8); fn(kn_series_work_doubles(int(l)), 8); fn(size_t(l) * l, 8);
+  fn(gkn_grouped_ddp_doubles(int(l), L), 8); fn((sizeof(GknJob) + 64) / 8, 8);
+}
+
+size_t gkn_state_bytes(const Context* c, const Dims& d) {
+  size_t b = 0;
+  gkn_layout(c, d, [&](size_t count, size_t elem) { b += arena_bytes_for(count, elem); });
+  return b;
+}
+
+// Carves the buffers with take(count, elem) (returns char*, null past the end).
+template <class Take>
+void gkn_carve(const Context* c, const Dims& d, Take take, GknBufs& b) {
+  char* p[17];
+  int i = 0;
+  gkn_layout(c, d, [&](size_t count, size_t elem) { p[i++] = take(count, elem); }, &b.spb);
+  b.bf16_bgc = c->mixed_gramian;
+  b.bs16 = reinterpret_cast<uint16_t*>(p[0]);
+  b.bsp = reinterpret_cast<uint16_t*>(p[1]);
+  b.bcp = reinterpret_cast<uint16_t*>(p[2]);
+  b.slices = reinterpret_cast<double*>(p[3]);
+  b.Bs = reinterpret_cast<double*>(p[4]);
+  b.EB[0] = reinterpret_cast<double*>(p[5]);
+  b.EB[1] = reinterpret_cast<double*>(p[6]);
+  b.DD = reinterpret_cast<double*>(p[7]);
+  b.FC = reinterpret_cast<double*>(p[8]);
+  b.FCN = reinterpret_cast<double*>(p[9]);
+  b.FF[0] = reinterpret_cast<double*>(p[10]);
+  b.FF[1] = reinterpret_cast<double*>(p[11]);
+  b.Ebar = reinterpret_cast<double*>(p[12]);
+  b.vwork = reinterpret_cast<double*>(p[13]);
+  b.cbuf = reinterpret_cast<double*>(p[14]);
+  b.ddp = reinterpret_cast<double*>(p[15]);
+  b.job = reinterpret_cast<double*>(p[16]);
+}
+
+// Cluster size of the grouped kernel for a problem: more CTAs as the
+// iteration's products grow (the results do not depend on it).
+int gkn_cluster_for(int l, int64_t L) {
+  const double w = 2.0 * double(L) * double(L) * l;   // flops of Bs Bc per iteration
+  return w < 4e6 ? 1 : (w < 2e7 ? 2 : (w < 8e7 ? 4 : 8));
+}
+
+GknJob gkn_job(const Context* c, const Dims& d, const GknBufs& b, int it0, int maxit, double tol) {
+  GknJob j = {};
+  j.l = d.l;
+  j.L = int(d.L);
+  j.it0 = it0;
+  j.maxit = maxit;
+  j.smax = gkn_grouped_smax(c, d.l);
+  j.inv_n = 1.0 / d.N;
+  j.tol = tol;
+  j.bs = b.Bs;
+  j.eb0 = b.EB[0];
+  j.eb1 = b.EB[1];
+  j.ff0 = b.FF[0];
+  j.ff1 = b.FF[1];
+  j.dd = b.DD;
+  j.fc = b.FC;
+  j.fcn = b.FCN;
+  j.work = b.vwork;
+  j.cbuf = b.cbuf;
+  j.ddp = b.ddp;
+  j.stop_it = INT_MAX;
+  j.resume_it = -1;
+  return j;
+}
+
+// Bs := Qs' Qs; Bc := Bs(:, 0:l); F~ := I; E~ := 0   (:112-133)
+int gkn_prepare(Context* c, const Dims& d, const double* Qs, const GknBufs& b, double* ws) {
+  const int l = d.l;
+  const int64_t L = d.L, l3 = 3 * l;
+  MB_CHECK(gramian_bs(c, d, Qs, b.Bs, b.EB[0] + l, l3, ws, b.bs16));
+  MB_CHECK(launch_fill(c, L, l, 0.0, b.EB[0], l3));
+  MB_CHECK(launch_set_identity(c, l, b.FF[0], l));
+  const int64_t ldL = (L + 7) & ~int64_t(7);
+  const size_t bpart = size_t(L) * ldL;
+  if (b.bf16_bgc)
+    MB_CHECK(launch_split_bf16(c, b.Bs, MCNLA_B200_ROW_MAJOR, L, L, L, b.bsp, b.bsp + bpart, b.bsp + 2 * bpart, ldL));
+  return MCNLA_B200_OK;
+}
+
+// Iteration i on the launch-per-product path (:152-204).
+int gkn_iteration(Context* c, const Dims& d, const GknBufs& b, int i, bool allow_series, double tol, double* ws) {
+  const int l = d.l;
+  const int64_t L = d.L, l3 = 3 * l, l2 = 2 * l;
+  const double inv_n = 1.0 / d.N;
+  const int cur = i & 1;
+  double* Ec = b.EB[cur];
+  double* Bc = b.EB[cur] + l;
+  double* Bgc = b.EB[cur] + l2;
+  // Bgc := 1/N Bs Bc   (:152)
+  if (b.bf16_bgc) {
+    // (Bs_hi + Bs_lo + Bs_lo2) [Bc_hi | Bc_lo | Bc_lo2] on tcgen05 (Bc' split from the column-major view
+    // of Bc), the three column groups and the K slices added in order, times 1/N
+    const int64_t ldL = (L + 7) & ~int64_t(7);
+    const size_t bpart = size_t(L) * ldL, cpart = size_t(l) * ldL;
+    MB_CHECK(launch_split_bf16(c, Bc, MCNLA_B200_COL_MAJOR, l3, l, L, b.bcp, b.bcp + cpart, b.bcp + 2 * cpart, ldL));
+    MB_CHECK(bf16_gemm_split(c, L, 3 * l, L, b.bsp, b.bsp + bpart, b.bsp + 2 * bpart, ldL, b.bcp, ldL, b.slices,
+                             3 * l, true, false, false, b.spb));
+    MB_CHECK(launch_sum_splits(c, b.slices, b.spb.splits, b.spb.split_stride, L, l, 3 * l, Bgc, l3, false, inv_n, 3,
+                               l));
+  } else {
+    MB_CHECK(dgemm(c, L, l, L, inv_n, crow(b.Bs, L), crow(Bc, l3), 0.0, drow(Bgc, l3), GemmBatch(), ws));
+  }
+  // [Dc | Dgc] := 1/N Bc' [Bc | Bgc]   (:155-158)
+  MB_CHECK(dgemm(c, l, l2, L, inv_n, cm(Bc, 1, l3), crow(Bc, l3), 0.0, drow(b.DD, l2), GemmBatch(), ws));
+  // Z, eig, C, inv(C), Fc; F~+ := F~c Fc; convergence test   (:164-214)
+  MB_CHECK(launch_kn_step(c, l, nullptr, b.DD, inv_n, b.FC, b.FCN, b.FF[cur], b.FF[1 - cur], b.vwork, tol,
+                          allow_series));
+  // E~+ := E~c Fc + 1/N Bc inv(C) = [E~c Bc] [Fc; inv(C)/N]   (:194, :200)
+  MB_CHECK(dgemm(c, L, l, l2, 1.0, crow(Ec, l3), crow(b.FCN, l), 0.0, drow(b.EB[1 - cur], l3), GemmBatch(), ws));
+  // B+ := [Bc Bgc] [Fc; inv(C)]   (:203-204)
+  MB_CHECK(dgemm(c, L, l, l2, 1.0, crow(Bc, l3), crow(b.FC, l), 0.0, drow(b.EB[1 - cur] + l, l3), GemmBatch(), ws));
+  return MCNLA_B200_OK;
+}
+
+// Qbar := Q0 F~ + Qs E~ after `it` iterations   (:225-226)
+int gkn_finish(Context* c, const Dims& d, const double* Qs, const GknBufs& b, int it, double* Qbar, double* ws) {
+  const int cur = it & 1;
+  return gramian_form_qbar(c, d, Qs, b.EB[cur], 3 * d.l, b.FF[cur], b.Ebar, Qbar, ws);
+}
+
+int run_rb_gramian_kn(Context* c, const Dims& d, const double* Qs, int maxit, double tol, double* Qbar, int* iters) {
+  const int l = d.l;
+  const int64_t L = d.L;
+  const size_t wsb = gkn_ws_bytes(c, d);
+  Plan pl;
+  gkn_layout(c, d, [&](size_t count, size_t elem) { pl.add(count, elem); });
+  pl.add(wsb / 8 + 1);
   MB_CHECK(ctx_reserve(c, pl.bytes));
-  uint16_t* bs16 = ctx_take<uint16_t>(c, n16);
-  uint16_t* bsp = ctx_take<uint16_t>(c, nbs);
-  uint16_t* bcp = ctx_take<uint16_t>(c, nbc);
-  double* slices = ctx_take<double>(c, nsl);
-  double* Bs = ctx_take<double>(c, size_t(L) * L);
-  double* EB[2] = {ctx_take<double>(c, size_t(L) * l3), ctx_take<double>(c, size_t(L) * l3)};
-  double* DD = ctx_take<double>(c, size_t(l2) * l);
-  double* FC = ctx_take<double>(c, size_t(l2) * l);
-  double* FCN = ctx_take<double>(c, size_t(l2) * l);
-  double* FF[2] = {ctx_take<double>(c, size_t(l) * l), ctx_take<double>(c, size_t(l) * l)};
-  double* Ebar = ctx_take<double>(c, size_t(L) * l);
-  double* vwork = ctx_take<double>(c, kn_series_work_doubles(l));
+  GknBufs b;
+  gkn_carve(c, d, [&](size_t count, size_t elem) -> char* {
+    return elem == 2 ? reinterpret_cast<char*>(ctx_take<uint16_t>(c, count))
+                     : reinterpret_cast<char*>(ctx_take<double>(c, count));
+  }, b);
   double* ws = take_ws(c, wsb);
   MB_CHECK(check_arena(c));
   MB_CHECK(ctx_tic(c));
-  // Bs := Qs' Qs; Bc := Bs(:, 0:l); F~ := I; E~ := 0   (:112-133)
-  MB_CHECK(gramian_bs(c, d, Qs, Bs, EB[0] + l, l3, ws, bs16));
-  MB_CHECK(launch_fill(c, L, l, 0.0, EB[0], l3));
-  MB_CHECK(launch_set_identity(c, l, FF[0], l));
-  const size_t bpart = size_t(L) * ldL, cpart = size_t(l) * ldL;
-  if (bf16_bgc) MB_CHECK(launch_split_bf16(c, Bs, MCNLA_B200_ROW_MAJOR, L, L, L, bsp, bsp + bpart, bsp + 2 * bpart, ldL));
+  MB_CHECK(gkn_prepare(c, d, Qs, b, ws));
   MB_CHECK(ctx_toc(c));
-  auto body = [&](int i, bool allow_series) -> int {
-    const int cur = i & 1;
-    double* Ec = EB[cur];
-    double* Bc = EB[cur] + l;
-    double* Bgc = EB[cur] + l2;
-    // Bgc := 1/N Bs Bc   (:152)
-    if (bf16_bgc) {
-      // (Bs_hi + Bs_lo + Bs_lo2) [Bc_hi | Bc_lo | Bc_lo2] on tcgen05 (Bc' split from the column-major view
-      // of Bc), the three column groups and the K slices added in order, times 1/N
-      MB_CHECK(launch_split_bf16(c, Bc, MCNLA_B200_COL_MAJOR, l3, l, L, bcp, bcp + cpart, bcp + 2 * cpart, ldL));
-      MB_CHECK(bf16_gemm_split(c, L, 3 * l, L, bsp, bsp + bpart, bsp + 2 * bpart, ldL, bcp, ldL, slices, 3 * l, true,
-                               false, false, spb));
-      MB_CHECK(launch_sum_splits(c, slices, spb.splits, spb.split_stride, L, l, 3 * l, Bgc, l3, false, inv_n, 3, l));
-    } else {
-      MB_CHECK(dgemm(c, L, l, L, inv_n, crow(Bs, L), crow(Bc, l3), 0.0, drow(Bgc, l3), GemmBatch(), ws));
-    }
-    // [Dc | Dgc] := 1/N Bc' [Bc | Bgc]   (:155-158)
-    MB_CHECK(dgemm(c, l, l2, L, inv_n, cm(Bc, 1, l3), crow(Bc, l3), 0.0, drow(DD, l2), GemmBatch(), ws));
-    // Z, eig, C, inv(C), Fc; F~+ := F~c Fc; convergence test   (:164-214)
-    MB_CHECK(launch_kn_step(c, l, nullptr, DD, inv_n, FC, FCN, FF[cur], FF[1 - cur], vwork, tol, allow_series));
-    // E~+ := E~c Fc + 1/N Bc inv(C) = [E~c Bc] [Fc; inv(C)/N]   (:194, :200)
-    MB_CHECK(dgemm(c, L, l, l2, 1.0, crow(Ec, l3), crow(FCN, l), 0.0, drow(EB[1 - cur], l3), GemmBatch(), ws));
-    // B+ := [Bc Bgc] [Fc; inv(C)]   (:203-204)
-    MB_CHECK(dgemm(c, L, l, l2, 1.0, crow(Bc, l3), crow(FC, l), 0.0, drow(EB[1 - cur] + l, l3), GemmBatch(), ws));
-    return MCNLA_B200_OK;
-  };
+  auto body = [&](int i, bool allow_series) -> int { return gkn_iteration(c, d, b, i, allow_series, tol, ws); };
   int it = 0;
-  if (c->kn_mode == MCNLA_B200_KN_AUTO && gkn_persistent_fits(c, l, L)) {
-    // whole iterations on one cooperative grid; an iteration whose KN step the
-    // series declines runs here on the launch-per-product path
+  if (c->kn_mode == MCNLA_B200_KN_AUTO && gkn_grouped_fits(c, l, L)) {
+    // whole iterations in the grouped kernel (one problem, one cluster); an
+    // iteration whose KN step the series declines runs here on the
+    // launch-per-product path
     MB_CHECK_CUDA(cudaMemsetAsync(&c->scal->stop_it, 0x7f, sizeof(int), c->stream));   // "not yet"
+    GknJob* jdev = reinterpret_cast<GknJob*>(b.job);
+    int* next = reinterpret_cast<int*>(reinterpret_cast<char*>(b.job) + sizeof(GknJob));
+    const size_t smem = gkn_grouped_smem(c, l);
+    const int cluster = gkn_cluster_for(l, L);
     int it0 = 0, done = -1;
     while (it0 < maxit && done < 0) {
-      MB_CHECK_CUDA(cudaMemsetAsync(&c->scal->resume_it, 0xff, sizeof(int), c->stream));   // -1
-      MB_CHECK(launch_gkn_persistent(c, l, L, d.N, tol, it0, maxit, Bs, EB, FF, DD, FC, FCN, vwork));
-      MB_CHECK(ctx_sync_scalars(c));
-      if (c->scal_host->status) return c->scal_host->status;
-      if (c->scal_host->stop_it < maxit) { done = c->scal_host->stop_it + 1; break; }
-      const int r = c->scal_host->resume_it;
+      GknJob j = gkn_job(c, d, b, it0, maxit, tol);
+      MB_CHECK_CUDA(cudaMemcpyAsync(jdev, &j, sizeof(GknJob), cudaMemcpyHostToDevice, c->stream));
+      MB_CHECK(launch_gkn_grouped(c, jdev, 1, next, smem, cluster));
+      MB_CHECK_CUDA(cudaMemcpyAsync(&j, jdev, sizeof(GknJob), cudaMemcpyDeviceToHost, c->stream));
+      MB_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+      if (j.stop_it != INT_MAX) { done = j.stop_it + 1; break; }
+      const int r = j.resume_it;
       if (r < 0) break;                                       // maxit reached
       struct Reset { Context* c; ~Reset() { c->guard_stop = nullptr; c->guard_it = 0; } } reset{c};
       c->guard_stop = &c->scal->stop_it;
@@ -489,10 +620,8 @@ int run_rb_gramian_kn(Context* c, const Dims& d, const double* Qs, int maxit, do
   } else {
     MB_CHECK(kn_loop(c, maxit, [&](int i) -> int { return body(i, true); }, &it));
   }
-  const int cur = it & 1;
   MB_CHECK(ctx_toc(c));
-  // Qbar := Q0 F~ + Qs E~   (:225-226)
-  MB_CHECK(gramian_form_qbar(c, d, Qs, EB[cur], l3, FF[cur], Ebar, Qbar, ws));
+  MB_CHECK(gkn_finish(c, d, Qs, b, it, Qbar, ws));
   MB_CHECK(ctx_toc(c));
   *iters = it;
   return MCNLA_B200_OK;
@@ -1059,6 +1188,509 @@ size_t stage_bytes_upper(Context* c, const Dims& d) {
 }
 
 }  // namespace
+
+// ---------------------------------------------------------------------------
+// Batched and served problems (mcnla_b200_problem): the whole solve of one
+// problem on a worker, and the grouped batch
+// ---------------------------------------------------------------------------
+namespace {
+
+__global__ void k_f32_to_f64(const float* src, int64_t rows, int64_t cols, int64_t lds, double* dst, int64_t ldd) {
+  const int64_t total = rows * cols;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t r = e / cols, cc = e % cols;
+    dst[r * ldd + cc] = double(src[r * lds + cc]);
+  }
+}
+
+// Grows a stream-ordered device buffer to at least `need` bytes.
+int grow(Context* c, void** p, size_t* have, size_t need) {
+  if (need <= *have) return MCNLA_B200_OK;
+  if (*p) MB_CHECK_CUDA(cudaFreeAsync(*p, c->stream));
+  *p = nullptr;
+  *have = 0;
+  const cudaError_t e = cudaMallocAsync(p, need, c->stream);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    set_last_cuda_error(e, "problem scratch cudaMalloc", __FILE__, __LINE__);
+    *p = nullptr;
+    return MCNLA_B200_ERR_NOMEM;
+  }
+  *have = need;
+  return MCNLA_B200_OK;
+}
+
+bool problem_mixed(const mcnla_b200_problem& p) {
+  return p.precision == MCNLA_B200_PRECISION_MIXED || p.precision == MCNLA_B200_PRECISION_MIXED3;
+}
+
+int problem_check(const mcnla_b200_problem& p, Dims& d) {
+  MB_CHECK(get_dims(&p.params, d));
+  if (p.precision < MCNLA_B200_PRECISION_FP64 || p.precision > MCNLA_B200_PRECISION_MIXED3) return MCNLA_B200_ERR_ARG;
+  if (!p.A && !p.A32 && !(problem_mixed(p) && p.a_hi && p.at_hi)) return MCNLA_B200_ERR_ARG;
+  if (p.a_layout != MCNLA_B200_ROW_MAJOR && p.a_layout != MCNLA_B200_COL_MAJOR) return MCNLA_B200_ERR_ARG;
+  return MCNLA_B200_OK;
+}
+
+}  // namespace
+
+void solve_scratch_free(Context* c, SolveScratch& s) {
+  if (s.a64) cudaFreeAsync(s.a64, c->stream);
+  if (s.split) cudaFreeAsync(s.split, c->stream);
+  if (s.tsplit) cudaFreeAsync(s.tsplit, c->stream);
+  s = SolveScratch();
+}
+
+// A in FP64: the caller's, or an FP32 A converted into scratch.
+int problem_a64(Context* c, const mcnla_b200_problem& p, SolveScratch& s, const double** A, int64_t* lda) {
+  if (p.A) {
+    *A = p.A;
+    *lda = p.lda;
+    return MCNLA_B200_OK;
+  }
+  if (!p.A32) return MCNLA_B200_ERR_ARG;
+  const int64_t m = p.params.nrow, n = p.params.ncol;
+  MB_CHECK(grow(c, reinterpret_cast<void**>(&s.a64), &s.a64_bytes, size_t(m) * n * sizeof(double)));
+  const bool row = p.a_layout == MCNLA_B200_ROW_MAJOR;
+  const int64_t rows = row ? m : n, cols = row ? n : m;
+  const int blocks = int(std::min<int64_t>(cdiv(rows * cols, 256), int64_t(c->num_sms) * 16));
+  k_f32_to_f64<<<blocks, 256, 0, c->stream>>>(p.A32, rows, cols, p.lda, s.a64, cols);
+  MB_CHECK_CUDA(cudaGetLastError());
+  c->kernels_launched++;
+  *A = s.a64;
+  *lda = cols;
+  return MCNLA_B200_OK;
+}
+
+// BF16 parts of A (row-major m x n) for the mixed sketch: the caller's, or split into scratch.
+int problem_parts(Context* c, const mcnla_b200_problem& p, SolveScratch& s, const uint16_t** part, int64_t* ld) {
+  const int nparts = p.precision == MCNLA_B200_PRECISION_MIXED3 ? 3 : 2;
+  if (p.a_hi) {
+    part[0] = p.a_hi;
+    part[1] = p.a_lo;
+    part[2] = nparts == 3 ? p.a_lo2 : nullptr;
+    *ld = p.lda16;
+    if (!p.a_lo || (nparts == 3 && !p.a_lo2)) return MCNLA_B200_ERR_ARG;
+    return MCNLA_B200_OK;
+  }
+  const int64_t m = p.params.nrow, n = p.params.ncol, ldo = (n + 7) & ~int64_t(7);
+  MB_CHECK(grow(c, reinterpret_cast<void**>(&s.split), &s.split_bytes, nparts * size_t(m) * ldo * sizeof(uint16_t)));
+  part[0] = s.split;
+  part[1] = s.split + size_t(m) * ldo;
+  part[2] = nparts == 3 ? s.split + 2 * size_t(m) * ldo : nullptr;
+  uint16_t* w[3] = {s.split, s.split + size_t(m) * ldo, nparts == 3 ? s.split + 2 * size_t(m) * ldo : nullptr};
+  if (p.A32) MB_CHECK(launch_split_bf16_f32(c, p.A32, p.a_layout, p.lda, m, n, w[0], w[1], w[2], ldo));
+  else MB_CHECK(launch_split_bf16(c, p.A, p.a_layout, p.lda, m, n, w[0], w[1], w[2], ldo));
+  *ld = ldo;
+  return MCNLA_B200_OK;
+}
+
+// Three BF16 parts of A' (n x m) for the precision former: A read with the other layout.
+int problem_tparts(Context* c, const mcnla_b200_problem& p, SolveScratch& s, AtParts* at) {
+  if (p.at_hi) {
+    if (!p.at_lo || !p.at_lo2) return MCNLA_B200_ERR_ARG;
+    at->hi = p.at_hi;
+    at->lo = p.at_lo;
+    at->lo2 = p.at_lo2;
+    at->ld = p.ldat16;
+    return MCNLA_B200_OK;
+  }
+  const int64_t m = p.params.nrow, n = p.params.ncol, ldo = (m + 7) & ~int64_t(7);
+  MB_CHECK(grow(c, reinterpret_cast<void**>(&s.tsplit), &s.tsplit_bytes, 3 * size_t(n) * ldo * sizeof(uint16_t)));
+  uint16_t* w[3] = {s.tsplit, s.tsplit + size_t(n) * ldo, s.tsplit + 2 * size_t(n) * ldo};
+  const int tl = p.a_layout == MCNLA_B200_ROW_MAJOR ? MCNLA_B200_COL_MAJOR : MCNLA_B200_ROW_MAJOR;
+  if (p.A32) MB_CHECK(launch_split_bf16_f32(c, p.A32, tl, p.lda, n, m, w[0], w[1], w[2], ldo));
+  else MB_CHECK(launch_split_bf16(c, p.A, tl, p.lda, n, m, w[0], w[1], w[2], ldo));
+  at->hi = w[0];
+  at->lo = w[1];
+  at->lo2 = w[2];
+  at->ld = ldo;
+  return MCNLA_B200_OK;
+}
+
+size_t problem_scratch_bytes(const mcnla_b200_problem& p) {
+  const int64_t m = p.params.nrow, n = p.params.ncol;
+  if (!problem_mixed(p)) return p.A ? 0 : size_t(m) * n * 8;
+  const int nparts = p.precision == MCNLA_B200_PRECISION_MIXED3 ? 3 : 2;
+  size_t b = 0;
+  if (!p.a_hi) b += nparts * size_t(m) * ((n + 7) & ~int64_t(7)) * 2;
+  if (!p.at_hi) b += 3 * size_t(n) * ((m + 7) & ~int64_t(7)) * 2;
+  return b;
+}
+
+// One whole solve on a worker: the plain path, or the precision form with
+// the sketch and the former on tcgen05 (mcnla_b200_isvd / _isvd_mixed).
+int solve_problem(Context* c, mcnla_b200_problem& p, SolveScratch& s) {
+  Dims d;
+  MB_CHECK(problem_check(p, d));
+  if (!problem_mixed(p)) {
+    const double* A = nullptr;
+    int64_t lda = 0;
+    MB_CHECK(problem_a64(c, p, s, &A, &lda));
+    return mcnla_b200_isvd(static_cast<mcnla_b200_ctx*>(c), &p.params, p.integrator, p.former, A, p.a_layout, lda, nullptr, p.seed,
+                           p.max_iteration, p.tolerance, p.S, p.U, p.V, &p.iteration);
+  }
+  const uint16_t* part[3];
+  int64_t ld16 = 0;
+  MB_CHECK(problem_parts(c, p, s, part, &ld16));
+  AtParts at;
+  MB_CHECK(problem_tparts(c, p, s, &at));
+  return mcnla_b200_isvd_mixed(static_cast<mcnla_b200_ctx*>(c), &p.params, p.integrator, p.former, nullptr, MCNLA_B200_ROW_MAJOR, 0, part[0],
+                               part[1], part[2], ld16, at.hi, at.lo, at.lo2, at.ld, p.seed, p.max_iteration,
+                               p.tolerance, p.S, p.U, p.V, &p.iteration);
+}
+
+namespace {
+
+// A problem of the grouped batch and its device state (carved from the wave arena).
+struct GItem {
+  mcnla_b200_problem* p = nullptr;
+  Dims d;
+  double* Q = nullptr;
+  double* Qbar = nullptr;
+  double* omega = nullptr;        // FP64 path
+  uint16_t* omega_t = nullptr;    // mixed path (L x ldo BF16)
+  GknBufs b;
+  int it0 = 0, iters = 0, status = MCNLA_B200_OK;
+  bool done = false;
+  double seconds = 0.0;
+};
+
+size_t gitem_bytes(const Context* c, const Dims& d, bool mixed) {
+  const int64_t ldo = (d.n + 7) & ~int64_t(7);
+  return arena_bytes_for(size_t(d.m) * d.L, 8) + arena_bytes_for(size_t(d.m) * d.l, 8) +
+         (mixed ? arena_bytes_for(size_t(d.L) * ldo, 2) : arena_bytes_for(size_t(d.n) * d.L, 8)) +
+         gkn_state_bytes(c, d);
+}
+
+// A problem runs in the grouped batch when it uses the row-block Gramian KN
+// integrator on the path whose iterations the grouped kernel runs in a single
+// solve too (the default step method, N l <= 1536) with the FP64 Gramian.
+bool grouped_eligible(const Context* c, const mcnla_b200_problem& p) {
+  Dims d;
+  if (problem_check(p, d) != MCNLA_B200_OK) return false;
+  if (p.integrator != MCNLA_B200_ROW_BLOCK_GRAMIAN_KOLMOGOROV_NAGUMO) return false;
+  if (p.former < MCNLA_B200_SVD_FORMER || p.former > MCNLA_B200_COL_BLOCK_GRAMIAN_FORMER || d.k > d.l) return false;
+  if (p.max_iteration < 0 || !(p.tolerance >= 0.0)) return false;
+  if (c->kn_mode != MCNLA_B200_KN_AUTO || !gkn_grouped_fits(c, d.l, d.L)) return false;
+  if (gkn_grouped_smem(c, d.l) == 0) return false;
+  if (problem_mixed(p) && double(d.L) * double(d.L) * double(d.m) >= kMixedGramianMinFlops) return false;
+  return true;
+}
+
+template <class F>
+int parallel_for(int device, int workers, int n, F f) {
+  std::atomic<int> next{0};
+  std::vector<std::thread> th;
+  for (int w = 0; w < workers; ++w) {
+    th.emplace_back([&, w] {
+      cudaSetDevice(device);
+      for (int i = next++; i < n; i = next++) f(w, i);
+    });
+  }
+  for (auto& t : th) t.join();
+  return MCNLA_B200_OK;
+}
+
+// Phase A of a grouped problem: Omega, the sketch, the orthogonalizer and the
+// Gramian (the operations of mcnla_b200_isvd / _isvd_mixed up to the
+// integrator's iterations).
+int gitem_phase_a(Context* c, GItem& it, SolveScratch& s) {
+  mcnla_b200_problem& p = *it.p;
+  const Dims& d = it.d;
+  if (!problem_mixed(p)) {
+    const double* A = nullptr;
+    int64_t lda = 0;
+    MB_CHECK(problem_a64(c, p, s, &A, &lda));
+    MB_CHECK(launch_gaussian(c, p.seed, int64_t(d.n) * d.L, it.omega));
+    MB_CHECK(run_sketch(c, d, A, p.a_layout, lda, it.omega, 0, it.Q, false));
+  } else {
+    const uint16_t* part[3];
+    int64_t ld16 = 0;
+    MB_CHECK(problem_parts(c, p, s, part, &ld16));
+    const int64_t ldo = (d.n + 7) & ~int64_t(7);
+    MB_CHECK_CUDA(cudaMemsetAsync(c->scal, 0, sizeof(DevScalars), c->stream));
+    MB_CHECK(launch_gaussian_bf16(c, p.seed, d.n, d.L, it.omega_t, ldo, nullptr));
+    MB_CHECK(bf16_gemm(c, d.m, d.L, d.n, part[0], part[1], part[2], ld16, it.omega_t, ldo, it.Q, d.L, true));
+  }
+  MB_CHECK(run_orthogonalize(c, d, it.Q));
+  MB_CHECK_CUDA(cudaMemsetAsync(c->scal, 0, sizeof(DevScalars), c->stream));
+  const size_t wsb = gkn_ws_bytes(c, d);
+  MB_CHECK(ctx_reserve(c, wsb + 512));
+  double* ws = take_ws(c, wsb);
+  MB_CHECK(gkn_prepare(c, d, it.Q, it.b, ws));
+  MB_CHECK(ctx_sync_scalars(c));
+  return c->scal_host->status;
+}
+
+// A declined iteration r on the launch-per-product path (the single solve's
+// host step).  Sets it.done / it.iters, or it.it0 = r + 1.
+int gitem_fallback(Context* c, GItem& it, int r) {
+  const Dims& d = it.d;
+  const size_t wsb = gkn_ws_bytes(c, d);
+  MB_CHECK(ctx_reserve(c, wsb + 512));
+  double* ws = take_ws(c, wsb);
+  MB_CHECK_CUDA(cudaMemsetAsync(c->scal, 0, sizeof(DevScalars), c->stream));
+  MB_CHECK_CUDA(cudaMemsetAsync(&c->scal->stop_it, 0x7f, sizeof(int), c->stream));
+  {
+    struct Reset { Context* c; ~Reset() { c->guard_stop = nullptr; c->guard_it = 0; } } reset{c};
+    c->guard_stop = &c->scal->stop_it;
+    c->guard_it = r;
+    MB_CHECK(gkn_iteration(c, d, it.b, r, false, it.p->tolerance, ws));
+  }
+  MB_CHECK(ctx_sync_scalars(c));
+  if (c->scal_host->status) return c->scal_host->status;
+  if (c->scal_host->stop_it == r) {
+    it.done = true;
+    it.iters = r + 1;
+  } else {
+    it.it0 = r + 1;
+    if (it.it0 >= it.p->max_iteration) {
+      it.done = true;
+      it.iters = it.p->max_iteration;
+    }
+  }
+  return MCNLA_B200_OK;
+}
+
+// Phase C: Qbar and the former.
+int gitem_phase_c(Context* c, GItem& it, SolveScratch& s) {
+  mcnla_b200_problem& p = *it.p;
+  const Dims& d = it.d;
+  const size_t wsb = gkn_ws_bytes(c, d);
+  MB_CHECK(ctx_reserve(c, wsb + 512));
+  double* ws = take_ws(c, wsb);
+  MB_CHECK_CUDA(cudaMemsetAsync(c->scal, 0, sizeof(DevScalars), c->stream));
+  MB_CHECK(gkn_finish(c, d, it.Q, it.b, it.iters, it.Qbar, ws));
+  if (!problem_mixed(p)) {
+    const double* A = nullptr;
+    int64_t lda = 0;
+    MB_CHECK(problem_a64(c, p, s, &A, &lda));
+    MB_CHECK(run_form(c, d, p.former, A, p.a_layout, lda, it.Qbar, p.S, p.U, p.V));
+  } else {
+    AtParts at;
+    MB_CHECK(problem_tparts(c, p, s, &at));
+    MB_CHECK(run_form(c, d, p.former, nullptr, MCNLA_B200_ROW_MAJOR, 0, it.Qbar, p.S, p.U, p.V, &at));
+  }
+  MB_CHECK(ctx_sync_scalars(c));
+  return c->scal_host->status;
+}
+
+using Clock = std::chrono::steady_clock;
+
+// The grouped integrator over the wave's problems: per round one launch per
+// cluster size (on the first workers' streams, side by side), then the
+// declined iterations on the workers.
+int grouped_rounds(int device, std::vector<Context*>& ctx, std::vector<GItem*>& items) {
+  Context* c0 = ctx[0];
+  const int n = int(items.size());
+  if (n == 0) return MCNLA_B200_OK;
+  constexpr int kClasses = 4;                        // clusters of 1, 2, 4, 8 CTAs
+  auto cls = [](const GItem& it) {
+    const int c = gkn_cluster_for(it.d.l, it.d.L);
+    return c >= 8 ? 3 : (c >= 4 ? 2 : (c >= 2 ? 1 : 0));
+  };
+  size_t smem[kClasses] = {0, 0, 0, 0};
+  for (auto* it : items) smem[cls(*it)] = std::max(smem[cls(*it)], gkn_grouped_smem(c0, it->d.l));
+  GknJob* jobs_dev = nullptr;
+  MB_CHECK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&jobs_dev), sizeof(GknJob) * n + 256, c0->stream));
+  int* next_dev = reinterpret_cast<int*>(reinterpret_cast<char*>(jobs_dev) + sizeof(GknJob) * n);
+  MB_CHECK_CUDA(cudaStreamSynchronize(c0->stream));
+  struct Free { Context* c; void* p; ~Free() { cudaFreeAsync(p, c->stream); cudaStreamSynchronize(c->stream); } }
+      release{c0, jobs_dev};
+  std::vector<GknJob> jobs;
+  std::vector<GItem*> pending;
+  for (auto* it : items)
+    if (!it->done && it->status == MCNLA_B200_OK) pending.push_back(it);
+  while (!pending.empty()) {
+    // jobs ordered by class (largest first), each class a contiguous range
+    std::stable_sort(pending.begin(), pending.end(), [&](const GItem* a, const GItem* b) { return cls(*a) > cls(*b); });
+    const int np = int(pending.size());
+    jobs.assign(size_t(np), GknJob());
+    int first[kClasses + 1] = {0, 0, 0, 0, 0};
+    for (int i = 0; i < np; ++i) {
+      GItem& it = *pending[size_t(i)];
+      jobs[size_t(i)] = gkn_job(c0, it.d, it.b, it.it0, it.p->max_iteration, it.p->tolerance);
+    }
+    for (int k = kClasses - 1, i = 0; k >= 0; --k) {
+      first[k + 1] = i;
+      while (i < np && cls(*pending[size_t(i)]) == k) ++i;
+      first[k] = i;
+    }
+    MB_CHECK_CUDA(cudaMemcpyAsync(jobs_dev, jobs.data(), sizeof(GknJob) * np, cudaMemcpyHostToDevice, c0->stream));
+    MB_CHECK_CUDA(cudaStreamSynchronize(c0->stream));
+    int lane = 0;
+    for (int k = kClasses - 1; k >= 0; --k) {
+      const int b0 = first[k + 1], cnt = first[k] - first[k + 1];
+      if (cnt == 0) continue;
+      Context* c = ctx[size_t(lane % int(ctx.size()))];
+      MB_CHECK(launch_gkn_grouped(c, jobs_dev + b0, cnt, next_dev + k, smem[k], 1 << k));
+      ++lane;
+    }
+    for (int w = 0; w < std::min(lane, int(ctx.size())); ++w) MB_CHECK_CUDA(cudaStreamSynchronize(ctx[size_t(w)]->stream));
+    MB_CHECK_CUDA(cudaMemcpyAsync(jobs.data(), jobs_dev, sizeof(GknJob) * np, cudaMemcpyDeviceToHost, c0->stream));
+    MB_CHECK_CUDA(cudaStreamSynchronize(c0->stream));
+    std::vector<std::pair<GItem*, int>> fallback;
+    for (int i = 0; i < np; ++i) {
+      GItem& it = *pending[size_t(i)];
+      const GknJob& j = jobs[size_t(i)];
+      it.seconds += double(j.ns) * 1e-9;
+      if (j.stop_it != INT_MAX) {
+        it.done = true;
+        it.iters = j.stop_it + 1;
+      } else if (j.resume_it >= 0) {
+        fallback.emplace_back(&it, j.resume_it);
+      } else {
+        it.done = true;
+        it.iters = it.p->max_iteration;
+      }
+    }
+    parallel_for(device, int(ctx.size()), int(fallback.size()), [&](int w, int i) {
+      GItem& it = *fallback[size_t(i)].first;
+      const auto tf = Clock::now();
+      const int st = gitem_fallback(ctx[size_t(w)], it, fallback[size_t(i)].second);
+      it.seconds += std::chrono::duration<double>(Clock::now() - tf).count();
+      if (st != MCNLA_B200_OK) {
+        it.status = st;
+        it.done = true;
+      }
+    });
+    pending.clear();
+    for (auto* it : items)
+      if (!it->done && it->status == MCNLA_B200_OK) pending.push_back(it);
+  }
+  return MCNLA_B200_OK;
+}
+
+}  // namespace
+
+// The grouped batch (mcnla_b200_isvd_batched): problems the grouped kernel
+// takes (grouped_eligible) run in waves through phases A / grouped rounds / C
+// on `workers` contexts; the others run whole solves through a worker pool.
+int batched_solve(int device, mcnla_b200_problem* problems, int count, int workers, int64_t budget) {
+  if (count < 0 || (count > 0 && !problems) || workers < 1 || workers > 256 || budget <= 0) return MCNLA_B200_ERR_ARG;
+  MB_CHECK_CUDA(cudaSetDevice(device));
+  const auto t0 = Clock::now();
+  std::vector<Context*> ctx;
+  std::vector<cudaStream_t> streams;
+  std::vector<SolveScratch> scratch(static_cast<size_t>(workers));
+  struct Cleanup {
+    std::vector<Context*>& ctx;
+    std::vector<cudaStream_t>& streams;
+    std::vector<SolveScratch>& scratch;
+    ~Cleanup() {
+      for (size_t i = 0; i < ctx.size(); ++i) {
+        solve_scratch_free(ctx[i], scratch[i]);
+        mcnla_b200_destroy(static_cast<mcnla_b200_ctx*>(ctx[i]));
+      }
+      for (auto s : streams) cudaStreamDestroy(s);
+    }
+  } cleanup{ctx, streams, scratch};
+  for (int w = 0; w < workers; ++w) {
+    cudaStream_t st = nullptr;
+    MB_CHECK_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    streams.push_back(st);
+    mcnla_b200_ctx* c = nullptr;
+    MB_CHECK(mcnla_b200_create(&c, device, st));
+    ctx.push_back(c);
+  }
+  for (int i = 0; i < count; ++i) {
+    problems[i].status = -1;
+    problems[i].iteration = 0;
+    problems[i].seconds = 0;
+    problems[i].latency = 0;
+  }
+  // ---- partition; grouped problems largest first (the work queue's order)
+  std::vector<GItem> items;
+  std::vector<int> others;
+  for (int i = 0; i < count; ++i) {
+    if (grouped_eligible(ctx[0], problems[i])) {
+      GItem it;
+      it.p = &problems[i];
+      problem_check(problems[i], it.d);
+      items.push_back(it);
+    } else {
+      others.push_back(i);
+    }
+  }
+  auto cost = [](const GItem& it) { return double(it.d.L) * double(it.d.L) * double(it.d.l); };
+  std::stable_sort(items.begin(), items.end(), [&](const GItem& a, const GItem& b) { return cost(a) > cost(b); });
+  // ---- waves within the budget (besides the workers' own workspaces and scratch)
+  size_t worker_bytes = 0;
+  for (auto& it : items) {
+    worker_bytes = std::max(worker_bytes, problem_scratch_bytes(*it.p) + size_t(it.d.m) * it.d.L * 8 +
+                                              gkn_ws_bytes(ctx[0], it.d) + (size_t(64) << 20));
+  }
+  const int64_t wave_cap = std::max<int64_t>(1, budget - int64_t(worker_bytes) * workers);
+  size_t pos = 0;
+  while (pos < items.size()) {
+    size_t end = pos, bytes = 0;
+    while (end < items.size()) {
+      const size_t b = gitem_bytes(ctx[0], items[end].d, problem_mixed(*items[end].p));
+      if (end > pos && int64_t(bytes + b) > wave_cap) break;
+      bytes += b;
+      ++end;
+    }
+    void* arena = nullptr;
+    MB_CHECK_CUDA(cudaMallocAsync(&arena, bytes + 4096, ctx[0]->stream));
+    MB_CHECK_CUDA(cudaStreamSynchronize(ctx[0]->stream));
+    struct Arena { Context* c; void* p; ~Arena() { cudaFreeAsync(p, c->stream); cudaStreamSynchronize(c->stream); } }
+        wave_arena{ctx[0], arena};
+    char* base = static_cast<char*>(arena);
+    size_t top = 0;
+    auto take = [&](size_t count_, size_t elem) -> char* {
+      const size_t off = (top + 255) & ~size_t(255);
+      top = off + count_ * elem + 256;
+      return base + off;
+    };
+    std::vector<GItem*> wave;
+    for (size_t i = pos; i < end; ++i) {
+      GItem& it = items[i];
+      const int64_t ldo = (it.d.n + 7) & ~int64_t(7);
+      it.Q = reinterpret_cast<double*>(take(size_t(it.d.m) * it.d.L, 8));
+      it.Qbar = reinterpret_cast<double*>(take(size_t(it.d.m) * it.d.l, 8));
+      if (problem_mixed(*it.p)) it.omega_t = reinterpret_cast<uint16_t*>(take(size_t(it.d.L) * ldo, 2));
+      else it.omega = reinterpret_cast<double*>(take(size_t(it.d.n) * it.d.L, 8));
+      gkn_carve(ctx[0], it.d, take, it.b);
+      wave.push_back(&it);
+    }
+    parallel_for(device, workers, int(wave.size()), [&](int w, int i) {
+      GItem& it = *wave[size_t(i)];
+      const auto ta = Clock::now();
+      it.status = gitem_phase_a(ctx[size_t(w)], it, scratch[size_t(w)]);
+      it.seconds += std::chrono::duration<double>(Clock::now() - ta).count();
+    });
+    MB_CHECK(grouped_rounds(device, ctx, wave));
+    parallel_for(device, workers, int(wave.size()), [&](int w, int i) {
+      GItem& it = *wave[size_t(i)];
+      const auto tc = Clock::now();
+      if (it.status == MCNLA_B200_OK) it.status = gitem_phase_c(ctx[size_t(w)], it, scratch[size_t(w)]);
+      it.seconds += std::chrono::duration<double>(Clock::now() - tc).count();
+      mcnla_b200_problem& p = *it.p;
+      p.status = it.status;
+      p.iteration = it.iters;
+      p.seconds = it.seconds;
+      p.latency = std::chrono::duration<double>(Clock::now() - t0).count();
+    });
+    pos = end;
+  }
+  // ---- the rest: whole solves on the workers
+  parallel_for(device, workers, int(others.size()), [&](int w, int i) {
+    mcnla_b200_problem& p = problems[others[size_t(i)]];
+    Context* c = ctx[size_t(w)];
+    const auto ts = Clock::now();
+    int st = solve_problem(c, p, scratch[size_t(w)]);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess && st == MCNLA_B200_OK) st = MCNLA_B200_ERR_CUDA;
+    p.status = st;
+    p.seconds = std::chrono::duration<double>(Clock::now() - ts).count();
+    p.latency = std::chrono::duration<double>(Clock::now() - t0).count();
+  });
+  int first = MCNLA_B200_OK;
+  for (int i = 0; i < count; ++i)
+    if (problems[i].status != MCNLA_B200_OK && first == MCNLA_B200_OK) first = problems[i].status;
+  return first;
+}
+
 }  // namespace mb
 
 using mb::Context;

@@ -746,10 +746,13 @@ def solve_mixed(a, k, p, N, seed=0, integrator="kn", former="svd", maxit=256, to
 class Request:
     """One solve for the server: A (CUDA float64 or float32, row- or column-major) and its
     parameters; the outputs S, U, V are allocated here on A's device.  mixed: False (FP64),
-    True or 2 (BF16 hi+lo sketch) or 3 (BF16 hi+lo+lo2 sketch)."""
+    True or 2 (BF16 hi+lo sketch) or 3 (BF16 hi+lo+lo2 sketch); the mixed solves run the
+    precision former from three BF16 parts of A'.  split / former_split: resident BF16 parts of
+    A and of A' (split_bf16(a, parts), split_bf16(a.t(), 3)) kept by the caller; without them
+    each solve splits A itself."""
 
     def __init__(self, a, k, p, N, seed=0, integrator="kn", former="svd", maxit=256, tol=1e-4, mixed=False,
-                 with_v=True):
+                 with_v=True, split=None, former_split=None):
         if not isinstance(a, torch.Tensor) or not a.is_cuda or a.dtype not in (torch.float64, torch.float32):
             raise TypeError("A must be a CUDA float64 or float32 tensor")
         layout, lda = _layout(a)
@@ -781,6 +784,15 @@ class Request:
         pr.S = self.s.data_ptr()
         pr.U = self.u.data_ptr()
         pr.V = self.v.data_ptr() if self.v is not None else None
+        # resident BF16 parts of A (sketch) and of A' (precision former), split once by the caller
+        self._keep = (split, former_split)
+        if split is not None:
+            pr.a_hi, pr.a_lo = split.hi.data_ptr(), split.lo.data_ptr()
+            pr.a_lo2 = split.lo2.data_ptr() if split.lo2 is not None else None
+            pr.lda16 = split.ld
+        if former_split is not None:
+            pr.at_hi, pr.at_lo, pr.at_lo2 = (t.data_ptr() for t in former_split[:3])
+            pr.ldat16 = former_split.ld
         self.problem = pr
         self.ticket = None
         self.result = None

@@ -37,7 +37,8 @@ def _alone(req):
     args = dict(seed=pr.seed, integrator=integ, former="svd", maxit=pr.max_iteration, tol=pr.tolerance)
     k, p, N = pr.params.rank, pr.params.over_rank, pr.params.num_sketch
     if pr.precision in (1, 2):
-        return isvd.solve_mixed(a, k, p, N, parts=pr.precision + 1, **args)
+        # the served mixed solve: the precision former from three BF16 parts of A'
+        return isvd.solve_mixed(a, k, p, N, parts=pr.precision + 1, former_split=isvd.split_bf16(a.t(), 3), **args)
     return isvd.solve(a, k, p, N, **args)
 
 
