@@ -376,6 +376,12 @@ MCNLA_B200_API int mcnla_b200_server_destroy(mcnla_b200_server* server);
  * (each problem's own status is in problems[i].status).                      */
 MCNLA_B200_API int mcnla_b200_isvd_batched(int device, mcnla_b200_problem* problems, int count, int workers,
                                            int64_t budget_bytes);
+/* Host seconds of the phases of the last mcnla_b200_isvd_batched call in this
+ * process: [0] sketch / orthogonalizer / Gramian of the grouped problems, [1]
+ * the grouped integrator kernels, [2] the iterations they handed back, [3]
+ * Qbar and the formers, [4] the other problems' whole solves.  Returns the
+ * number of phases (5); writes at most capacity.                            */
+MCNLA_B200_API int mcnla_b200_batched_times(double* seconds, int capacity);
 
 /* ---- row-block decomposition over several GPUs -------------------------------
  * The reference's MPI decomposition of one solve (src/isvd_dense_rb.cpp:118-221

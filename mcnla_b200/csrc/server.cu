@@ -224,4 +224,9 @@ int mcnla_b200_isvd_batched(int device, mcnla_b200_problem* problems, int count,
   return mb::batched_solve(device, problems, count, workers, budget_bytes);
 }
 
+int mcnla_b200_batched_times(double* seconds, int capacity) {
+  if (!seconds && capacity > 0) return -MCNLA_B200_ERR_ARG;
+  return mb::batched_times(seconds, capacity);
+}
+
 }  // extern "C"

@@ -24,5 +24,8 @@ size_t problem_scratch_bytes(const mcnla_b200_problem& p);
 int solve_problem(Context* c, mcnla_b200_problem& p, SolveScratch& s);
 // mcnla_b200_isvd_batched.
 int batched_solve(int device, mcnla_b200_problem* problems, int count, int workers, int64_t budget);
+// Host seconds of the last batch's phases (mcnla_b200_batched_times).
+constexpr int kBatchPhases = 5;
+int batched_times(double* seconds, int capacity);
 
 }  // namespace mb

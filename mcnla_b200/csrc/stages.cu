@@ -19,6 +19,7 @@
 #include <chrono>
 #include <climits>
 #include <cmath>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -1481,7 +1482,8 @@ using Clock = std::chrono::steady_clock;
 // The grouped integrator over the wave's problems: per round one launch per
 // cluster size (on the first workers' streams, side by side), then the
 // declined iterations on the workers.
-int grouped_rounds(int device, std::vector<Context*>& ctx, std::vector<GItem*>& items) {
+int grouped_rounds(int device, std::vector<Context*>& ctx, std::vector<GItem*>& items, double* t_kernel,
+                   double* t_fallback) {
   Context* c0 = ctx[0];
   const int n = int(items.size());
   if (n == 0) return MCNLA_B200_OK;
@@ -1517,6 +1519,7 @@ int grouped_rounds(int device, std::vector<Context*>& ctx, std::vector<GItem*>& 
       while (i < np && cls(*pending[size_t(i)]) == k) ++i;
       first[k] = i;
     }
+    const auto tk = Clock::now();
     MB_CHECK_CUDA(cudaMemcpyAsync(jobs_dev, jobs.data(), sizeof(GknJob) * np, cudaMemcpyHostToDevice, c0->stream));
     MB_CHECK_CUDA(cudaStreamSynchronize(c0->stream));
     int lane = 0;
@@ -1530,6 +1533,8 @@ int grouped_rounds(int device, std::vector<Context*>& ctx, std::vector<GItem*>& 
     for (int w = 0; w < std::min(lane, int(ctx.size())); ++w) MB_CHECK_CUDA(cudaStreamSynchronize(ctx[size_t(w)]->stream));
     MB_CHECK_CUDA(cudaMemcpyAsync(jobs.data(), jobs_dev, sizeof(GknJob) * np, cudaMemcpyDeviceToHost, c0->stream));
     MB_CHECK_CUDA(cudaStreamSynchronize(c0->stream));
+    *t_kernel += std::chrono::duration<double>(Clock::now() - tk).count();
+    const auto tf0 = Clock::now();
     std::vector<std::pair<GItem*, int>> fallback;
     for (int i = 0; i < np; ++i) {
       GItem& it = *pending[size_t(i)];
@@ -1555,6 +1560,7 @@ int grouped_rounds(int device, std::vector<Context*>& ctx, std::vector<GItem*>& 
         it.done = true;
       }
     });
+    *t_fallback += std::chrono::duration<double>(Clock::now() - tf0).count();
     pending.clear();
     for (auto* it : items)
       if (!it->done && it->status == MCNLA_B200_OK) pending.push_back(it);
@@ -1564,6 +1570,10 @@ int grouped_rounds(int device, std::vector<Context*>& ctx, std::vector<GItem*>& 
 
 }  // namespace
 
+// Host seconds of the phases of the last grouped batch (mcnla_b200_batched_times).
+std::mutex g_batch_times_mu;
+double g_batch_times[kBatchPhases] = {0, 0, 0, 0, 0};
+
 // The grouped batch (mcnla_b200_isvd_batched): problems the grouped kernel
 // takes (grouped_eligible) run in waves through phases A / grouped rounds / C
 // on `workers` contexts; the others run whole solves through a worker pool.
@@ -1571,6 +1581,8 @@ int batched_solve(int device, mcnla_b200_problem* problems, int count, int worke
   if (count < 0 || (count > 0 && !problems) || workers < 1 || workers > 256 || budget <= 0) return MCNLA_B200_ERR_ARG;
   MB_CHECK_CUDA(cudaSetDevice(device));
   const auto t0 = Clock::now();
+  double phase[kBatchPhases] = {0, 0, 0, 0, 0};
+  auto since = [](Clock::time_point t) { return std::chrono::duration<double>(Clock::now() - t).count(); };
   std::vector<Context*> ctx;
   std::vector<cudaStream_t> streams;
   std::vector<SolveScratch> scratch(static_cast<size_t>(workers));
@@ -1654,13 +1666,16 @@ int batched_solve(int device, mcnla_b200_problem* problems, int count, int worke
       gkn_carve(ctx[0], it.d, take, it.b);
       wave.push_back(&it);
     }
+    auto tp = Clock::now();
     parallel_for(device, workers, int(wave.size()), [&](int w, int i) {
       GItem& it = *wave[size_t(i)];
       const auto ta = Clock::now();
       it.status = gitem_phase_a(ctx[size_t(w)], it, scratch[size_t(w)]);
       it.seconds += std::chrono::duration<double>(Clock::now() - ta).count();
     });
-    MB_CHECK(grouped_rounds(device, ctx, wave));
+    phase[0] += since(tp);
+    MB_CHECK(grouped_rounds(device, ctx, wave, &phase[1], &phase[2]));
+    tp = Clock::now();
     parallel_for(device, workers, int(wave.size()), [&](int w, int i) {
       GItem& it = *wave[size_t(i)];
       const auto tc = Clock::now();
@@ -1672,9 +1687,11 @@ int batched_solve(int device, mcnla_b200_problem* problems, int count, int worke
       p.seconds = it.seconds;
       p.latency = std::chrono::duration<double>(Clock::now() - t0).count();
     });
+    phase[3] += since(tp);
     pos = end;
   }
   // ---- the rest: whole solves on the workers
+  const auto to = Clock::now();
   parallel_for(device, workers, int(others.size()), [&](int w, int i) {
     mcnla_b200_problem& p = problems[others[size_t(i)]];
     Context* c = ctx[size_t(w)];
@@ -1685,10 +1702,22 @@ int batched_solve(int device, mcnla_b200_problem* problems, int count, int worke
     p.seconds = std::chrono::duration<double>(Clock::now() - ts).count();
     p.latency = std::chrono::duration<double>(Clock::now() - t0).count();
   });
+  phase[4] = since(to);
+  {
+    std::lock_guard<std::mutex> lock(g_batch_times_mu);
+    for (int i = 0; i < kBatchPhases; ++i) g_batch_times[i] = phase[i];
+  }
   int first = MCNLA_B200_OK;
   for (int i = 0; i < count; ++i)
     if (problems[i].status != MCNLA_B200_OK && first == MCNLA_B200_OK) first = problems[i].status;
   return first;
+}
+
+int batched_times(double* seconds, int capacity) {
+  std::lock_guard<std::mutex> lock(g_batch_times_mu);
+  const int n = std::min(capacity, kBatchPhases);
+  for (int i = 0; i < n; ++i) seconds[i] = g_batch_times[i];
+  return kBatchPhases;
 }
 
 }  // namespace mb

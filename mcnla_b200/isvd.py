@@ -850,6 +850,17 @@ class Server:
             pass
 
 
+BATCH_PHASES = ("sketch_orthogonalize_gramian", "grouped_kernel", "declined_iterations", "qbar_former",
+                "other_problems")
+
+
+def batched_times():
+    """Host seconds of the phases of the last solve_batched call (BATCH_PHASES order)."""
+    buf = (ctypes.c_double * len(BATCH_PHASES))()
+    _lib.load().mcnla_b200_batched_times(buf, len(BATCH_PHASES))
+    return dict(zip(BATCH_PHASES, (round(buf[i], 4) for i in range(len(BATCH_PHASES)))))
+
+
 def solve_batched(requests, workers=4, budget_bytes=150 << 30):
     """All requests through one temporary pool (mcnla_b200_isvd_batched)."""
     if not requests:
