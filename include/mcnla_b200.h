@@ -376,11 +376,13 @@ MCNLA_B200_API int mcnla_b200_server_destroy(mcnla_b200_server* server);
  * (each problem's own status is in problems[i].status).                      */
 MCNLA_B200_API int mcnla_b200_isvd_batched(int device, mcnla_b200_problem* problems, int count, int workers,
                                            int64_t budget_bytes);
-/* Host seconds of the phases of the last mcnla_b200_isvd_batched call in this
- * process: [0] sketch / orthogonalizer / Gramian of the grouped problems, [1]
- * the grouped integrator kernels, [2] the iterations they handed back, [3]
- * Qbar and the formers, [4] the other problems' whole solves.  Returns the
- * number of phases (5); writes at most capacity.                            */
+/* Seconds of the phases of the last mcnla_b200_isvd_batched call in this
+ * process (host clock): [0] sketch / orthogonalizer / Gramian of the grouped
+ * problems, [1] the grouped integrator kernels, [2] the iterations they handed
+ * back, [3] Qbar and the formers, [4] the other problems' whole solves; and
+ * (device clock, summed over the grouped problems) [5] Bs Bc, [6] [Dc | Dgc],
+ * [7] the KN step, [8] the E~ and B updates.  Returns the number of entries
+ * (9); writes at most capacity.                                              */
 MCNLA_B200_API int mcnla_b200_batched_times(double* seconds, int capacity);
 
 /* ---- row-block decomposition over several GPUs -------------------------------

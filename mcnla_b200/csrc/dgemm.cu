@@ -517,4 +517,31 @@ int dgemm(Context* ctx, int64_t M, int64_t N, int64_t K, double alpha, CMat A, C
   return run_plan(ctx, g, batch.count, p, AK, BKM, vec2);
 }
 
+int dgemm_rows_in_place(Context* ctx, int64_t M, int64_t N, int64_t K, CMat A, CMat B, DMat Cm, GemmBatch batch) {
+  if (M < 0 || N < 0 || K < 0 || batch.count < 1) return MCNLA_B200_ERR_SHAPE;
+  if (M == 0 || N == 0) return MCNLA_B200_OK;
+  bool AK, BKM;
+  if (A.cs == 1) AK = true; else if (A.rs == 1) AK = false; else return MCNLA_B200_ERR_LAYOUT;
+  if (B.cs == 1) BKM = false; else if (B.rs == 1) BKM = true; else return MCNLA_B200_ERR_LAYOUT;
+  const int64_t lda = AK ? A.rs : A.cs;
+  const int64_t ldb = BKM ? B.cs : B.rs;
+  auto al16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+  const bool vec2 = al16(A.p) && al16(B.p) && (lda % 2 == 0 || (AK ? M == 1 : K == 1)) &&
+                    (ldb % 2 == 0 || (BKM ? N == 1 : K == 1)) && batch.a % 2 == 0 && batch.b % 2 == 0;
+  const Plan p = prefer_two_cta(make_plan(ctx, M, N, K, batch.count, 1), AK, BKM, M, N);
+  // one CTA per row panel: it reads all of its rows' K before its epilogue writes them
+  if (p.bn < N || p.splits != 1) return MCNLA_B200_ERR_UNSUPPORTED;
+  KArgs g;
+  g.M = M; g.N = N; g.K = K; g.alpha = 1.0; g.beta = 0.0;
+  g.A = A.p; g.a_rs = A.rs; g.a_cs = A.cs; g.a_bs = batch.a;
+  g.B = B.p; g.b_rs = B.rs; g.b_cs = B.cs; g.b_bs = batch.b;
+  g.C = Cm.p; g.c_rs = Cm.rs; g.c_cs = Cm.cs; g.c_bs = batch.c;
+  g.splits = 1; g.kps = p.kps;
+  g.ws = nullptr;
+  g.guard_stop = ctx->guard_stop;
+  g.guard_it = ctx->guard_it;
+  g.lower = 0;
+  return run_plan(ctx, g, batch.count, p, AK, BKM, vec2);
+}
+
 }  // namespace mb

@@ -36,4 +36,12 @@ int dgemm_heuristic_splits(const Context* c, int64_t M, int64_t N, int64_t K, in
 int dgemm(Context* ctx, int64_t M, int64_t N, int64_t K, double alpha, CMat A, CMat B, double beta, DMat C,
           GemmBatch batch = GemmBatch(), double* ws = nullptr, int force_splits = 0, bool lower_only = false);
 
+// C := A B where C holds the same rows as A (an in-place update of A's row
+// panels, e.g. Q_i := Q_i T_i): run only when one CTA covers all N output
+// columns of its rows with no split-K, so that it has read its rows of A
+// before it writes them; otherwise MCNLA_B200_ERR_UNSUPPORTED (nothing runs).
+// The element arithmetic is that of dgemm() with the same shape.
+int dgemm_rows_in_place(Context* ctx, int64_t M, int64_t N, int64_t K, CMat A, CMat B, DMat C,
+                        GemmBatch batch = GemmBatch());
+
 }  // namespace mb

@@ -44,7 +44,7 @@ constexpr int kUnitMaxRows = 64;
 constexpr int kUnitMaxCols = 128;
 constexpr int kLdA = kUnitK + 4;        // A stage: row r at r * kLdA (conflict-free fragment reads)
 constexpr int kLdB = kUnitMaxCols + 8;  // B stage: k-row at k * kLdB
-constexpr int kStageDoubles = kUnitMaxRows * kLdA + kUnitK * kLdB;
+constexpr int kStageDoubles = kUnitMaxRows * (kLdA + 1) + kUnitK * kLdB;
 constexpr int kDdSlice = 256;           // K slice of the [Dc | Dgc] product
 
 __host__ __device__ constexpr size_t unit_smem_doubles() { return 2 * size_t(kStageDoubles); }
@@ -55,22 +55,28 @@ __device__ __forceinline__ void cluster_sync(const cg::cluster_group& cl) { cl.s
 // (R <= 64, Cn <= 128), written through fo(r0 + r, c0 + c, value).  A(i, k) at
 // A[i * ars + k * acs], B(k, j) at B[k * brs + j * bcs] (global memory, read
 // through L2: other CTAs of the cluster may have written them).  sm:
-// unit_smem_doubles().  Begins and ends with a block barrier.
+// unit_smem_doubles().  Begins and ends with a block barrier.  Every element is
+// one chain of MMA steps over k in ascending order, whatever R, Cn and the CTA.
 template <class FO>
 __device__ void gemm_unit(const double* A, int64_t ars, int64_t acs, const double* B, int64_t brs, int64_t bcs,
                           int r0, int R, int c0, int Cn, int k0, int k1, double* sm, FO fo) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int g = lane >> 2, t4 = lane & 3;
-  const int wt_rows = (R + 15) >> 4, wt_cols = (Cn + 15) >> 4, nwt = wt_rows * wt_cols;
-  double acc[4][2][2][2];
+  // 2 x 4 warps of 32 x 32 (4 x 4 MMA tiles of 8 x 8) over the unit's at most 64 x 128 outputs.
+  // The stages hold the 32-aligned extents Rp x 32 and 32 x Cp, zeros past R / Cn.
+  const int Rp = (R + 31) & ~31, Cp = (Cn + 31) & ~31;
+  const int wr = (warp >> 2) * 32, wc = (warp & 3) * 32;
+  const bool active = wr < Rp && wc < Cp;
+  double acc[4][4][2];
 #pragma unroll
-  for (int q = 0; q < 4; ++q)
+  for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-      for (int j = 0; j < 2; ++j) acc[q][i][j][0] = acc[q][i][j][1] = 0.0;
-  const int nA = R * kUnitK, nB = kUnitK * Cn;
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  const int nA = Rp * kUnitK, nB = kUnitK * Cp;
   const bool a_k_contig = acs == 1;
+  // A staged k-contiguous: row r at r * ldA.  With A's rows contiguous in memory instead, threads
+  // walk r fastest (coalesced reads) and an odd stride keeps their stores off each other's banks.
+  const int ldA = a_k_contig ? kLdA : kLdA + 1;
   constexpr int kAPer = kUnitMaxRows * kUnitK / kGThreads;    // 8
   constexpr int kBPer = kUnitK * kUnitMaxCols / kGThreads;    // 16
   double reg[kAPer + kBPer];
@@ -81,41 +87,38 @@ __device__ void gemm_unit(const double* A, int64_t ars, int64_t acs, const doubl
       const int e = tid + q * kGThreads;
       if (e < nA) {
         int r, k;
-        if (a_k_contig) { r = e / kUnitK; k = e % kUnitK; } else { k = e / R; r = e % R; }
+        if (a_k_contig) { r = e / kUnitK; k = e % kUnitK; } else { k = e / Rp; r = e % Rp; }
         const int kk = kc + k;
-        reg[q] = kk < k1 ? __ldcg(A + int64_t(r0 + r) * ars + int64_t(kk) * acs) : 0.0;
+        reg[q] = (kk < k1 && r < R) ? __ldcg(A + int64_t(r0 + r) * ars + int64_t(kk) * acs) : 0.0;
       }
     }
 #pragma unroll
     for (int q = 0; q < kBPer; ++q) {
       const int e = tid + q * kGThreads;
       if (e < nB) {
-        const int k = e / Cn, cc = e % Cn, kk = kc + k;
-        reg[kAPer + q] = kk < k1 ? __ldcg(B + int64_t(kk) * brs + int64_t(c0 + cc) * bcs) : 0.0;
+        const int k = e / Cp, cc = e % Cp, kk = kc + k;
+        reg[kAPer + q] = (kk < k1 && cc < Cn) ? __ldcg(B + int64_t(kk) * brs + int64_t(c0 + cc) * bcs) : 0.0;
       }
     }
   };
   auto stash = [&](double* st) {
     double* As = st;
-    double* Bs = st + kUnitMaxRows * kLdA;
+    double* Bs = st + kUnitMaxRows * (kLdA + 1);
 #pragma unroll
     for (int q = 0; q < kAPer; ++q) {
       const int e = tid + q * kGThreads;
       if (e < nA) {
         int r, k;
-        if (a_k_contig) { r = e / kUnitK; k = e % kUnitK; } else { k = e / R; r = e % R; }
-        As[r * kLdA + k] = reg[q];
+        if (a_k_contig) { r = e / kUnitK; k = e % kUnitK; } else { k = e / Rp; r = e % Rp; }
+        As[r * ldA + k] = reg[q];
       }
     }
 #pragma unroll
     for (int q = 0; q < kBPer; ++q) {
       const int e = tid + q * kGThreads;
-      if (e < nB) Bs[(e / Cn) * kLdB + e % Cn] = reg[kAPer + q];
+      if (e < nB) Bs[(e / Cp) * kLdB + e % Cp] = reg[kAPer + q];
     }
   };
-  // rows / columns of a stage past R / Cn are read by partial warp tiles: keep them zero
-  __syncthreads();
-  for (int e = tid; e < 2 * kStageDoubles; e += kGThreads) sm[e] = 0.0;
   __syncthreads();
   const int nchunks = (k1 - k0 + kUnitK - 1) / kUnitK;
   if (nchunks > 0) {
@@ -127,22 +130,19 @@ __device__ void gemm_unit(const double* A, int64_t ars, int64_t acs, const doubl
     const double* st = sm + (ch & 1) * kStageDoubles;
     if (ch + 1 < nchunks) fetch(k0 + (ch + 1) * kUnitK);
     const double* As = st;
-    const double* Bs = st + kUnitMaxRows * kLdA;
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int wt = warp + q * 8;
-      if (wt >= nwt) break;
-      const int wr = (wt / wt_cols) * 16, wc = (wt % wt_cols) * 16;
+    const double* Bs = st + kUnitMaxRows * (kLdA + 1);
+    if (active) {
 #pragma unroll
       for (int ks = 0; ks < kUnitK; ks += 4) {
-        const double a0 = As[(wr + g) * kLdA + ks + t4];
-        const double a1 = As[(wr + 8 + g) * kLdA + ks + t4];
-        const double b0 = Bs[(ks + t4) * kLdB + wc + g];
-        const double b1 = Bs[(ks + t4) * kLdB + wc + 8 + g];
-        dmma(acc[q][0][0][0], acc[q][0][0][1], a0, b0);
-        dmma(acc[q][0][1][0], acc[q][0][1][1], a0, b1);
-        dmma(acc[q][1][0][0], acc[q][1][0][1], a1, b0);
-        dmma(acc[q][1][1][0], acc[q][1][1][1], a1, b1);
+        double a[4], b[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] = As[(wr + 8 * i + g) * ldA + ks + t4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) b[j] = Bs[(ks + t4) * kLdB + wc + 8 * j + g];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
       }
     }
     if (ch + 1 < nchunks) {
@@ -152,29 +152,18 @@ __device__ void gemm_unit(const double* A, int64_t ars, int64_t acs, const doubl
     }
     __syncthreads();
   }
+  if (active) {
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const int wt = warp + q * 8;
-    if (wt >= nwt) break;
-    const int wr = (wt / wt_cols) * 16, wc = (wt % wt_cols) * 16;
+    for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-      for (int j = 0; j < 2; ++j)
+      for (int j = 0; j < 4; ++j)
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           const int r = wr + 8 * i + g, cc = wc + 8 * j + 2 * t4 + h;
-          if (r < R && cc < Cn) fo(r0 + r, c0 + cc, acc[q][i][j][h]);
+          if (r < R && cc < Cn) fo(r0 + r, c0 + cc, acc[i][j][h]);
         }
   }
   __syncthreads();
-}
-
-// Unit rows for an M-row product spread over `ncta` CTAs: 64, or 32 when that
-// gives the CTAs a more even share (the arithmetic does not depend on it).
-__device__ __forceinline__ int unit_rows(int M, int ncta) {
-  const int u64 = (M + 63) / 64;
-  return (u64 % ncta == 0 || u64 >= 4 * ncta) ? 64 : 32;
 }
 
 // The KN step of kn_series_step with its 8-row blocks spread over the
@@ -532,13 +521,24 @@ __global__ void __launch_bounds__(kGThreads, 1) k_gkn_grouped(GknJob* jobs, int 
     const double inv_n = a.inv_n;
     int stop = INT_MAX, resume = -1, degree = 0;
     double norm = 0.0;
+    long long ph[4] = {0, 0, 0, 0};
+    auto stamp = [&](int i, long long& t) {   // rank 0 accumulates the phases' wall time
+      if (rank == 0 && tid == 0) {
+        long long now;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+        if (i >= 0) ph[i] += now - t;
+        t = now;
+      }
+    };
+    long long tph = 0;
+    stamp(-1, tph);
     for (int it = a.it0; it < a.maxit; ++it) {
       const int cur = it & 1;
       double* E = cur ? a.eb1 : a.eb0;                   // [E~c | Bc | Bgc]
       double* En = cur ? a.eb0 : a.eb1;
       // P1: Bgc := 1/N Bs Bc   (row panels x column panels of at most 128)
       {
-        const int R = unit_rows(L, ncta), rp = (L + R - 1) / R, cp = (l + kUnitMaxCols - 1) / kUnitMaxCols;
+        const int R = kUnitMaxRows, rp = (L + R - 1) / R, cp = (l + kUnitMaxCols - 1) / kUnitMaxCols;
         const int cw = (l + cp - 1) / cp;
         for (int u = rank; u < rp * cp; u += ncta) {
           const int r0 = (u / cp) * R, c0 = (u % cp) * cw;
@@ -547,6 +547,7 @@ __global__ void __launch_bounds__(kGThreads, 1) k_gkn_grouped(GknJob* jobs, int 
         }
       }
       cluster_sync(cl);
+      stamp(0, tph);
       // P2: [Dc | Dgc] := 1/N Bc' [Bc | Bgc]: partial sums over K slices of 256 into
       // the slices buffer, then the slices added in order
       {
@@ -569,6 +570,7 @@ __global__ void __launch_bounds__(kGThreads, 1) k_gkn_grouped(GknJob* jobs, int 
         }
       }
       cluster_sync(cl);
+      stamp(1, tph);
       // P3: KN step (C, inv(C), Fc, F~+) by power series
       SeriesArgs s;
       s.l = l;
@@ -584,13 +586,15 @@ __global__ void __launch_bounds__(kGThreads, 1) k_gkn_grouped(GknJob* jobs, int 
       s.partials = a.work + 2 * size_t(l) * l;
       s.scal = nullptr;
       s.smax = a.smax;
-      if (kn_series_step_cluster(s, sm, a.cbuf, cl, rank, ncta, &norm, &degree) == kStepDeclined) {
+      const int step = kn_series_step_cluster(s, sm, a.cbuf, cl, rank, ncta, &norm, &degree);
+      stamp(2, tph);
+      if (step == kStepDeclined) {
         resume = it;
         break;
       }
       // P4: E~+ := [E~c Bc] [Fc; inv(C)/N];  B+ := [Bc Bgc] [Fc; inv(C)]
       {
-        const int R = unit_rows(2 * L, ncta), rp = (L + R - 1) / R, cp = (l + kUnitMaxCols - 1) / kUnitMaxCols;
+        const int R = kUnitMaxRows, rp = (L + R - 1) / R, cp = (l + kUnitMaxCols - 1) / kUnitMaxCols;
         const int cw = (l + cp - 1) / cp;
         for (int u = rank; u < 2 * rp * cp; u += ncta) {
           const int which = u / (rp * cp), rc = u % (rp * cp);
@@ -603,6 +607,7 @@ __global__ void __launch_bounds__(kGThreads, 1) k_gkn_grouped(GknJob* jobs, int 
         }
       }
       cluster_sync(cl);
+      stamp(3, tph);
       if (!(norm >= a.tol)) {                            // the same norm in every CTA
         stop = it;
         break;
@@ -616,6 +621,7 @@ __global__ void __launch_bounds__(kGThreads, 1) k_gkn_grouped(GknJob* jobs, int 
       a.norm = norm;
       a.degree = degree;
       a.ns = t_end - t_start;
+      for (int i = 0; i < 4; ++i) a.phase_ns[i] = ph[i];
     }
     cluster_sync(cl);
   }

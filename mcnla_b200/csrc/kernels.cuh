@@ -59,6 +59,7 @@ struct GknJob {
   double norm;
   int degree, pad1;
   long long ns;     // out: nanoseconds the cluster spent on the job (device global timer)
+  long long phase_ns[4];   // out: of which in P1 (Bs Bc), P2 ([Dc | Dgc]), the KN step, P4 (E~+, B+)
 };
 // Largest N l the grouped kernel takes (beyond it the launch-per-product loop's
 // shared-memory-pipelined GEMMs are faster).

@@ -25,7 +25,7 @@ int solve_problem(Context* c, mcnla_b200_problem& p, SolveScratch& s);
 // mcnla_b200_isvd_batched.
 int batched_solve(int device, mcnla_b200_problem* problems, int count, int workers, int64_t budget);
 // Host seconds of the last batch's phases (mcnla_b200_batched_times).
-constexpr int kBatchPhases = 5;
+constexpr int kBatchPhases = 9;
 int batched_times(double* seconds, int capacity);
 
 }  // namespace mb

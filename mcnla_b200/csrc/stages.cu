@@ -135,9 +135,16 @@ int run_orthogonalize(Context* c, const Dims& d, double* Q) {
   MB_CHECK(launch_syev(c, l, N, W, l, int64_t(ll), S, V, 1));
   // T_i := V_i diag(S_i)^(-1/2)   (:94-99)
   MB_CHECK(launch_scale_cols_rsqrt(c, l, N, V, S, T));
-  // Q_i := tmp_i T_i   (:97-101, the reference also copies Q to a temporary first)
-  MB_CHECK_CUDA(cudaMemcpyAsync(tmp, Q, size_t(m) * L * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-  MB_CHECK(dgemm(c, m, l, l, 1.0, crow(tmp, L), crow(T, l), 0.0, drow(Q, L), GemmBatch{N, l, int64_t(ll), l}, ws));
+  // Q_i := Q_i T_i in place: each CTA reads its rows of Q_i before it writes them (the reference
+  // copies Q to a temporary first, :97-101; that copy remains for the shapes where one CTA cannot
+  // own whole row panels)
+  const int st = dgemm_rows_in_place(c, m, l, l, crow(Q, L), crow(T, l), drow(Q, L), GemmBatch{N, l, int64_t(ll), l});
+  if (st == MCNLA_B200_ERR_UNSUPPORTED) {
+    MB_CHECK_CUDA(cudaMemcpyAsync(tmp, Q, size_t(m) * L * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    MB_CHECK(dgemm(c, m, l, l, 1.0, crow(tmp, L), crow(T, l), 0.0, drow(Q, L), GemmBatch{N, l, int64_t(ll), l}, ws));
+  } else {
+    MB_CHECK(st);
+  }
   MB_CHECK(ctx_toc(c));
   return MCNLA_B200_OK;
 }
@@ -482,11 +489,12 @@ void gkn_carve(const Context* c, const Dims& d, Take take, GknBufs& b) {
   b.job = reinterpret_cast<double*>(p[16]);
 }
 
-// Cluster size of the grouped kernel for a problem: more CTAs as the
-// iteration's products grow (the results do not depend on it).
+// Cluster size of the grouped kernel for a problem: about three 64-row units
+// of the Bs Bc product per CTA (fuller units keep the FP64 MMA busier than more
+// CTAs would; the results do not depend on it).
 int gkn_cluster_for(int l, int64_t L) {
-  const double w = 2.0 * double(L) * double(L) * l;   // flops of Bs Bc per iteration
-  return w < 4e6 ? 1 : (w < 2e7 ? 2 : (w < 8e7 ? 4 : 8));
+  const int64_t units = ((L + 63) / 64) * ((l + 127) / 128);
+  return units <= 3 ? 1 : (units <= 7 ? 2 : (units <= 15 ? 4 : 8));
 }
 
 GknJob gkn_job(const Context* c, const Dims& d, const GknBufs& b, int it0, int maxit, double tol) {
@@ -1483,7 +1491,7 @@ using Clock = std::chrono::steady_clock;
 // cluster size (on the first workers' streams, side by side), then the
 // declined iterations on the workers.
 int grouped_rounds(int device, std::vector<Context*>& ctx, std::vector<GItem*>& items, double* t_kernel,
-                   double* t_fallback) {
+                   double* t_fallback, double* t_parts) {
   Context* c0 = ctx[0];
   const int n = int(items.size());
   if (n == 0) return MCNLA_B200_OK;
@@ -1540,6 +1548,7 @@ int grouped_rounds(int device, std::vector<Context*>& ctx, std::vector<GItem*>& 
       GItem& it = *pending[size_t(i)];
       const GknJob& j = jobs[size_t(i)];
       it.seconds += double(j.ns) * 1e-9;
+      for (int q = 0; q < 4; ++q) t_parts[q] += double(j.phase_ns[q]) * 1e-9;
       if (j.stop_it != INT_MAX) {
         it.done = true;
         it.iters = j.stop_it + 1;
@@ -1572,7 +1581,7 @@ int grouped_rounds(int device, std::vector<Context*>& ctx, std::vector<GItem*>& 
 
 // Host seconds of the phases of the last grouped batch (mcnla_b200_batched_times).
 std::mutex g_batch_times_mu;
-double g_batch_times[kBatchPhases] = {0, 0, 0, 0, 0};
+double g_batch_times[kBatchPhases] = {};
 
 // The grouped batch (mcnla_b200_isvd_batched): problems the grouped kernel
 // takes (grouped_eligible) run in waves through phases A / grouped rounds / C
@@ -1581,7 +1590,7 @@ int batched_solve(int device, mcnla_b200_problem* problems, int count, int worke
   if (count < 0 || (count > 0 && !problems) || workers < 1 || workers > 256 || budget <= 0) return MCNLA_B200_ERR_ARG;
   MB_CHECK_CUDA(cudaSetDevice(device));
   const auto t0 = Clock::now();
-  double phase[kBatchPhases] = {0, 0, 0, 0, 0};
+  double phase[kBatchPhases] = {};
   auto since = [](Clock::time_point t) { return std::chrono::duration<double>(Clock::now() - t).count(); };
   std::vector<Context*> ctx;
   std::vector<cudaStream_t> streams;
@@ -1674,7 +1683,7 @@ int batched_solve(int device, mcnla_b200_problem* problems, int count, int worke
       it.seconds += std::chrono::duration<double>(Clock::now() - ta).count();
     });
     phase[0] += since(tp);
-    MB_CHECK(grouped_rounds(device, ctx, wave, &phase[1], &phase[2]));
+    MB_CHECK(grouped_rounds(device, ctx, wave, &phase[1], &phase[2], &phase[5]));
     tp = Clock::now();
     parallel_for(device, workers, int(wave.size()), [&](int w, int i) {
       GItem& it = *wave[size_t(i)];

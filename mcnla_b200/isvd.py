@@ -851,11 +851,12 @@ class Server:
 
 
 BATCH_PHASES = ("sketch_orthogonalize_gramian", "grouped_kernel", "declined_iterations", "qbar_former",
-                "other_problems")
+                "other_problems", "kernel_bs_bc", "kernel_d_dg", "kernel_kn_step", "kernel_e_b_update")
 
 
 def batched_times():
-    """Host seconds of the phases of the last solve_batched call (BATCH_PHASES order)."""
+    """Seconds of the phases of the last solve_batched call (BATCH_PHASES order; the kernel_* entries are
+    the grouped kernel's device time summed over the problems)."""
     buf = (ctypes.c_double * len(BATCH_PHASES))()
     _lib.load().mcnla_b200_batched_times(buf, len(BATCH_PHASES))
     return dict(zip(BATCH_PHASES, (round(buf[i], 4) for i in range(len(BATCH_PHASES)))))
