@@ -621,23 +621,36 @@ def run_serving(args, dev):
 
     order = sorted(range(len(shapes)), key=lambda i: -shapes[i]["m"] * shapes[i]["n"] * shapes[i]["k"])
 
-    def timed_batch(workers, mixed):
+    def timed_batch(workers, mixed, grouped):
+        """grouped: the whole batch through mcnla_b200_isvd_batched (grouped integrator kernel);
+        else one worker pool of the server (per-request solves)."""
         reqs = [request(i, mixed) for i in range(len(shapes))]
-        with isvd.Server(workers=workers, budget_bytes=budget, device=dev) as srv:
-            warm = [request(i, mixed) for i in order[:2 * workers]]        # grow every worker's buffers
-            for r in warm:
-                srv.submit(r)
-            for r in warm:
-                srv.wait(r)
+        phases = None
+        if grouped:
+            isvd.solve_batched([request(i, mixed) for i in order[:64]], workers=workers, budget_bytes=budget)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            for r in reqs:
-                srv.submit(r)
-            for r in reqs:
-                srv.wait(r)
+            isvd.solve_batched(reqs, workers=workers, budget_bytes=budget)
             torch.cuda.synchronize()
             t = time.perf_counter() - t0
-            st = srv.stats()
+            phases = isvd.batched_times()
+            st = {"peak_bytes": 0}
+        else:
+            with isvd.Server(workers=workers, budget_bytes=budget, device=dev) as srv:
+                warm = [request(i, mixed) for i in order[:2 * workers]]        # grow every worker's buffers
+                for r in warm:
+                    srv.submit(r)
+                for r in warm:
+                    srv.wait(r)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                for r in reqs:
+                    srv.submit(r)
+                for r in reqs:
+                    srv.wait(r)
+                torch.cuda.synchronize()
+                t = time.perf_counter() - t0
+                st = srv.stats()
         bad = sum(1 for r in reqs if r.result.status != 0)
         its = [r.result.iteration for r in reqs]
         svc = [r.result.seconds for r in reqs]
@@ -647,11 +660,13 @@ def run_serving(args, dev):
                       "iterations_mean": round(float(np.mean(its)), 2), "iterations_max": int(max(its)),
                       "service_p50_ms": round(_pct(svc, 0.5) * 1e3, 3),
                       "service_p99_ms": round(_pct(svc, 0.99) * 1e3, 3),
-                      "peak_admitted_gb": round(st["peak_bytes"] / 1e9, 3)}
+                      "peak_admitted_gb": round(st["peak_bytes"] / 1e9, 3),
+                      "path": "grouped batch (mcnla_b200_isvd_batched)" if grouped else "server worker pool",
+                      "phases_s": phases}
 
-    _, serial64 = timed_batch(1, False)
-    _, batched64 = timed_batch(W, False)
-    mixed_reqs, batched_mx = timed_batch(W, args.serve_parts)
+    _, serial64 = timed_batch(1, False, False)
+    _, batched64 = timed_batch(W, False, True)
+    mixed_reqs, batched_mx = timed_batch(W, args.serve_parts, True)
 
     # accuracy of the mixed results against FP64 solves on the same A and Omega (BF16 Omega
     # drawn from the same seed, FP64 copy), and against FP64 dgesvd singular values of A

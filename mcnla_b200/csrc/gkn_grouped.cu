@@ -1,7 +1,8 @@
 // Grouped row-block Gramian Kolmogorov-Nagumo integrator: the iterations of
 // many independent problems of uneven sizes in one persistent launch over a
 // device work queue (row_block_gramian_kolmogorov_nagumo_integrator.hpp:137-214
-// for each problem).  The single solve runs the same kernel with one problem.
+// for each problem): the batch's throughput path.  A single solve instead
+// spreads one problem over the whole GPU (gkn_persistent.cu) for latency.
 //
 // The launch is a grid of thread-block clusters.  Each cluster takes the next
 // problem from the queue (one atomic add on a device counter; the host orders
@@ -20,8 +21,9 @@
 // cut into fixed slices of 256 whose partial sums are added in order
 // afterwards.  The KN step walks its 8-row blocks, block b on the cluster's
 // CTA b mod (cluster size).  No element's arithmetic depends on the cluster
-// size or on which CTA computes it, so a problem gives the same bits alone
-// and in any batch.  A declined iteration (usually the first) is recorded in
+// size or on which CTA computes it, so a problem gives the same bits in any
+// batch (and agrees with the single solve's differently ordered sums to
+// rounding).  A declined iteration (usually the first) is recorded in
 // the problem's resume field; the host runs it on the launch-per-product path
 // with the matrix-function / eigendecomposition step and queues the problem
 // again from the next iteration.  The only waits are cluster barriers among

@@ -42,9 +42,20 @@ size_t kn_series_work_doubles(int l);
 // large for the series; the launcher then runs the other form after it.
 int launch_kn_series(Context* c, int l, const double* z, const double* dd, double inv_n, double* out, double* outn,
                      const double* ff, double* ffn, double* work, double tol);
+// Persistent row-block Gramian KN integrator (gkn_persistent.cu): runs
+// iterations [it0, maxit) of one problem on one cooperative grid (the single
+// solve: lowest latency).  On return (after a stream sync) scal->stop_it is the
+// converged iteration, or scal->resume_it the iteration whose KN step the
+// series declined (to be run by the caller with allow_series = false), or
+// neither (maxit reached).  EB, FF, DD, FC, FCN, work: the buffers of the
+// launch-per-product loop.
+bool gkn_persistent_fits(const Context* c, int l, int64_t L);
+int launch_gkn_persistent(Context* c, int l, int64_t L, int N, double tol, int it0, int maxit, const double* Bs,
+                          double* const EB[2], double* const FF[2], double* DD, double* FC, double* FCN,
+                          double* work);
 // Grouped row-block Gramian KN integrator (gkn_grouped.cu): the iterations of
-// one or many problems, a cluster of CTAs per problem from a device work
-// queue.  A job's fields above stop_it are inputs (the buffers of the
+// many problems (a batch: highest throughput), a cluster of CTAs per problem
+// from a device work queue.  A job's fields above stop_it are inputs (the buffers of the
 // launch-per-product loop, plus cbuf: l x l doubles and ddp:
 // gkn_grouped_ddp_doubles of scratch); after the launch stop_it is the
 // converged iteration (INT_MAX: not converged), resume_it the iteration whose

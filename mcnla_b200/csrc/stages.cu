@@ -408,7 +408,7 @@ struct GknBufs {
   double* vwork = nullptr;    // KN step scratch
   double* cbuf = nullptr;     // l x l scratch of the grouped kernel's step
   double* ddp = nullptr;      // the grouped kernel's K-slice partials of [Dc | Dgc]
-  double* job = nullptr;      // device GknJob and work-queue counter of a single solve
+  double* job = nullptr;      // device GknJob and work-queue counter (the grouped kernel's single-job use)
   Bf16Split spb;
   bool bf16_bgc = false;
 };
@@ -597,24 +597,18 @@ int run_rb_gramian_kn(Context* c, const Dims& d, const double* Qs, int maxit, do
   MB_CHECK(ctx_toc(c));
   auto body = [&](int i, bool allow_series) -> int { return gkn_iteration(c, d, b, i, allow_series, tol, ws); };
   int it = 0;
-  if (c->kn_mode == MCNLA_B200_KN_AUTO && gkn_grouped_fits(c, l, L)) {
-    // whole iterations in the grouped kernel (one problem, one cluster); an
-    // iteration whose KN step the series declines runs here on the
-    // launch-per-product path
+  if (c->kn_mode == MCNLA_B200_KN_AUTO && gkn_persistent_fits(c, l, L)) {
+    // whole iterations on one cooperative grid; an iteration whose KN step the
+    // series declines runs here on the launch-per-product path
     MB_CHECK_CUDA(cudaMemsetAsync(&c->scal->stop_it, 0x7f, sizeof(int), c->stream));   // "not yet"
-    GknJob* jdev = reinterpret_cast<GknJob*>(b.job);
-    int* next = reinterpret_cast<int*>(reinterpret_cast<char*>(b.job) + sizeof(GknJob));
-    const size_t smem = gkn_grouped_smem(c, l);
-    const int cluster = gkn_cluster_for(l, L);
     int it0 = 0, done = -1;
     while (it0 < maxit && done < 0) {
-      GknJob j = gkn_job(c, d, b, it0, maxit, tol);
-      MB_CHECK_CUDA(cudaMemcpyAsync(jdev, &j, sizeof(GknJob), cudaMemcpyHostToDevice, c->stream));
-      MB_CHECK(launch_gkn_grouped(c, jdev, 1, next, smem, cluster));
-      MB_CHECK_CUDA(cudaMemcpyAsync(&j, jdev, sizeof(GknJob), cudaMemcpyDeviceToHost, c->stream));
-      MB_CHECK_CUDA(cudaStreamSynchronize(c->stream));
-      if (j.stop_it != INT_MAX) { done = j.stop_it + 1; break; }
-      const int r = j.resume_it;
+      MB_CHECK_CUDA(cudaMemsetAsync(&c->scal->resume_it, 0xff, sizeof(int), c->stream));   // -1
+      MB_CHECK(launch_gkn_persistent(c, l, L, d.N, tol, it0, maxit, b.Bs, b.EB, b.FF, b.DD, b.FC, b.FCN, b.vwork));
+      MB_CHECK(ctx_sync_scalars(c));
+      if (c->scal_host->status) return c->scal_host->status;
+      if (c->scal_host->stop_it < maxit) { done = c->scal_host->stop_it + 1; break; }
+      const int r = c->scal_host->resume_it;
       if (r < 0) break;                                       // maxit reached
       struct Reset { Context* c; ~Reset() { c->guard_stop = nullptr; c->guard_it = 0; } } reset{c};
       c->guard_stop = &c->scal->stop_it;
@@ -1373,15 +1367,18 @@ size_t gitem_bytes(const Context* c, const Dims& d, bool mixed) {
 }
 
 // A problem runs in the grouped batch when it uses the row-block Gramian KN
-// integrator on the path whose iterations the grouped kernel runs in a single
-// solve too (the default step method, N l <= 1536) with the FP64 Gramian.
+// integrator on the path whose iterations a single solve runs in one
+// persistent kernel too (the default step method, N l <= 1536) with the FP64
+// Gramian.  The grouped kernel sums each product in its own fixed order, so a
+// batch result matches the single solve to rounding (same iteration count).
 bool grouped_eligible(const Context* c, const mcnla_b200_problem& p) {
   Dims d;
   if (problem_check(p, d) != MCNLA_B200_OK) return false;
   if (p.integrator != MCNLA_B200_ROW_BLOCK_GRAMIAN_KOLMOGOROV_NAGUMO) return false;
   if (p.former < MCNLA_B200_SVD_FORMER || p.former > MCNLA_B200_COL_BLOCK_GRAMIAN_FORMER || d.k > d.l) return false;
   if (p.max_iteration < 0 || !(p.tolerance >= 0.0)) return false;
-  if (c->kn_mode != MCNLA_B200_KN_AUTO || !gkn_grouped_fits(c, d.l, d.L)) return false;
+  if (c->kn_mode != MCNLA_B200_KN_AUTO || !gkn_grouped_fits(c, d.l, d.L) || !gkn_persistent_fits(c, d.l, d.L))
+    return false;
   if (gkn_grouped_smem(c, d.l) == 0) return false;
   if (problem_mixed(p) && double(d.L) * double(d.L) * double(d.m) >= kMixedGramianMinFlops) return false;
   return true;

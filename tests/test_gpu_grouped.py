@@ -1,11 +1,12 @@
 """The grouped batch (mcnla_b200_isvd_batched): row-block Gramian Kolmogorov-Nagumo problems of
 uneven sizes go through the workers' sketch / orthogonalizer / Gramian phase, one grouped
-persistent kernel for every problem's iterations (one problem per CTA from a device work queue;
-the iterations the power series declines run on the workers in between), and the workers'
-Qbar / former phase.  Each problem takes the operations of its single solve, so the results
-must equal mcnla_b200_isvd / mcnla_b200_isvd_mixed bit for bit, with the same iteration count,
-and the FP64 ones must match the CPU oracle (1e-10 relative for sigma, 1e-10 for the singular
-vectors up to sign, identical iteration counts)."""
+persistent kernel for every problem's iterations (a cluster of CTAs per problem from a device
+work queue; the iterations the power series declines run on the workers in between), and the
+workers' Qbar / former phase.  Every stage but the iterations is the single solve's own; the
+grouped kernel sums its products in a fixed order of its own, so each result must match
+mcnla_b200_isvd / mcnla_b200_isvd_mixed to 1e-10 (sigma relative, singular vectors up to sign)
+with the same iteration count, be the same bits in any batch, and the FP64 ones must match the
+CPU oracle to 1e-10 with identical iteration counts."""
 import numpy as np
 import pytest
 import torch
@@ -47,17 +48,33 @@ def _alone(req):
     return isvd.solve(a, k, p, N, **args)
 
 
-def test_grouped_batch_equals_single_solves(cuda):
+def _close(got, ref, tol=1e-10):
+    s, u, v = (x.cpu().numpy() for x in got)
+    rs, ru, rv = (x.cpu().numpy() for x in ref)
+    np.testing.assert_allclose(s, rs, rtol=tol)
+    assert np.abs(O.align_signs(u, ru) - ru).max() < tol
+    assert np.abs(O.align_signs(v, rv) - rv).max() < tol
+
+
+def test_grouped_batch_matches_single_solves(cuda):
     from mcnla_b200 import isvd
     reqs = _problems(cuda, 24, seed=7)
     isvd.solve_batched(reqs, workers=4)
+    first = [(r.s.clone(), r.u.clone(), r.v.clone(), r.result.iteration) for r in reqs]
     for r in reqs:
         assert r.result.status == 0
         s, u, v, it = _alone(r)
         assert it == r.result.iteration, (it, r.result.iteration)
-        assert torch.equal(s, r.s), (s - r.s).abs().max().item()
-        assert torch.equal(u, r.u)
-        assert torch.equal(v, r.v)
+        _close((r.s, r.u, r.v), (s, u, v))
+    # the same problems in another batch (other neighbours, other order): the same bits
+    again = list(reversed(reqs[:10]))
+    for r in again:
+        r.s.zero_()
+    isvd.solve_batched(again, workers=3)
+    for r in again:
+        s0, u0, v0, it0 = first[reqs.index(r)]
+        assert r.result.iteration == it0
+        assert torch.equal(r.s, s0) and torch.equal(r.u, u0) and torch.equal(r.v, v0)
 
 
 def test_grouped_batch_matches_the_oracle(cuda):
@@ -100,9 +117,11 @@ def test_grouped_batch_waves_and_other_integrators(cuda):
         pr = r.problem
         if pr.integrator == isvd.INTEGRATORS["rb_gramian_kn"]:
             s, u, v, it = _alone(r)
-        else:
+            assert it == r.result.iteration
+            _close((r.s, r.u, r.v), (s, u, v))
+        else:                           # whole solves on the workers: the single solve's bits
             integ = {v_: k_ for k_, v_ in isvd.INTEGRATORS.items()}[pr.integrator]
             s, u, v, it = isvd.solve(r.a, pr.params.rank, pr.params.over_rank, pr.params.num_sketch, seed=pr.seed,
                                      integrator=integ, former="svd", tol=pr.tolerance)
-        assert it == r.result.iteration
-        assert torch.equal(s, r.s) and torch.equal(u, r.u)
+            assert it == r.result.iteration
+            assert torch.equal(s, r.s) and torch.equal(u, r.u)
