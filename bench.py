@@ -627,13 +627,13 @@ def run_serving(args, dev):
         reqs = [request(i, mixed) for i in range(len(shapes))]
         phases = None
         if grouped:
-            isvd.solve_batched([request(i, mixed) for i in order[:64]], workers=workers, budget_bytes=budget)
+            isvd.solve_grouped([request(i, mixed) for i in order[:64]], workers=workers, budget_bytes=budget)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            isvd.solve_batched(reqs, workers=workers, budget_bytes=budget)
+            isvd.solve_grouped(reqs, workers=workers, budget_bytes=budget)
             torch.cuda.synchronize()
             t = time.perf_counter() - t0
-            phases = isvd.batched_times()
+            phases = isvd.grouped_times()
             st = {"peak_bytes": 0}
         else:
             with isvd.Server(workers=workers, budget_bytes=budget, device=dev) as srv:
@@ -661,12 +661,14 @@ def run_serving(args, dev):
                       "service_p50_ms": round(_pct(svc, 0.5) * 1e3, 3),
                       "service_p99_ms": round(_pct(svc, 0.99) * 1e3, 3),
                       "peak_admitted_gb": round(st["peak_bytes"] / 1e9, 3),
-                      "path": "grouped batch (mcnla_b200_isvd_batched)" if grouped else "server worker pool",
+                      "path": "grouped batch (mcnla_b200_isvd_grouped)" if grouped else "worker pool (server)",
                       "phases_s": phases}
 
     _, serial64 = timed_batch(1, False, False)
-    _, batched64 = timed_batch(W, False, True)
-    mixed_reqs, batched_mx = timed_batch(W, args.serve_parts, True)
+    _, batched64 = timed_batch(W, False, False)
+    mixed_reqs, batched_mx = timed_batch(W, args.serve_parts, False)
+    _, grouped64 = timed_batch(W, False, True)
+    _, grouped_mx = timed_batch(W, args.serve_parts, True)
 
     # accuracy of the mixed results against FP64 solves on the same A and Omega (BF16 Omega
     # drawn from the same seed, FP64 copy), and against FP64 dgesvd singular values of A
@@ -757,6 +759,8 @@ def run_serving(args, dev):
                     % (len(shapes), args.serve_integrator, args.serve_former),
         "timing": "host wall clock, device synchronized on both sides; solves on the workers' own streams",
         "per_request_fp64": serial64, "batched_fp64": batched64, "batched_mixed": batched_mx,
+        "grouped_fp64": grouped64, "grouped_mixed": grouped_mx,
+        "grouped_mixed_speedup_vs_grouped_fp64": round(grouped_mx["solves_per_s"] / grouped64["solves_per_s"], 3),
         "mixed_speedup_vs_per_request_fp64": round(batched_mx["solves_per_s"] / serial64["solves_per_s"], 3),
         "mixed_speedup_vs_batched_fp64": round(batched_mx["solves_per_s"] / batched64["solves_per_s"], 3),
         "accuracy_mixed_vs_fp64_same_A_Omega": acc,
@@ -838,17 +842,17 @@ def run_kernel_case(args, dev):
         def reqs():
             return [isvd.Request(pool[i % len(pool)], k, k // 2, 8, seed=i, integrator="rb_gramian_kn",
                                  former="rb_gramian", maxit=args.maxit, tol=1e-5) for i in range(args.batch_count)]
-        isvd.solve_batched(reqs(), workers=args.serve_workers)
+        isvd.solve_grouped(reqs(), workers=args.serve_workers)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        rs = isvd.solve_batched(reqs(), workers=args.serve_workers)
+        rs = isvd.solve_grouped(reqs(), workers=args.serve_workers)
         torch.cuda.synchronize()
         t = time.perf_counter() - t0
         its = [r.result.iteration for r in rs]
         del shapes
         return {"kernel": "k_gkn_grouped (grouped batch)", "m": m, "n": n, "k": k, "count": args.batch_count,
                 "s": round(t, 4), "solves_per_s": round(args.batch_count / t, 2), "iterations_mean": float(np.mean(its)),
-                "iterations_max": int(max(its)), "phases": isvd.batched_times()}
+                "iterations_max": int(max(its)), "phases": isvd.grouped_times()}
     if args.kernel == "sketch_bf16":
         a = torch.randn(m, n, dtype=torch.float64, device=dev)
         sp = isvd.split_bf16(a, args.parts)

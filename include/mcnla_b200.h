@@ -299,20 +299,23 @@ MCNLA_B200_API int mcnla_b200_isvd_mixed(mcnla_b200_ctx* ctx, const mcnla_b200_p
 /* ---- batched and served solves ----------------------------------------------
  * Many independent solves of uneven sizes share the GPU.  (The reference runs
  * one problem per MPI job; this has no counterpart there.)
- *   mcnla_b200_isvd_batched runs a batch in waves that fit the budget.  The
- *   problems that use the row-block Gramian Kolmogorov-Nagumo integrator with
- *   N l <= 1536 go through three phases: a pool of workers (each with its own
- *   stream and workspaces) sketches and orthogonalizes them and forms their
- *   Gramians; one grouped persistent kernel then runs every problem's
- *   iterations, one problem per CTA from a device work queue, with per-problem
- *   iteration counts; the workers finish Qbar and the formers.  Other problems
- *   run whole solves on the workers.
- *   mcnla_b200_server_* keeps a worker pool for requests that arrive over
- *   time: a request is admitted when a worker is free and the estimated device
- *   bytes of the requests in flight stay within the budget.
- * A itself is the caller's and is not counted.  Every solve is deterministic
- * and a problem takes the same operations on every path, so it gives the same
- * result alone, in a batch and in a served mix.
+ *   mcnla_b200_server_* keeps a pool of workers (each with its own stream and
+ *   workspaces) for requests that arrive over time: a request is admitted when
+ *   a worker is free and the estimated device bytes of the requests in flight
+ *   stay within the budget; the workers' solves overlap on the device.
+ *   mcnla_b200_isvd_batched runs a whole batch through such a pool.
+ *   mcnla_b200_isvd_grouped runs a batch in phases instead, in waves that fit
+ *   the budget: the problems that use the row-block Gramian Kolmogorov-Nagumo
+ *   integrator with N l <= 1536 are sketched, orthogonalized and given their
+ *   Gramians by the workers; one grouped persistent kernel then runs every
+ *   problem's iterations (a cluster of CTAs per problem from a device work
+ *   queue, per-problem iteration counts); the workers finish Qbar and the
+ *   formers.  Other problems run whole solves on the workers.
+ * A itself is the caller's and is not counted.  Every solve is deterministic:
+ * a problem gives the same bits alone, in a batch of the pool and in a served
+ * mix; in a grouped batch it gives the same bits in any batch and agrees with
+ * the single solve to rounding with the same iteration count (the grouped
+ * kernel sums its products in its own fixed order).
  * Precisions: FP64 runs the plain path (an FP32 A is converted to FP64 on the
  * device for the sketch and the former).  The mixed precisions run the
  * precision form: the sketch on tcgen05 from BF16 parts of A, Omega drawn in
@@ -376,14 +379,17 @@ MCNLA_B200_API int mcnla_b200_server_destroy(mcnla_b200_server* server);
  * (each problem's own status is in problems[i].status).                      */
 MCNLA_B200_API int mcnla_b200_isvd_batched(int device, mcnla_b200_problem* problems, int count, int workers,
                                            int64_t budget_bytes);
-/* Seconds of the phases of the last mcnla_b200_isvd_batched call in this
+/* All problems as a grouped batch (see above); same statuses.                */
+MCNLA_B200_API int mcnla_b200_isvd_grouped(int device, mcnla_b200_problem* problems, int count, int workers,
+                                           int64_t budget_bytes);
+/* Seconds of the phases of the last mcnla_b200_isvd_grouped call in this
  * process (host clock): [0] sketch / orthogonalizer / Gramian of the grouped
  * problems, [1] the grouped integrator kernels, [2] the iterations they handed
  * back, [3] Qbar and the formers, [4] the other problems' whole solves; and
  * (device clock, summed over the grouped problems) [5] Bs Bc, [6] [Dc | Dgc],
  * [7] the KN step, [8] the E~ and B updates.  Returns the number of entries
  * (9); writes at most capacity.                                              */
-MCNLA_B200_API int mcnla_b200_batched_times(double* seconds, int capacity);
+MCNLA_B200_API int mcnla_b200_grouped_times(double* seconds, int capacity);
 
 /* ---- row-block decomposition over several GPUs -------------------------------
  * The reference's MPI decomposition of one solve (src/isvd_dense_rb.cpp:118-221

@@ -127,7 +127,8 @@ SIGNATURES = {
     "mcnla_b200_server_stats": (_INT, [_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64), ctypes.POINTER(_I64)]),
     "mcnla_b200_server_destroy": (_INT, [_P]),
     "mcnla_b200_isvd_batched": (_INT, [_INT, ctypes.POINTER(Problem), _INT, _INT, _I64]),
-    "mcnla_b200_batched_times": (_INT, [ctypes.POINTER(_D), _INT]),
+    "mcnla_b200_isvd_grouped": (_INT, [_INT, ctypes.POINTER(Problem), _INT, _INT, _I64]),
+    "mcnla_b200_grouped_times": (_INT, [ctypes.POINTER(_D), _INT]),
     "mcnla_b200_dgemm_noalloc": (_INT, [_P, _I64, _I64, _I64, _D, _P, _I64, _I64, _P, _I64, _I64, _D, _P, _I64,
                                         _I64]),
 }

@@ -221,10 +221,32 @@ int mcnla_b200_server_destroy(mcnla_b200_server* s) {
 }
 
 int mcnla_b200_isvd_batched(int device, mcnla_b200_problem* problems, int count, int workers, int64_t budget_bytes) {
+  if (count < 0 || (count > 0 && !problems)) return MCNLA_B200_ERR_ARG;
+  mcnla_b200_server* s = nullptr;
+  MB_CHECK(mcnla_b200_server_create(&s, device, workers, budget_bytes));
+  std::vector<int64_t> tickets(static_cast<size_t>(count));
+  int first = MCNLA_B200_OK;
+  for (int i = 0; i < count; ++i) {
+    const int st = mcnla_b200_server_submit(s, &problems[i], &tickets[size_t(i)]);
+    if (st != MCNLA_B200_OK) { first = st; tickets[size_t(i)] = 0; }
+  }
+  for (int i = 0; i < count; ++i) {
+    if (!tickets[size_t(i)]) continue;
+    const int st = mcnla_b200_server_wait(s, tickets[size_t(i)], &problems[i]);
+    if (st != MCNLA_B200_OK && first == MCNLA_B200_OK) first = st;
+  }
+  int64_t inflight = 0, peak = 0, done = 0;
+  const int sst = mcnla_b200_server_stats(s, &inflight, &peak, &done);
+  mcnla_b200_server_destroy(s);
+  if (first == MCNLA_B200_OK && sst != MCNLA_B200_OK) first = sst;
+  return first;
+}
+
+int mcnla_b200_isvd_grouped(int device, mcnla_b200_problem* problems, int count, int workers, int64_t budget_bytes) {
   return mb::batched_solve(device, problems, count, workers, budget_bytes);
 }
 
-int mcnla_b200_batched_times(double* seconds, int capacity) {
+int mcnla_b200_grouped_times(double* seconds, int capacity) {
   if (!seconds && capacity > 0) return -MCNLA_B200_ERR_ARG;
   return mb::batched_times(seconds, capacity);
 }

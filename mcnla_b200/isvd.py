@@ -35,7 +35,7 @@ __all__ = [
     "RowBlockWenYinIntegrator", "RowBlockGramianWenYinIntegrator",
     "SvdFormer", "GramianFormer", "RowBlockGramianFormer", "ColBlockGramianFormer",
     "solve", "solve_host", "Split", "split_bf16", "gaussian_bf16", "gemm_bf16", "solve_mixed",
-    "Request", "Server", "solve_batched",
+    "Request", "Server", "solve_batched", "solve_grouped", "grouped_times",
 ]
 
 
@@ -854,23 +854,33 @@ BATCH_PHASES = ("sketch_orthogonalize_gramian", "grouped_kernel", "declined_iter
                 "other_problems", "kernel_bs_bc", "kernel_d_dg", "kernel_kn_step", "kernel_e_b_update")
 
 
-def batched_times():
-    """Seconds of the phases of the last solve_batched call (BATCH_PHASES order; the kernel_* entries are
+def grouped_times():
+    """Seconds of the phases of the last solve_grouped call (BATCH_PHASES order; the kernel_* entries are
     the grouped kernel's device time summed over the problems)."""
     buf = (ctypes.c_double * len(BATCH_PHASES))()
-    _lib.load().mcnla_b200_batched_times(buf, len(BATCH_PHASES))
+    _lib.load().mcnla_b200_grouped_times(buf, len(BATCH_PHASES))
     return dict(zip(BATCH_PHASES, (round(buf[i], 4) for i in range(len(BATCH_PHASES)))))
 
 
-def solve_batched(requests, workers=4, budget_bytes=150 << 30):
-    """All requests through one temporary pool (mcnla_b200_isvd_batched)."""
+def _run_batch(entry, requests, workers, budget_bytes):
     if not requests:
         return requests
     torch.cuda.synchronize()
     arr = (_lib.Problem * len(requests))(*[r.problem for r in requests])
     dev = requests[0].a.device.index
-    st = _lib.load().mcnla_b200_isvd_batched(dev, arr, len(requests), workers, budget_bytes)
+    st = getattr(_lib.load(), entry)(dev, arr, len(requests), workers, budget_bytes)
     for r, out in zip(requests, arr):
         r.result = out
-    _lib.check(st, "isvd_batched")
+    _lib.check(st, entry)
     return requests
+
+
+def solve_batched(requests, workers=4, budget_bytes=150 << 30):
+    """All requests through one temporary worker pool (mcnla_b200_isvd_batched)."""
+    return _run_batch("mcnla_b200_isvd_batched", requests, workers, budget_bytes)
+
+
+def solve_grouped(requests, workers=4, budget_bytes=150 << 30):
+    """All requests as a grouped batch (mcnla_b200_isvd_grouped): the row-block Gramian KN problems'
+    iterations in one grouped kernel, the rest of every solve on `workers` workers."""
+    return _run_batch("mcnla_b200_isvd_grouped", requests, workers, budget_bytes)

@@ -1,4 +1,4 @@
-"""The grouped batch (mcnla_b200_isvd_batched): row-block Gramian Kolmogorov-Nagumo problems of
+"""The grouped batch (mcnla_b200_isvd_grouped): row-block Gramian Kolmogorov-Nagumo problems of
 uneven sizes go through the workers' sketch / orthogonalizer / Gramian phase, one grouped
 persistent kernel for every problem's iterations (a cluster of CTAs per problem from a device
 work queue; the iterations the power series declines run on the workers in between), and the
@@ -59,7 +59,7 @@ def _close(got, ref, tol=1e-10):
 def test_grouped_batch_matches_single_solves(cuda):
     from mcnla_b200 import isvd
     reqs = _problems(cuda, 24, seed=7)
-    isvd.solve_batched(reqs, workers=4)
+    isvd.solve_grouped(reqs, workers=4)
     first = [(r.s.clone(), r.u.clone(), r.v.clone(), r.result.iteration) for r in reqs]
     for r in reqs:
         assert r.result.status == 0
@@ -70,7 +70,7 @@ def test_grouped_batch_matches_single_solves(cuda):
     again = list(reversed(reqs[:10]))
     for r in again:
         r.s.zero_()
-    isvd.solve_batched(again, workers=3)
+    isvd.solve_grouped(again, workers=3)
     for r in again:
         s0, u0, v0, it0 = first[reqs.index(r)]
         assert r.result.iteration == it0
@@ -80,7 +80,7 @@ def test_grouped_batch_matches_single_solves(cuda):
 def test_grouped_batch_matches_the_oracle(cuda):
     from mcnla_b200 import isvd
     reqs = _problems(cuda, 6, seed=11, mixed_every=0)
-    isvd.solve_batched(reqs, workers=3)
+    isvd.solve_grouped(reqs, workers=3)
     for r in reqs:
         pr = r.problem
         k, p, N = pr.params.rank, pr.params.over_rank, pr.params.num_sketch
@@ -111,7 +111,7 @@ def test_grouped_batch_waves_and_other_integrators(cuda):
         a = torch.as_tensor(synthetic.lowrank_np(700 + i, 400, np.arange(1, 401) ** -1.0, seed=i), device=cuda)
         reqs.append(isvd.Request(a, 8, 4, 4, seed=99 + i, integrator=integ, former="svd", tol=1e-4))
     budget = 3 * max(r.bytes() for r in reqs)
-    isvd.solve_batched(reqs, workers=3, budget_bytes=budget)
+    isvd.solve_grouped(reqs, workers=3, budget_bytes=budget)
     for r in reqs:
         assert r.result.status == 0
         pr = r.problem
