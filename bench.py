@@ -613,11 +613,12 @@ def run_serving(args, dev):
             for sh in shapes]
     torch.cuda.synchronize()
 
-    def request(i, mixed, a=None, sh=None):
+    def request(i, mixed, a=None, sh=None, parts=None):
         sh = shapes[i] if sh is None else sh
+        sp, fsp = parts if parts is not None else (None, None)
         return isvd.Request(pool[i] if a is None else a, sh["k"], sh["p"], sh["N"], seed=sh["seed"],
                             integrator=args.serve_integrator, former=args.serve_former, maxit=256, tol=1e-5,
-                            mixed=mixed)
+                            mixed=mixed, split=sp, former_split=fsp)
 
     order = sorted(range(len(shapes)), key=lambda i: -shapes[i]["m"] * shapes[i]["n"] * shapes[i]["k"])
 
@@ -715,9 +716,16 @@ def run_serving(args, dev):
     fp64_mix_rate = 1.0 / (0.95 * t_small + 0.05 * t_large[-1])
     served = []
     rates = [float(x) for x in args.serve_rates.split(",") if x]
+    # resident matrices keep their BF16 parts (A for the sketch, A' for the precision former), split once
+    t_split = time.perf_counter()
+    resident = [isvd.resident_parts(pool[i], args.serve_parts) for i in range(keep)]
+    large_parts = [isvd.resident_parts(x, args.serve_parts) for x in large]
+    torch.cuda.synchronize()
+    t_split = time.perf_counter() - t_split
+    n_resident = keep + len(large)
     with isvd.Server(workers=W, budget_bytes=budget, device=dev) as srv:
-        warm = [request(0, args.serve_parts, a=large[j], sh=lsh[j]) for j in range(2)] + \
-               [request(i, args.serve_parts) for i in range(min(keep, 2 * W))]
+        warm = [request(0, args.serve_parts, a=large[j], sh=lsh[j], parts=large_parts[j]) for j in range(2)] + \
+               [request(i, args.serve_parts, parts=resident[i]) for i in range(min(keep, 2 * W))]
         for r in warm:
             srv.submit(r)
         for r in warm:
@@ -728,8 +736,8 @@ def run_serving(args, dev):
             arrivals = np.cumsum(rng.exponential(1.0 / rate, count))
             is_large = rng.random(count) < 0.05
             pick = rng.integers(0, keep, count)
-            reqs = [request(0, args.serve_parts, a=large[j % 2], sh=lsh[j % 2]) if is_large[j]
-                    else request(int(pick[j]), args.serve_parts)
+            reqs = [request(0, args.serve_parts, a=large[j % 2], sh=lsh[j % 2], parts=large_parts[j % 2])
+                    if is_large[j] else request(int(pick[j]), args.serve_parts, parts=resident[int(pick[j])])
                     for j in range(count)]
             torch.cuda.synchronize()
             t0 = time.perf_counter()
@@ -751,7 +759,7 @@ def run_serving(args, dev):
                            "failed": sum(1 for r in reqs if r.result.status != 0)})
             del reqs
         st = srv.stats()
-    del large, pool
+    del large, pool, resident, large_parts
     torch.cuda.empty_cache()
     return {
         "workload": "%d uneven FP32 matrices (m~U[512,16384], n~U[256,4096], k in {8,16,32,64}, p=k/2, N=8, "
@@ -764,7 +772,9 @@ def run_serving(args, dev):
         "mixed_speedup_vs_per_request_fp64": round(batched_mx["solves_per_s"] / serial64["solves_per_s"], 3),
         "mixed_speedup_vs_batched_fp64": round(batched_mx["solves_per_s"] / batched64["solves_per_s"], 3),
         "accuracy_mixed_vs_fp64_same_A_Omega": acc,
-        "served": {"precision": "mixed, A as %d BF16 parts" % args.serve_parts, "workers": W, "admission_cap_gb": budget / 1e9,
+        "served": {"precision": "mixed, A as %d BF16 parts and A' as 3, resident (split once: %.2f s for the %d "
+                                "matrices)" % (args.serve_parts, t_split, n_resident),
+                   "workers": W, "admission_cap_gb": budget / 1e9,
                    "large": "5%% of requests: 65536 x 8192 FP32, k=128 p=32 N=16 (%s)" % "two resident matrices",
                    "resident_pool": keep, "fp64_per_request_solves_per_s_same_mix": round(fp64_mix_rate, 2),
                    "fp64_large_request_s": round(t_large[-1], 4), "rates": served,

@@ -35,7 +35,7 @@ __all__ = [
     "RowBlockWenYinIntegrator", "RowBlockGramianWenYinIntegrator",
     "SvdFormer", "GramianFormer", "RowBlockGramianFormer", "ColBlockGramianFormer",
     "solve", "solve_host", "Split", "split_bf16", "gaussian_bf16", "gemm_bf16", "solve_mixed",
-    "Request", "Server", "solve_batched", "solve_grouped", "grouped_times",
+    "Request", "Server", "solve_batched", "solve_grouped", "grouped_times", "resident_parts",
 ]
 
 
@@ -669,6 +669,16 @@ def split_bf16(a, parts=2):
     _lib.check(ctx.lib.mcnla_b200_split_bf16(ctx.bind(), _ptr(a), layout, lda, m, n, _ptr(hi), _ptr(lo), _ptr(lo2),
                                              ld), "split_bf16")
     return Split(hi, lo, lo2, ld)
+
+
+def resident_parts(a, parts=3):
+    """The BF16 parts a served matrix keeps resident (split once, not per request): `parts` parts of A
+    for the mixed sketch and three of A' for the precision former, as (Split, Split).  A may be FP32
+    or FP64 (an FP32 A is widened for the split only; its parts are those of the exact FP64 copy)."""
+    a64 = a if a.dtype == torch.float64 else a.double()
+    out = split_bf16(a64, parts), split_bf16(a64.t(), 3)
+    del a64
+    return out
 
 
 def gaussian_bf16(n, L, seed, device=None, with_fp64=False):
