@@ -66,6 +66,44 @@ inline mcnla_b200_ctx* context() {
   return c;
 }
 
+// Row blocks over the reference's MPI ranks (Parameters::mpi_size > 1, one GPU
+// per rank): the context gets the library's NCCL communicator, its id made by
+// the Parameters' root rank and broadcast over the Parameters' communicator,
+// so each stage sums its row-dependent partial products over NVLink where the
+// reference's row-block stages call MPI_Allreduce
+// (row_block_gramian_orthogonalizer.hpp:86, the row-block integrators and
+// formers).  Every rank then has to run the same stages in the same order, as
+// the reference's drivers do.  force attaches on one rank too.
+inline void attach_ranks(const Parameters<double>& p, mcnla_b200_ctx* c, bool force = false) {
+  static std::mutex mu;
+  static std::map<mcnla_b200_ctx*, MPI_Comm> attached;
+  if (p.mpi_size <= 1 && !force) return;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = attached.find(c);
+  if (it != attached.end()) {
+    if (it->second != p.mpi_comm) {
+      std::fprintf(stderr, "mcnla_b200: a device's context serves one MPI communicator\n");
+      std::abort();
+    }
+    return;
+  }
+  unsigned char id[MCNLA_B200_NCCL_ID_BYTES] = {};
+  if (p.mpi_rank == p.mpi_root) check(mcnla_b200_nccl_unique_id(id), "mcnla_b200_nccl_unique_id");
+  if (MPI_Bcast(id, MCNLA_B200_NCCL_ID_BYTES, MPI_BYTE, p.mpi_root, p.mpi_comm) != MPI_SUCCESS) {
+    std::fprintf(stderr, "mcnla_b200: MPI_Bcast of the NCCL id failed\n");
+    std::abort();
+  }
+  check(mcnla_b200_set_nccl(c, id, int(p.mpi_size), int(p.mpi_rank)), "mcnla_b200_set_nccl");
+  attached.emplace(c, p.mpi_comm);
+}
+
+// The context a stage runs on, with the ranks attached.
+inline mcnla_b200_ctx* context(const Parameters<double>& p) {
+  mcnla_b200_ctx* c = context();
+  attach_ranks(p, c);
+  return c;
+}
+
 // A device buffer owned by a stage.
 struct DeviceBuffer {
   double* p = nullptr;
@@ -148,7 +186,7 @@ class Sketcher<GaussianProjectionSketcherB200Tag, double>
   }
   template <class _Matrix>
   void runImpl(const _Matrix& matrix_a, DenseMatrixCollectionColBlockRowMajor<double>& collection_q) noexcept {
-    mcnla_b200_ctx* ctx = b200::context();
+    mcnla_b200_ctx* ctx = b200::context(parameters_);
     const mcnla_b200_params p = b200::params_of(parameters_);
     const int64_t n = parameters_.ncol(), L = parameters_.dimSketchTotal();
     double comm_time;
@@ -196,7 +234,7 @@ class Orthogonalizer<GramianOrthogonalizerB200Tag, double>
     this->tic(comm_time);
     auto qu = collection_q.unfold();
     b200::to_device(qu, q_.p);
-    b200::check(mcnla_b200_orthogonalize(b200::context(), &p, q_.p), "mcnla_b200_orthogonalize");
+    b200::check(mcnla_b200_orthogonalize(b200::context(parameters_), &p, q_.p), "mcnla_b200_orthogonalize");
     b200::to_host(q_.p, qu);
     this->toc(comm_time);
   }
@@ -266,7 +304,7 @@ class Integrator<IntegratorB200Tag<_kind>, double> : public StageWrapper<Integra
     b200::to_device(collection_q.unfold(), q_.p);
     this->toc(comm_time);
     int it = 0;
-    b200::check(mcnla_b200_integrate(b200::context(), &p, _kind, q_.p, int(max_iteration_), tolerance_, qbar_.p, &it),
+    b200::check(mcnla_b200_integrate(b200::context(parameters_), &p, _kind, q_.p, int(max_iteration_), tolerance_, qbar_.p, &it),
                 "mcnla_b200_integrate");
     iteration_ = it;
     this->toc(comm_time);
@@ -331,7 +369,7 @@ class Former<FormerB200Tag<_kind>, double> : public StageWrapper<Former<FormerB2
     this->tic(comm_time);
     b200::to_device(matrix_a, a_.p);
     b200::to_device(matrix_qbar, qbar_.p);
-    b200::check(mcnla_b200_form(b200::context(), &p, _kind, a_.p, b200::layout_of(matrix_a), b200::ld_of(matrix_a),
+    b200::check(mcnla_b200_form(b200::context(parameters_), &p, _kind, a_.p, b200::layout_of(matrix_a), b200::ld_of(matrix_a),
                                 qbar_.p, s_.p, u_.p, v_.p), "mcnla_b200_form");
     b200::check_cuda(cudaMemcpy(vector_s_.valPtr(), s_.p, vector_s_.len() * sizeof(double), cudaMemcpyDeviceToHost),
                      "cudaMemcpy");

@@ -6,7 +6,9 @@
 // (check/isvd/integrator/*.cpp, check/isvd/orthogonalizer/*.cpp,
 // check/isvd/former/*.cpp): the row-block Gramian and plain KN integrators
 // stop after 81 iterations with Qbar within 1e-8 of qb_kn; the Gramian
-// orthogonalizer's and the formers' results agree with the CPU stages.
+// orthogonalizer's and the formers' results agree with the CPU stages; and with
+// the MPI row-block attachment (a one-rank NCCL communicator) the row-block
+// integrators still agree while their sums go through the communicator.
 // Built by oracle/Makefile (it includes the reference headers); test
 // infrastructure, not part of the product.
 #include <limits>
@@ -174,6 +176,45 @@ int main(int argc, char** argv) {
       for (int j = 0; j < 32; ++j) nrm += q.unfold()(i, j) * q.unfold()(i, j);
     std::printf("sketch ||Q||_F^2 %.3e\n", nrm);
     EXPECT(std::isfinite(nrm) && nrm > 0, "sketch");
+  }
+  // ---- the MPI row-block attachment (last: the device's context keeps it), at one rank:
+  // the stages' sums now go through the library's NCCL communicator.  The row-block KN
+  // integrator sums its row-dependent products every iteration
+  // (row_block_kolmogorov_nagumo_integrator.hpp:115, :143), the Gramian one its Gramian once
+  // (row_block_gramian_kolmogorov_nagumo_integrator.hpp:117); both must still match the CPU
+  // stages, and the context counts the all-reduces.
+  {
+    mcnla_b200_ctx* ctx = isvd::b200::context();
+    isvd::b200::attach_ranks(prm, ctx, /*force=*/true);
+    auto q = prm.createCollectionQj();
+    fill(q.unfold(), qs, m, N * l);
+    auto qbar_b = prm.createMatrixQbarj();
+    auto qbar_c = prm.createMatrixQbarj();
+    int64_t before = mcnla_b200_allreduces(ctx);
+    isvd::RowBlockKolmogorovNagumoIntegratorB200<double> gpu(prm, 256, 1e-4);
+    isvd::RowBlockKolmogorovNagumoIntegrator<double> cpu(prm, 256, 1e-4);
+    gpu.initialize();
+    cpu.initialize();
+    gpu(q, qbar_b);
+    cpu(q, qbar_c);
+    int64_t sums = mcnla_b200_allreduces(ctx) - before;
+    std::printf("rb_kn over a one-rank NCCL communicator: iterations %d (reference %d), all-reduces %lld, "
+                "|Qbar - reference| %.3e\n", int(gpu.iteration()), int(cpu.iteration()),
+                static_cast<long long>(sums), max_diff(qbar_b, qbar_c, m, l));
+    EXPECT(gpu.iteration() == cpu.iteration(), "iterations %d vs %d", int(gpu.iteration()), int(cpu.iteration()));
+    EXPECT(max_diff(qbar_b, qbar_c, m, l) < 1e-10, "Qbar vs the CPU stage");
+    EXPECT(sums >= gpu.iteration(), "all-reduces %lld", static_cast<long long>(sums));
+
+    before = mcnla_b200_allreduces(ctx);
+    isvd::RowBlockGramianKolmogorovNagumoIntegratorB200<double> gg(prm, 256, 1e-4);
+    gg.initialize();
+    gg(q, qbar_b);
+    sums = mcnla_b200_allreduces(ctx) - before;
+    std::printf("rb_gramian_kn over it: iterations %d, all-reduces %lld, |Qbar - qb_kn| %.3e\n", int(gg.iteration()),
+                static_cast<long long>(sums), max_diff(qbar_b, qb_ref, m, l));
+    EXPECT(gg.iteration() == 81, "iterations %d", int(gg.iteration()));
+    EXPECT(max_diff(qbar_b, qb_ref, m, l) < 1e-8, "Qbar vs the fixture");
+    EXPECT(sums >= 1, "all-reduces %lld", static_cast<long long>(sums));
   }
   std::printf("%s (%d failures)\n", failures ? "FAILED" : "OK", failures);
   return failures ? 1 : 0;
