@@ -11,6 +11,7 @@ namespace mb {
 namespace {
 
 constexpr int kSmallThreads = 512;
+constexpr int kSyevThreads = 1024;   // the Jacobi rounds are latency-bound: more warps hide more of it
 constexpr int kMaxSweeps = 40;
 constexpr int kKnNsMaxDim = 80;   // the matrix-function KN step keeps four padded l x l matrices on chip
 
@@ -29,21 +30,19 @@ struct SmemCarve {
 };
 
 __host__ __device__ inline size_t jacobi_scratch_bytes(int n) {
-  const int np = (n + 2) / 2;
-  return 6 * (np * 8 + 16) + 2 * (np * 4 + 16) + 16 + 32 * 8 + 16 + (n + 4) * 4 + 64;
+  const int np = (n + 2) / 2;   // cs, pq, t, apq, app, aqq, count, red (16-byte aligned each)
+  return (np * 16 + 16) + (np * 8 + 16) + 4 * (np * 8 + 16) + 16 + 32 * 8 + 16 + (n + 4) * 4 + 64;
 }
 
 __device__ small::JacobiScratch carve_jacobi(SmemCarve& sc, int n) {
   const int np = (n + 2) / 2;
   small::JacobiScratch js;
-  js.c = sc.take<double>(np);
-  js.s = sc.take<double>(np);
+  js.cs = sc.take<double2>(np);
+  js.pq = sc.take<int2>(np);
   js.t = sc.take<double>(np);
   js.apq = sc.take<double>(np);
   js.app = sc.take<double>(np);
   js.aqq = sc.take<double>(np);
-  js.p = sc.take<int>(np);
-  js.q = sc.take<int>(np);
   js.count = sc.take<int>(1);
   js.red = sc.take<double>(32);
   return js;
@@ -67,7 +66,7 @@ __device__ void eig_ranks(const double* a, int lda, int n, int order, int* rank)
 // ---------------------------------------------------------------------------
 // batched symmetric eigendecomposition
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kSmallThreads) k_syev(int n, const double* A, int64_t lda, int64_t a_bs,
+__global__ void __launch_bounds__(kSyevThreads) k_syev(int n, const double* A, int64_t lda, int64_t a_bs,
                                                         double* W, double* V, int order, int v_smem,
                                                         double* vwork_all) {
   extern __shared__ __align__(16) char smem_raw[];
@@ -118,7 +117,7 @@ __global__ void k_scale_cols_rsqrt(int n, int batch, const double* V, const doub
 // ---------------------------------------------------------------------------
 // Kolmogorov-Nagumo step
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kSmallThreads) k_kn_step(int l, const double* z_in, const double* dd,
+__global__ void __launch_bounds__(kSyevThreads) k_kn_step(int l, const double* z_in, const double* dd,
                                                            double inv_n, double* out, double* outn,
                                                            const double* ff, double* ffn, double* vwork,
                                                            int v_smem, DevScalars* scal, double tol,
@@ -875,7 +874,7 @@ int launch_syev(Context* c, int n, int batch, const double* A, int64_t lda, int6
   const size_t smem = small_smem_syev(n, v_smem);
   if (smem > c->smem_optin) return MCNLA_B200_ERR_UNSUPPORTED;
   MB_CHECK(set_smem(c, reinterpret_cast<const void*>(k_syev), smem));
-  k_syev<<<batch, kSmallThreads, smem, c->stream>>>(n, A, lda, a_bs, W, V, order, v_smem ? 1 : 0, vwork);
+  k_syev<<<batch, kSyevThreads, smem, c->stream>>>(n, A, lda, a_bs, W, V, order, v_smem ? 1 : 0, vwork);
   c->kernels_launched++;
   MB_CHECK_CUDA(cudaGetLastError());
   return MCNLA_B200_OK;
@@ -915,7 +914,7 @@ int launch_kn_step(Context* c, int l, const double* z, const double* dd, double 
   const size_t smem = small_smem_syev(l, v_smem) + l * 8 + 64;
   if (smem > c->smem_optin) return MCNLA_B200_ERR_UNSUPPORTED;
   MB_CHECK(set_smem(c, reinterpret_cast<const void*>(k_kn_step), smem));
-  k_kn_step<<<1, kSmallThreads, smem, c->stream>>>(l, z, dd, inv_n, out, outn, ff, ffn, vwork, v_smem ? 1 : 0,
+  k_kn_step<<<1, kSyevThreads, smem, c->stream>>>(l, z, dd, inv_n, out, outn, ff, ffn, vwork, v_smem ? 1 : 0,
                                                     c->scal, tol, c->guard_stop, c->guard_it, only_if);
   c->kernels_launched++;
   MB_CHECK_CUDA(cudaGetLastError());

@@ -31,14 +31,12 @@ __device__ __forceinline__ void rr_pair(int P, int r, int k, int& p, int& q) {
 }
 
 struct JacobiScratch {
-  double* c;    // npairs
-  double* s;    // npairs
+  double2* cs;  // npairs: (cos, sin) of each pair's rotation
+  int2* pq;     // npairs: the pair's indices (p < q)
   double* t;    // npairs (tangent, for the exact diagonal update)
   double* apq;  // npairs
   double* app;  // npairs
   double* aqq;  // npairs
-  int* p;       // npairs
-  int* q;       // npairs
   int* count;   // 1 (rotations applied this round)
   double* red;  // 32
 };
@@ -68,9 +66,17 @@ __device__ inline double cta_frob2(const double* a, int lda, int n, double* red)
 // V, so that a rotation of two eigenvectors touches two contiguous rows, which
 // matters when v lives in global memory).  When init_v is false, v must hold
 // an orthogonal starting basis (rows) in which a is expressed (warm start);
-// otherwise v is set to I.  Each phase of a round (angles; rows of a; columns
-// of a and rows of v) is spread over the whole CTA as (pair, element) items.
-// Returns the number of sweeps.
+// otherwise v is set to I.  Returns the number of sweeps.
+//
+// A round has two phases and two barriers: the angles (one thread per pair),
+// then one update phase.  The rotations of a round act on disjoint index
+// pairs, so a <- J' a J splits into 2 x 2 blocks (rows of pair K1, columns of
+// pair K2) that depend only on their own four entries and the two pairs'
+// rotations: each (K1, K2) block is one item (rows rotated first, then
+// columns; the diagonal blocks are written exactly, J' B J = diag(app - t apq,
+// aqq + t apq)).  The eigenvector rows of each pair are items of the same
+// phase.  The rounds are latency-bound: launch it with many warps (1024
+// threads) rather than give a thread several items' loads at once.
 __device__ inline int cta_jacobi_eig(double* a, int lda, double* v, int ldv, int n, bool init_v,
                                      const JacobiScratch& js, int max_sweeps) {
   const int tid = threadIdx.x, nt = blockDim.x;
@@ -90,10 +96,12 @@ __device__ inline int cta_jacobi_eig(double* a, int lda, double* v, int ldv, int
   const double eps = 2.220446049250313e-16;
   const double eps2 = eps * eps;
   const double abs_floor = eps2 * fro2;
-  // items (pair k, element j) of a round, k-major: thread tid takes e = tid, tid + nt, ...,
-  // walked as (k, j) with a fixed increment instead of dividing e by n for every item
-  const int k_start = tid / n, j_start = tid - k_start * n;
-  const int k_step = nt / n, j_step = nt - k_step * n;
+  // block items (K1, K2), K2 fastest, and eigenvector items (pair k, component i), i fastest:
+  // thread tid takes e = tid, tid + nt, ..., walked with fixed increments
+  const int b1_start = tid / npairs, b2_start = tid - b1_start * npairs;
+  const int b1_step = nt / npairs, b2_step = nt - b1_step * npairs;
+  const int k_start = tid / n, i_start = tid - k_start * n;
+  const int k_step = nt / n, i_step = nt - k_step * n;
   int sweep = 0;
   for (; sweep < max_sweeps; ++sweep) {
     int rotated = 0;
@@ -120,49 +128,68 @@ __device__ inline int cta_jacobi_eig(double* a, int lda, double* v, int ldv, int
             apq = 0.0;
           }
         }
-        js.c[k] = c; js.s[k] = s; js.t[k] = t; js.apq[k] = apq; js.app[k] = app; js.aqq[k] = aqq;
-        js.p[k] = p; js.q[k] = q;
+        js.cs[k] = make_double2(c, s);
+        js.pq[k] = make_int2(p, q);
+        js.t[k] = t; js.apq[k] = apq; js.app[k] = app; js.aqq[k] = aqq;
       }
       // the barrier also counts the threads that set up a rotation
       const int cnt = __syncthreads_count(mine);
       if (cnt == 0) continue;
       rotated += cnt;
-      // 2. rows: a <- J' a   (item (k, j): element j of rows p, q of pair k)
-      for (int k = k_start, j = j_start; k < npairs;) {
-        const double s = js.s[k];
-        if (s != 0.0) {
-          const double c = js.c[k];
-          const int p = js.p[k], q = js.q[k];
-          const double x = a[p * lda + j], y = a[q * lda + j];
-          a[p * lda + j] = c * x - s * y;
-          a[q * lda + j] = s * x + c * y;
+      // 2a. a <- J' a J by 2 x 2 blocks
+      for (int k1 = b1_start, k2 = b2_start; k1 < npairs;) {
+        const double2 cs1 = js.cs[k1], cs2 = js.cs[k2];
+        const double s1 = cs1.y, s2 = cs2.y;
+        if (s1 != 0.0 || s2 != 0.0) {
+          const int2 pq1 = js.pq[k1], pq2 = js.pq[k2];
+          const int p1 = pq1.x, q1 = pq1.y, p2 = pq2.x, q2 = pq2.y;
+          if (k1 == k2) {
+            const double ta = js.t[k1] * js.apq[k1];
+            a[p1 * lda + p1] = js.app[k1] - ta;
+            a[q1 * lda + q1] = js.aqq[k1] + ta;
+            a[p1 * lda + q1] = 0.0;
+            a[q1 * lda + p1] = 0.0;
+          } else {
+            // q1 / q2 is the padding index n of an odd n only in a pair that does not rotate
+            const bool h1 = q1 < n, h2 = q2 < n;
+            double xpp = a[p1 * lda + p2];
+            double xpq = h2 ? a[p1 * lda + q2] : 0.0;
+            double xqp = h1 ? a[q1 * lda + p2] : 0.0;
+            double xqq = (h1 && h2) ? a[q1 * lda + q2] : 0.0;
+            if (s1 != 0.0) {
+              const double c1 = cs1.x;
+              const double rpp = c1 * xpp - s1 * xqp, rqp = s1 * xpp + c1 * xqp;
+              const double rpq = c1 * xpq - s1 * xqq, rqq = s1 * xpq + c1 * xqq;
+              xpp = rpp; xqp = rqp; xpq = rpq; xqq = rqq;
+            }
+            if (s2 != 0.0) {
+              const double c2 = cs2.x;
+              const double ypp = c2 * xpp - s2 * xpq, ypq = s2 * xpp + c2 * xpq;
+              const double yqp = c2 * xqp - s2 * xqq, yqq = s2 * xqp + c2 * xqq;
+              xpp = ypp; xpq = ypq; xqp = yqp; xqq = yqq;
+            }
+            a[p1 * lda + p2] = xpp;
+            if (h2) a[p1 * lda + q2] = xpq;
+            if (h1) a[q1 * lda + p2] = xqp;
+            if (h1 && h2) a[q1 * lda + q2] = xqq;
+          }
+        }
+        k1 += b1_step;
+        k2 += b2_step;
+        if (k2 >= npairs) { k2 -= npairs; ++k1; }
+      }
+      // 2b. rows p, q of v
+      for (int k = k_start, i = i_start; k < npairs;) {
+        const double2 cs = js.cs[k];
+        if (cs.y != 0.0) {
+          const int2 pq = js.pq[k];
+          const double vx = v[pq.x * ldv + i], vy = v[pq.y * ldv + i];
+          v[pq.x * ldv + i] = cs.x * vx - cs.y * vy;
+          v[pq.y * ldv + i] = cs.y * vx + cs.x * vy;
         }
         k += k_step;
-        j += j_step;
-        if (j >= n) { j -= n; ++k; }
-      }
-      __syncthreads();
-      // 3. columns: a <- a J (the 2x2 block of each pair written exactly:
-      //    J' B J = diag(app - t apq, aqq + t apq)), and rows p, q of v
-      for (int k = k_start, i = j_start; k < npairs; k += k_step, i += j_step, (i >= n ? (i -= n, ++k) : 0)) {
-        const double s = js.s[k];
-        if (s == 0.0) continue;
-        const double c = js.c[k];
-        const int p = js.p[k], q = js.q[k];
-        if (i == p) {
-          a[p * lda + p] = js.app[k] - js.t[k] * js.apq[k];
-          a[p * lda + q] = 0.0;
-        } else if (i == q) {
-          a[q * lda + q] = js.aqq[k] + js.t[k] * js.apq[k];
-          a[q * lda + p] = 0.0;
-        } else {
-          const double x = a[i * lda + p], y = a[i * lda + q];
-          a[i * lda + p] = c * x - s * y;
-          a[i * lda + q] = s * x + c * y;
-        }
-        const double vx = v[p * ldv + i], vy = v[q * ldv + i];
-        v[p * ldv + i] = c * vx - s * vy;
-        v[q * ldv + i] = s * vx + c * vy;
+        i += i_step;
+        if (i >= n) { i -= n; ++k; }
       }
       __syncthreads();
     }
