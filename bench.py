@@ -77,6 +77,8 @@ def parse():
     ap.add_argument("--serve-workers", type=int, default=8, help="concurrent solves of the server")
     ap.add_argument("--serve-pool", type=int, default=256, help="distinct resident matrices the requests use")
     ap.add_argument("--serve-rates", default="200,1000,5000", help="Poisson arrival rates, requests/s")
+    ap.add_argument("--serve-rates-fp64", default="200,1000",
+                    help="arrival rates also served in plain FP64 (the same arrivals as the mixed ones)")
     ap.add_argument("--serve-seconds", type=float, default=0.5, help="arrival window per rate (>= 400 requests)")
     ap.add_argument("--serve-integrator", default="rb_gramian_kn", help="KN integrator of the batched / served solves")
     ap.add_argument("--serve-former", default="rb_gramian",
@@ -307,6 +309,102 @@ def run_config1_b200(args, dev):
                     "d2h_bytes_per_step": int((10 + 1000 * 10 + 2000 * 10) * 8)},
             "reconstruction_rel_err": reconstruction_error_torch(a, s, u, v),
             "sigma": [float(x) for x in s[:3].tolist()]}
+
+
+def _svd_metrics(s, u, s_ref, u_ref):
+    """sigma relative error, largest principal angle between the U subspaces, ||U'U - I||_F."""
+    import numpy as np
+    k = s.shape[0]
+    rel = float(np.max(np.abs(s - s_ref[:k]) / s_ref[:k]))
+    cosmin = np.clip(np.linalg.svd(u_ref[:, :k].T @ u, compute_uv=False).min(), -1.0, 1.0)
+    orth = float(np.linalg.norm(u.T @ u - np.eye(k)))
+    return {"sigma_rel_err": rel, "max_principal_angle_U": float(np.arccos(cosmin)), "UtU_minus_I_fro": orth}
+
+
+def run_config3_b200(args, dev):
+    """The precision form at the configuration-1 shape with an ill-conditioned spectrum: m = 1000,
+    n = 2000, sigma_j = 10^(-6 (j-1)/199) for j <= 200 plus a 1e-8 G noise floor, k = 64, p = 16,
+    N = 32; A stored in FP32 (the FP64 path reads its exact FP64 widening) and as BF16 parts of A
+    and A' (resident, split once).  Gramian orthogonalizer, row-block Gramian KN (tol 1e-6), SVD
+    former (the mixed solve: the precision former).  Timed solves of both paths (CUDA events),
+    and for each the sigma relative error, the largest principal angle of U and ||U'U - I||
+    against LAPACK dgesvd of the same FP64 matrix, plus mixed against FP64 on the same Omega."""
+    import numpy as np
+    import scipy.linalg
+    import torch
+    from mcnla_b200 import isvd, synthetic
+    m, n, k, p, N = 1000, 2000, 64, 16, 32
+    a32 = torch.as_tensor(synthetic.lowrank_np(m, n, synthetic.config3_sigma(), seed=3, noise=1e-8),
+                          device=dev).float()
+    a64 = a32.double()
+    a_np = a64.cpu().numpy()
+    u_ref, s_ref, _ = scipy.linalg.svd(a_np, full_matrices=False, lapack_driver="gesvd")
+    split, fsplit = isvd.resident_parts(a32, 3)
+    seed = 11
+    _, _, omega = isvd.gaussian_bf16(n, (k + p) * N, seed, dev, with_fp64=True)
+    kw = dict(integrator="rb_gramian_kn", former="svd", tol=1e-6, maxit=256)
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(fn, steps):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return out, e0.elapsed_time(e1) / 1e3 / steps
+
+    steps = max(3, args.steps)
+    (s64, u64, _, it64), t64 = timed(lambda: isvd.solve(a64, k, p, N, omega=omega, **kw), steps)
+    (smx, umx, _, itmx), tmx = timed(lambda: isvd.solve_mixed(a64, k, p, N, seed=seed, split=split,
+                                                              former_split=fsplit, **kw), steps)
+    s64, u64, smx, umx = (x.cpu().numpy() for x in (s64, u64, smx, umx))
+    fp64 = dict(_svd_metrics(s64, u64, s_ref, u_ref), value=round(1.0 / t64, 3), unit="iSVD/s", iterations=it64)
+    mixed = dict(_svd_metrics(smx, umx, s_ref, u_ref), value=round(1.0 / tmx, 3), unit="iSVD/s", iterations=itmx)
+    mixed["vs_fp64_same_A_Omega"] = _svd_metrics(smx, umx, s64, u64)
+    del split, fsplit, a32, a64, omega
+    torch.cuda.empty_cache()
+    return {"workload": "precision form, m=1000 n=2000, sigma_j=10^(-6(j-1)/199) j<=200 + 1e-8 G, k=64 p=16 N=32, "
+                        "A in FP32 + resident BF16 parts (3 of A, 3 of A')",
+            "stages": "Gramian / RowBlockGramianKolmogorovNagumo (tol 1e-6) / Svd (mixed: precision former)",
+            "oracle": "LAPACK dgesvd (scipy.linalg.svd, lapack_driver='gesvd') of the FP64 widening of A",
+            "fp64": fp64, "mixed": mixed, "speedup_mixed_vs_fp64": round(t64 / tmx, 3)}
+
+
+def run_colblock_b200(args, dev, a_rm):
+    """Configuration 2 in the column-block layout (the reference's isvd_dense_cb: column-major
+    A, column-block Gramian former) with the Kolmogorov-Nagumo and Wen-Yin integrators: a
+    column-major copy of the same A, one warm-up and `steps` timed solves each (CUDA events),
+    sigma against the row-major solve with the same Omega seed."""
+    import torch
+    from mcnla_b200 import isvd
+    a_cm = a_rm.t().contiguous().t()
+    stream = torch.cuda.current_stream(dev)
+    out = {}
+    for integ in ("rb_gramian_kn", "rb_wy"):
+        kw = dict(integrator=integ, former="cb_gramian", maxit=args.maxit, tol=args.tol)
+        isvd.solve(a_cm, args.k, args.p, args.N, seed=0, **kw)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        steps = 2
+        e0.record(stream)
+        for step in range(steps):
+            s, u, v, it = isvd.solve(a_cm, args.k, args.p, args.N, seed=100 + step, **kw)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3 / steps
+        entry = {"value": round(1.0 / t, 4), "unit": "iSVD/s", "iterations": it}
+        if integ == args.integrator:
+            s_rm = isvd.solve(a_rm, args.k, args.p, args.N, seed=100 + steps - 1, integrator=integ,
+                              former=args.former, maxit=args.maxit, tol=args.tol)[0]
+            entry["sigma_rel_diff_vs_row_major"] = float(((s - s_rm).abs() / s_rm).max().item())
+        out[integ] = entry
+    del a_cm
+    torch.cuda.empty_cache()
+    return {"layout": "column-major A (isvd_dense_cb), ColBlockGramianFormer", "integrators": out}
 
 
 def run_row_block_b200(args, world, rank, local):
@@ -565,6 +663,16 @@ def run_b200(args, world, rank, local):
 
     recon = reconstruction_error_torch(a, s, u, v)
     c1 = run_config1_b200(args, dev) if world == 1 and not args.quick else None
+    c3 = colblock = None
+    if world == 1 and not args.quick:
+        for name, fn in (("config3", lambda: run_config3_b200(args, dev) if not args.no_mixed else None),
+                         ("colblock", lambda: run_colblock_b200(args, dev, a) if not args.colmajor else None)):
+            try:
+                r_ = fn()
+            except Exception as e:          # an extra leg's failure is reported, not fatal
+                r_ = {"error": "%s: %s" % (type(e).__name__, e)}
+                torch.cuda.synchronize()
+            c3, colblock = (r_, colblock) if name == "config3" else (c3, r_)
     row_block = None
     if world > 1 and not args.no_row_block:
         del a
@@ -581,7 +689,7 @@ def run_b200(args, world, rank, local):
         "iterations": iters[-1], "stages": stages, "integrators": variants, "mixed": mixed, "roofline": roofline,
         "stage_roofline": stage_roof, "e2e": e2e,
         "gpu_launches": int(launches), "clocks": clk,
-        "reconstruction_rel_err": recon, "config1": c1, "row_block": row_block,
+        "reconstruction_rel_err": recon, "config1": c1, "config3": c3, "colblock": colblock, "row_block": row_block,
     }
     return result
 
@@ -599,9 +707,10 @@ def run_serving(args, dev):
     p = k/2, N = 8, sigma_j = j^-alpha, KN tol 1e-5, SVD former) through the server:
     per-request plain FP64 (one worker), batched FP64 and batched mixed precision (W
     workers), then Poisson arrivals at each rate with 5 % large requests (65536 x 8192,
-    k = 128, p = 32, N = 16), mixed precision, 150 GB admission cap.  A stays resident in
-    HBM as FP32; wall-clock times on the host with the device synchronized on both sides
-    (the solves run on the workers' own streams)."""
+    k = 128, p = 32, N = 16), mixed precision, 150 GB admission cap, and the same arrivals
+    again in plain FP64 at the --serve-rates-fp64 rates.  A stays resident in HBM as FP32
+    (and, for the mixed requests, as BF16 parts); wall-clock times on the host with the
+    device synchronized on both sides (the solves run on the workers' own streams)."""
     import numpy as np
     import torch
     from mcnla_b200 import isvd, synthetic
@@ -730,14 +839,17 @@ def run_serving(args, dev):
             srv.submit(r)
         for r in warm:
             srv.wait(r)
-        for rate in rates:
+        def serve(rate, mixed):
+            """Poisson arrivals at `rate` (seeded by the rate: the same arrivals, sizes and
+            matrices for every precision), submitted as they arrive; latency per request."""
             rng = np.random.default_rng(int(rate))
             count = max(400, int(rate * args.serve_seconds)) if not args.quick else 64
             arrivals = np.cumsum(rng.exponential(1.0 / rate, count))
             is_large = rng.random(count) < 0.05
             pick = rng.integers(0, keep, count)
-            reqs = [request(0, args.serve_parts, a=large[j % 2], sh=lsh[j % 2], parts=large_parts[j % 2])
-                    if is_large[j] else request(int(pick[j]), args.serve_parts, parts=resident[int(pick[j])])
+            reqs = [request(0, mixed, a=large[j % 2], sh=lsh[j % 2], parts=large_parts[j % 2] if mixed else None)
+                    if is_large[j] else
+                    request(int(pick[j]), mixed, parts=resident[int(pick[j])] if mixed else None)
                     for j in range(count)]
             torch.cuda.synchronize()
             t0 = time.perf_counter()
@@ -751,15 +863,24 @@ def run_serving(args, dev):
             t = time.perf_counter() - t0
             lat = [r.result.latency for r in reqs]
             lat_small = [r.result.latency for r, big in zip(reqs, is_large) if not big]
-            served.append({"rate_per_s": rate, "requests": count, "large": int(is_large.sum()),
-                           "solves_per_s": round(count / t, 2), "seconds": round(t, 4),
-                           "p50_ms": round(_pct(lat, 0.5) * 1e3, 3), "p99_ms": round(_pct(lat, 0.99) * 1e3, 3),
-                           "p50_ms_small": round(_pct(lat_small, 0.5) * 1e3, 3),
-                           "p99_ms_small": round(_pct(lat_small, 0.99) * 1e3, 3),
-                           "failed": sum(1 for r in reqs if r.result.status != 0)})
-            del reqs
+            return {"rate_per_s": rate, "requests": count, "large": int(is_large.sum()),
+                    "solves_per_s": round(count / t, 2), "seconds": round(t, 4),
+                    "p50_ms": round(_pct(lat, 0.5) * 1e3, 3), "p99_ms": round(_pct(lat, 0.99) * 1e3, 3),
+                    "p50_ms_small": round(_pct(lat_small, 0.5) * 1e3, 3),
+                    "p99_ms_small": round(_pct(lat_small, 0.99) * 1e3, 3),
+                    "failed": sum(1 for r in reqs if r.result.status != 0)}
+
+        for rate in rates:
+            served.append(serve(rate, args.serve_parts))
         st = srv.stats()
-    del large, pool, resident, large_parts
+    # the same arrivals in plain FP64 (the server widens each FP32 A per request), on a server
+    # whose admission cap leaves room for the resident FP32 matrices once the BF16 parts are freed
+    del resident, large_parts
+    torch.cuda.empty_cache()
+    budget64 = int(min(budget, torch.cuda.mem_get_info(dev)[0] - 12e9))
+    with isvd.Server(workers=W, budget_bytes=budget64, device=dev) as srv:
+        served64 = [serve(rate, False) for rate in [float(x) for x in args.serve_rates_fp64.split(",") if x]]
+    del large, pool
     torch.cuda.empty_cache()
     return {
         "workload": "%d uneven FP32 matrices (m~U[512,16384], n~U[256,4096], k in {8,16,32,64}, p=k/2, N=8, "
@@ -778,6 +899,11 @@ def run_serving(args, dev):
                    "large": "5%% of requests: 65536 x 8192 FP32, k=128 p=32 N=16 (%s)" % "two resident matrices",
                    "resident_pool": keep, "fp64_per_request_solves_per_s_same_mix": round(fp64_mix_rate, 2),
                    "fp64_large_request_s": round(t_large[-1], 4), "rates": served,
+                   "fp64_same_arrivals": served64, "fp64_admission_cap_gb": round(budget64 / 1e9, 1),
+                   "mixed_speedup_vs_fp64_same_arrivals": [
+                       {"rate_per_s": x["rate_per_s"], "solves_per_s": round(x["solves_per_s"] / y["solves_per_s"], 3),
+                        "p50": round(y["p50_ms"] / x["p50_ms"], 3)}
+                       for x in served for y in served64 if x["rate_per_s"] == y["rate_per_s"]],
                    "peak_admitted_gb": round(st["peak_bytes"] / 1e9, 3)},
     }
 
@@ -1126,7 +1252,11 @@ def main():
         if world == 1 and not args.no_serving:
             import torch
             torch.cuda.empty_cache()
-            res["serving"] = run_serving(args, torch.device("cuda", local))
+            try:
+                res["serving"] = run_serving(args, torch.device("cuda", local))
+            except Exception as e:          # the headline line is printed whatever this leg does
+                res["serving"] = {"error": "%s: %s" % (type(e).__name__, e)}
+                torch.cuda.synchronize()
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             est, info = cpu_sample(args)
             res["cpu_baseline"] = {"value": round(1.0 / est, 6), "unit": "iSVD/s", "cores": info["cores"],

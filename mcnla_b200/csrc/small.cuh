@@ -23,9 +23,11 @@ namespace small {
 // distinct players meets exactly once per sweep.
 __device__ __forceinline__ void rr_pair(int P, int r, int k, int& p, int& q) {
   if (k == 0) { p = r; q = P - 1; }
-  else {
-    p = (r + k) % (P - 1);
-    q = (r - k + (P - 1)) % (P - 1);
+  else {                        // 0 <= r < P - 1 and 1 <= k < P / 2: one wrap at most
+    p = r + k;
+    if (p >= P - 1) p -= P - 1;
+    q = r - k;
+    if (q < 0) q += P - 1;
   }
   if (p > q) { int t = p; p = q; q = t; }
 }
@@ -118,10 +120,17 @@ __device__ inline int cta_jacobi_eig(double* a, int lda, double* v, int ldv, int
           aqq = a[q * lda + q];
           const double apq2 = apq * apq;
           if (apq2 > eps2 * fabs(app * aqq) && apq2 > abs_floor) {
-            const double theta = (aqq - app) / (2.0 * apq);
-            const double at = fabs(theta);
-            t = (at > 1e150) ? 0.5 / theta : ((theta >= 0.0 ? 1.0 : -1.0) / (at + sqrt(1.0 + theta * theta)));
-            c = 1.0 / sqrt(1.0 + t * t);
+            // t = sgn(theta) / (|theta| + sqrt(1 + theta^2)), theta = d / g (d = aqq - app,
+            // g = 2 apq), written as sgn(d) g / (|d| + sqrt(d^2 + g^2)): one division, one
+            // square root and one reciprocal square root on the round's critical path.  t is
+            // invariant under scaling d and g together, so entries far from 1 are scaled by
+            // 2^-600 or 2^600 (exactly) before d^2 + g^2 could overflow or lose precision.
+            double d = aqq - app, g = 2.0 * apq;
+            const double mx = fmax(fabs(d), fabs(g));
+            if (mx > 1e150) { d *= 0x1p-600; g *= 0x1p-600; }
+            else if (mx < 1e-150) { d *= 0x1p600; g *= 0x1p600; }
+            t = (d >= 0.0 ? g : -g) / (fabs(d) + sqrt(fma(d, d, g * g)));
+            c = rsqrt(fma(t, t, 1.0));
             s = t * c;
             ++mine;
           } else {
