@@ -56,7 +56,7 @@ struct DevScalars {
   unsigned bar_count; // grid barrier of cooperative kernels: arrivals (only grows within a stage)
   unsigned bar_spare;
   int resume_it;      // persistent integrator: iteration it handed back to the host (-1: none)
-  int pad;
+  int kn_ns_failed;   // 1: the Newton-Schulz KN step with its matrices in global memory failed
 };
 
 // Per-device context: one stream, a growable workspace arena, timing events.

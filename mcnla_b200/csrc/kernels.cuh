@@ -26,8 +26,9 @@ int launch_scale_cols_rsqrt(Context* c, int n, int batch, const double* V, const
 // scal->norm := || s - 1 ||_2, s = sqrt(1/2 + sqrt(1/4 - eig(Z))).
 // vwork: kn_series_work_doubles(l) doubles of global scratch.
 // Method (mcnla_b200_set_kn_method): KN_AUTO runs the series kernel and, for
-// the iterations it declines, the Newton-Schulz kernel (l <= 80) or the
-// eigendecomposition; KN_NEWTON_SCHULZ starts at Newton-Schulz; KN_EIGEN
+// the iterations it declines, the Newton-Schulz kernel (its matrices in shared
+// memory for l <= 80, in vwork above), and the eigendecomposition only where
+// Newton-Schulz fails; KN_NEWTON_SCHULZ starts at Newton-Schulz; KN_EIGEN
 // always uses the eigendecomposition.
 // When the context's iteration guard is set, the step is skipped for an
 // iteration past convergence, and scal->stop_it is set to the guard

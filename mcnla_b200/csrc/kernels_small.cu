@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(kSyevThreads) k_kn_step(int l, const double* z
 }
 
 // ---------------------------------------------------------------------------
-// Kolmogorov-Nagumo step by matrix functions (l <= 80)
+// Kolmogorov-Nagumo step by matrix functions
 //
 // The step needs C = f(Z) and inv(C) for f(x) = sqrt(1/2 + sqrt(1/4 - x)),
 // which the reference forms from an eigendecomposition of Z
@@ -223,7 +223,8 @@ __global__ void __launch_bounds__(kSyevThreads) k_kn_step(int l, const double* z
 // eq. 6.35; inversion-free, built from matrix products only):
 //   S = (I - 4Z)^(1/2)            -> sqrt(1/4 - Z) = S/2
 //   C = ((I + S)/2)^(1/2), inv(C) = ((I + S)/2)^(-1/2)
-// The products run on the FP64 MMA inside one CTA.  Jacobi on the
+// The products run on the FP64 MMA inside one CTA, on matrices in shared
+// memory (l <= 80) or in global memory (L2-resident, l <= 160).  Jacobi on the
 // clustered spectrum Z has near convergence (dozens of near-zero
 // eigenvalues) needs 15-20 sweeps; the iteration above needs a handful of
 // products.  When an iteration fails (non-finite values or no convergence,
@@ -306,23 +307,28 @@ __device__ int cta_ns_sqrt(double*& Y, double*& Zm, double*& T, double*& W, int 
   return -1;
 }
 
-__global__ void __launch_bounds__(kSmallThreads) k_kn_step_ns(int l, const double* z_in, const double* dd,
-                                                              double inv_n, double* out, double* outn,
-                                                              const double* ff, double* ffn, double* vwork,
-                                                              DevScalars* scal, double tol, const int* guard_stop,
-                                                              int guard_it, const int* only_if) {
+// GMEM: the four matrices live in vwork (global memory, L2-resident) instead of
+// shared memory (80 < l <= 160); a failed iteration then sets
+// scal->kn_ns_failed, and the launcher's eigendecomposition kernel after it
+// takes the step (it returns at once otherwise).
+template <bool GMEM>
+__global__ void __launch_bounds__(GMEM ? kSyevThreads : kSmallThreads)
+    k_kn_step_ns(int l, const double* z_in, const double* dd, double inv_n, double* out, double* outn,
+                 const double* ff, double* ffn, double* vwork, DevScalars* scal, double tol, const int* guard_stop,
+                 int guard_it, const int* only_if) {
   extern __shared__ __align__(16) char smem_raw[];
+  if (GMEM && threadIdx.x == 0) scal->kn_ns_failed = 0;
   if (guard_stop && *guard_stop < guard_it) return;
   if (only_if && *only_if == 0) return;
   const int tid = threadIdx.x, nt = blockDim.x;
   const int lp = (l + 15) & ~15, ld = lp + 4;
   const size_t mat = size_t(lp) * ld;
-  double* buf = reinterpret_cast<double*>(smem_raw);
+  double* buf = GMEM ? vwork : reinterpret_cast<double*>(smem_raw);
   double* B0 = buf;
   double* B1 = buf + mat;
   double* B2 = buf + 2 * mat;
   double* B3 = buf + 3 * mat;
-  double* red = buf + 4 * mat;          // 64 doubles
+  double* red = GMEM ? reinterpret_cast<double*>(smem_raw) : buf + 4 * mat;   // 64 doubles
   double* sv = red + 64;                // 96 doubles (eigen fallback)
   const int ldd = 2 * l;
   // ---- Z (upper triangle mirrored, as a symmetric eigensolver reads it) into B0
@@ -368,6 +374,14 @@ __global__ void __launch_bounds__(kSmallThreads) k_kn_step_ns(int l, const doubl
     Y = Zm;
     Zm = tmp;
     it2 = cta_ns_sqrt(Y, Zm, T, W, l, lp, ld, red, 60);
+  }
+  if ((it1 < 0 || it2 < 0) && GMEM) {
+    // the eigendecomposition kernel launched after this one takes the step
+    if (tid == 0) {
+      scal->sweeps = -1;
+      scal->kn_ns_failed = 1;
+    }
+    return;
   }
   if (it1 < 0 || it2 < 0) {
     // eigendecomposition fallback (the reference's path, NaN semantics included)
@@ -902,13 +916,23 @@ int launch_kn_step(Context* c, int l, const double* z, const double* dd, double 
     const size_t smem = 4 * size_t(lp) * (lp + 4) * sizeof(double) + (64 + 96) * sizeof(double) +
                         jacobi_scratch_bytes(l) + 64;
     if (smem <= c->smem_optin) {
-      MB_CHECK(set_smem(c, reinterpret_cast<const void*>(k_kn_step_ns), smem));
-      k_kn_step_ns<<<1, kSmallThreads, smem, c->stream>>>(l, z, dd, inv_n, out, outn, ff, ffn, vwork, c->scal, tol,
-                                                          c->guard_stop, c->guard_it, only_if);
+      MB_CHECK(set_smem(c, reinterpret_cast<const void*>(k_kn_step_ns<false>), smem));
+      k_kn_step_ns<false><<<1, kSmallThreads, smem, c->stream>>>(l, z, dd, inv_n, out, outn, ff, ffn, vwork, c->scal,
+                                                                 tol, c->guard_stop, c->guard_it, only_if);
       c->kernels_launched++;
       MB_CHECK_CUDA(cudaGetLastError());
       return MCNLA_B200_OK;
     }
+  }
+  if (l > kKnNsMaxDim && c->kn_mode != MCNLA_B200_KN_EIGEN) {
+    // Newton-Schulz with its matrices in vwork (kn_series_work_doubles(l) covers them); the
+    // eigendecomposition kernel below runs only if it fails
+    const size_t smem = (64 + 96) * sizeof(double) + 64;
+    k_kn_step_ns<true><<<1, kSyevThreads, smem, c->stream>>>(l, z, dd, inv_n, out, outn, ff, ffn, vwork, c->scal, tol,
+                                                             c->guard_stop, c->guard_it, only_if);
+    c->kernels_launched++;
+    MB_CHECK_CUDA(cudaGetLastError());
+    only_if = &c->scal->kn_ns_failed;
   }
   const bool v_smem = small_smem_syev(l, true) + l * 8 + 64 <= c->smem_optin;
   const size_t smem = small_smem_syev(l, v_smem) + l * 8 + 64;

@@ -2,6 +2,7 @@
 // ceil(l/8) cooperative CTAs.  Launched in front of the matrix-function /
 // eigendecomposition step kernel, which runs only when this one declined
 // (scal->kn_fallback).
+#include <algorithm>
 #include "kn_series.cuh"
 
 namespace mb {
@@ -37,7 +38,12 @@ __global__ void __launch_bounds__(kSerThreads) k_kn_series(StepArgs a) {
 
 }  // namespace
 
-size_t kn_series_work_doubles(int l) { return 2 * size_t(l) * l + 3 * size_t((l + 7) / 8) + 8; }
+size_t kn_series_work_doubles(int l) {
+  // the series' scratch, or the four padded l x l matrices of the Newton-Schulz step where they do
+  // not fit in shared memory (l > 80)
+  const size_t lp = (size_t(l) + 15) & ~size_t(15);
+  return std::max(2 * size_t(l) * l + 3 * size_t((l + 7) / 8) + 8, l > 80 ? 4 * lp * (lp + 4) : 0);
+}
 
 int launch_kn_series(Context* c, int l, const double* z, const double* dd, double inv_n, double* out, double* outn,
                      const double* ff, double* ffn, double* work, double tol) {
