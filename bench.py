@@ -66,7 +66,8 @@ def parse():
                     help="reference arm: seconds of timed full solves; no step starts that would end past it")
     ap.add_argument("--quick", action="store_true", help="small shape for a smoke run")
     ap.add_argument("--no-serving", action="store_true", help="skip the batched / served leg")
-    ap.add_argument("--kernel", choices=["sketch_bf16", "gkn", "trace", "grouped"], default=None,
+    ap.add_argument("--kernel", choices=["sketch_bf16", "gkn", "trace", "grouped", "served_trace", "gkn_scaling"],
+                    default=None,
                     help="time one kernel alone (profiling case) instead of the benchmark: the BF16 sketch GEMM "
                          "on --m x --n x (--k + --p) --N with --parts parts, or the persistent row-block Gramian "
                          "KN integrator on the sketches of a seeded --m x --n matrix (sigma_j = 1/j, tol 1e-5); "
@@ -961,6 +962,125 @@ def run_trace(args, dev):
     return out
 
 
+def run_served_trace(args, dev, count=500):
+    """The served mix in throughput mode: `count` requests (5 % large: 65536 x 8192, k = 128,
+    p = 32, N = 16; the rest from 256 resident matrices of the uneven batch) submitted at once to
+    a --serve-workers server, mixed (3 BF16 parts, resident) and FP64; wall time, mean service
+    time per request kind, and per-kernel device time of a second pass (CUPTI activity records
+    through torch.profiler: every launch's own start and end, no replay)."""
+    import collections
+    import numpy as np
+    import torch
+    from torch.profiler import profile, ProfilerActivity
+    from mcnla_b200 import isvd, synthetic
+    W = args.serve_workers
+    shapes = synthetic.batch_shapes(256, seed=4)
+    pool = [synthetic.lowrank_torch(sh["m"], sh["n"], sh["sigma"], seed=sh["seed"], device=dev, dtype=torch.float32)
+            for sh in shapes]
+    lsh = [synthetic.large_shape(seed=s_) for s_ in (1, 2)]
+    large = [synthetic.lowrank_torch(x["m"], x["n"], x["sigma"], seed=x["seed"], device=dev, dtype=torch.float32)
+             for x in lsh]
+    parts = [isvd.resident_parts(a_, 3) for a_ in pool]
+    lparts = [isvd.resident_parts(a_, 3) for a_ in large]
+    torch.cuda.synchronize()
+    rng = np.random.default_rng(1000)
+    is_large = rng.random(count) < 0.05
+    pick = rng.integers(0, len(pool), count)
+
+    def request(j, mixed):
+        big = bool(is_large[j])
+        i = j % 2 if big else int(pick[j])
+        sh = lsh[i] if big else shapes[i]
+        sp, fsp = ((lparts[i] if big else parts[i]) if mixed else (None, None))
+        return isvd.Request(large[i] if big else pool[i], sh["k"], sh["p"], sh["N"], seed=sh["seed"],
+                            integrator="rb_gramian_kn", former="rb_gramian", maxit=256, tol=1e-5, mixed=mixed,
+                            split=sp, former_split=fsp)
+
+    out = {}
+    for name, mixed in (("mixed", 3), ("fp64", False)):
+        with isvd.Server(workers=W, budget_bytes=int(90e9), device=dev) as srv:
+            warm = [request(j, mixed) for j in range(32)]
+            for r in warm:
+                srv.submit(r)
+            for r in warm:
+                srv.wait(r)
+            torch.cuda.synchronize()
+            reqs = [request(j, mixed) for j in range(count)]
+            t0 = time.perf_counter()
+            for r in reqs:
+                srv.submit(r)
+            for r in reqs:
+                srv.wait(r)
+            torch.cuda.synchronize()
+            wall = time.perf_counter() - t0
+            kinds = collections.defaultdict(list)
+            for j, r in enumerate(reqs):
+                kinds["large" if is_large[j] else "k%d" % shapes[int(pick[j])]["k"]].append(r.result.seconds)
+            reqs = [request(j, mixed) for j in range(count)]
+            with profile(activities=[ProfilerActivity.CUDA]) as prof:
+                for r in reqs:
+                    srv.submit(r)
+                for r in reqs:
+                    srv.wait(r)
+                torch.cuda.synchronize()
+        agg = collections.defaultdict(lambda: [0, 0.0])
+        for e in prof.events():
+            if e.device_type.name == "CUDA" and e.time_range.end > e.time_range.start:
+                key = e.name.replace("(anonymous namespace)::", "").split("(")[0][:90]
+                agg[key][0] += 1
+                agg[key][1] += (e.time_range.end - e.time_range.start) / 1e3
+        top = sorted(agg.items(), key=lambda kv: -kv[1][1])[:16]
+        out[name] = {"wall_s": round(wall, 3), "solves_per_s": round(count / wall, 1),
+                     "kernel_ms_total": round(sum(v[1] for v in agg.values()), 1),
+                     "service_mean_ms": {k_: round(1e3 * float(np.mean(v)), 2) for k_, v in sorted(kinds.items())},
+                     "kernels": [{"name": k_, "launches": v[0], "ms": round(v[1], 1)} for k_, v in top]}
+    del pool, large, parts, lparts
+    torch.cuda.empty_cache()
+    return {"case": "served mix, throughput mode, %d requests, %d workers" % (count, W), **out}
+
+
+def run_gkn_scaling(args, dev):
+    """The persistent row-block Gramian KN integrator's time per iteration against its CTA share
+    (mcnla_b200_set_cta_limit) for l = 96, 48, 24 (N = 8, m = 8448, n = 2176, sigma_j = 1/j,
+    tol 1e-5): stage part timer, best of three calls."""
+    import numpy as np
+    import torch
+    from mcnla_b200 import isvd, synthetic
+    ctx = isvd.context(dev)
+    rows = []
+    for k, p in ((64, 32), (32, 16), (16, 8)):
+        m, n, N = 8448, 2176, 8
+        l, L = k + p, (k + p) * N
+        a = synthetic.lowrank_torch(m, n, np.arange(1, min(m, n) + 1) ** -1.0, seed=1, device=dev)
+        prm = isvd.Parameters(device=dev).setSize(m, n).setRank(k).setOverRank(p).setNumSketch(N).sync()
+        sk = isvd.RowBlockGaussianProjectionSketcher(prm, 7)
+        sk.initialize()
+        q = prm.createCollectionQ()
+        sk(a, q)
+        orth = isvd.RowBlockGramianOrthogonalizer(prm)
+        orth.initialize()
+        orth(q)
+        try:
+            for ctas in (18, 37, 74, 0):
+                ctx.set_cta_limit(ctas)
+                integ = isvd.RowBlockGramianKolmogorovNagumoIntegrator(prm, 256, 1e-5)
+                integ.initialize()
+                qbar = prm.createMatrixQbar()
+                integ(q, qbar)
+                t = 1e9
+                for _ in range(3):
+                    integ(q, qbar)
+                    t = min(t, integ.times()[1])
+                it = integ.iteration()
+                flops = 2.0 * L * L * l + 6.0 * L * l * l
+                rows.append({"l": l, "L": L, "ctas": ctas or torch.cuda.get_device_properties(dev).multi_processor_count, "iterations": it,
+                             "us_per_iteration": round(t / it * 1e6, 2), "tflops": round(flops * it / t / 1e12, 3)})
+        finally:
+            ctx.set_cta_limit(0)
+        del a, q
+    return {"kernel": "k_gkn_persistent", "rows": rows}
+
+
 def run_kernel_case(args, dev):
     import numpy as np
     import torch
@@ -970,6 +1090,10 @@ def run_kernel_case(args, dev):
     ctx = isvd.context(dev)
     if args.kernel == "trace":
         return run_trace(args, dev)
+    if args.kernel == "served_trace":
+        return run_served_trace(args, dev)
+    if args.kernel == "gkn_scaling":
+        return run_gkn_scaling(args, dev)
     if args.kernel == "grouped":
         # the grouped batch integrator on --batch-count copies of one shape (m x n, k, p = k/2, N = 8)
         shapes = [dict(sh, k=k, p=k // 2) for sh in synthetic.batch_shapes(args.batch_count, seed=4)]

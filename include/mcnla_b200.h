@@ -131,6 +131,12 @@ MCNLA_B200_API int mcnla_b200_set_autotune(mcnla_b200_ctx* ctx, int on);
  * either way.  Off: every iteration is launched.                             */
 MCNLA_B200_API int mcnla_b200_set_graph_loop(mcnla_b200_ctx* ctx, int on);
 
+/* SM share of the context's persistent cooperative kernels (the row-block
+ * Gramian KN integrator): at most `ctas` CTAs, 0 = one per SM.  For callers
+ * that run several contexts side by side on one GPU (the server sets it to
+ * SMs / workers for each worker's context).                                 */
+MCNLA_B200_API int mcnla_b200_set_cta_limit(mcnla_b200_ctx* ctx, int ctas);
+
 #define MCNLA_B200_KN_AUTO  0
 #define MCNLA_B200_KN_EIGEN 1
 #define MCNLA_B200_KN_NEWTON_SCHULZ 2

@@ -97,6 +97,7 @@ SIGNATURES = {
     "mcnla_b200_graph_replays": (_I64, [_P]),
     "mcnla_b200_set_kn_method": (_INT, [_P, _INT]),
     "mcnla_b200_set_autotune": (_INT, [_P, _INT]),
+    "mcnla_b200_set_cta_limit": (_INT, [_P, _INT]),
     "mcnla_b200_set_graph_loop": (_INT, [_P, _INT]),
     "mcnla_b200_last_times": (_INT, [_P, ctypes.POINTER(_D), _INT]),
     "mcnla_b200_initialize": (_INT, [_P, ctypes.POINTER(Params), _INT, _INT]),

@@ -191,6 +191,12 @@ int mcnla_b200_set_autotune(mcnla_b200_ctx* c, int on) {
   return MCNLA_B200_OK;
 }
 
+int mcnla_b200_set_cta_limit(mcnla_b200_ctx* c, int ctas) {
+  if (!c || ctas < 0) return MCNLA_B200_ERR_ARG;
+  c->coop_cta_limit = ctas;
+  return MCNLA_B200_OK;
+}
+
 int mcnla_b200_set_graph_loop(mcnla_b200_ctx* c, int on) {
   if (!c) return MCNLA_B200_ERR_ARG;
   c->graph_loop = on != 0;

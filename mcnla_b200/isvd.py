@@ -81,6 +81,10 @@ class Context:
         """GEMM tile autotuner on (default) or off (fixed shape heuristic)."""
         _lib.check(self.lib.mcnla_b200_set_autotune(self.handle, 1 if on else 0), "set_autotune")
 
+    def set_cta_limit(self, ctas):
+        """At most `ctas` CTAs for the persistent integrator kernels (0: one per SM)."""
+        _lib.check(self.lib.mcnla_b200_set_cta_limit(self.handle, int(ctas)), "set_cta_limit")
+
     def set_graph_loop(self, on):
         """KN iteration loops as replayed CUDA graphs (default on) or direct launches."""
         _lib.check(self.lib.mcnla_b200_set_graph_loop(self.handle, 1 if on else 0), "set_graph_loop")

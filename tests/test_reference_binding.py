@@ -3,8 +3,9 @@ specialise the reference's own Sketcher / Orthogonalizer / Integrator / Former t
 C ABI.  Here (CPU) it compiles against the reference's headers with the one-rank MPI stub the
 oracle uses; on a GPU the reference's stage templates run with those tags next to its CPU stages
 on the reference's own fixtures (tests/cpp/check_mcnla_tags.cpp, built by oracle/Makefile):
-81 KN iterations with Qbar within 1e-8 of qb_kn, and the orthogonalizer and formers within 1e-10
-of the CPU stages."""
+81 KN iterations with Qbar within 1e-8 of qb_kn, the orthogonalizer and formers within 1e-10
+of the CPU stages, and the row-block integrators again with their sums through the library's NCCL
+communicator (the attachment an MPI run makes, here at one rank)."""
 import os
 import subprocess
 
@@ -35,3 +36,5 @@ def test_reference_stage_templates_with_b200_tags(tmp_path, golden):
     assert r.returncode == 0, r.stdout + r.stderr
     assert "OK (0 failures)" in r.stdout
     assert "rb_gramian_kn B200 iterations 81, reference 81" in r.stdout
+    # the MPI row-block attachment: the library's NCCL communicator (one rank) carries the sums
+    assert "rb_kn over a one-rank NCCL communicator" in r.stdout
