@@ -6,8 +6,8 @@
 //
 // State (the same buffers and parity as the launch-per-product loop):
 // EB[i & 1] = [E~c | Bc | Bgc] (L x 3l), FF[i & 1] = F~c (l x l); Bs (L x L).
-// Iteration i (the products over 8 x 8 tiles spread over the grid, each
-// tile's sum split over the CTA's warps and added in a fixed order):
+// Iteration i (the products over 16 x 16 tiles spread over the grid, each
+// element the same fold of K chunks whatever the grid size; grid_tiles):
 //   P1  Bgc := 1/N Bs Bc                                              (:152)
 //   --- grid barrier
 //   P2  [Dc | Dgc] := 1/N Bc' [Bc | Bgc]                              (:155-158)
@@ -49,61 +49,104 @@ struct GknArgs {
   int smax;                 // power slabs of the series step
 };
 
+// Sum over k in [kb, ke) of one 16 x 16 tile with the m8n8k4 FP64 MMA: 2 x 2
+// register blocking (four DMMAs per pair of A and B fragment loads), the loads
+// of kU consecutive k-steps issued before their MMAs, two chains (even and odd
+// k-steps) added at the end; s[ib][jb][h] := the lane's elements.
+template <class FA, class FB>
+__device__ __forceinline__ void tile_chunk(FA fa, FB fb, int i0, int j0, bool iv0, bool iv1, bool jv0, bool jv1, int kb,
+                                           int ke, double (&s)[2][2][2]) {
+  const int t4 = threadIdx.x & 3;
+  const int i1 = i0 + 8, j1 = j0 + 8;
+  double c[2][2][2], e[2][2][2];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    (&c[0][0][0])[q] = 0.0;
+    (&e[0][0][0])[q] = 0.0;
+  }
+  for (int k = kb; k < ke; k += 4 * kU) {
+    double a0[kU], a1[kU], b0[kU], b1[kU];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      const int kk = k + 4 * u + t4;
+      const bool kv = kk < ke;
+      a0[u] = kv && iv0 ? fa(i0, kk) : 0.0;
+      a1[u] = kv && iv1 ? fa(i1, kk) : 0.0;
+      b0[u] = kv && jv0 ? fb(kk, j0) : 0.0;
+      b1[u] = kv && jv1 ? fb(kk, j1) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < kU; u += 2) {
+      dmma(c[0][0][0], c[0][0][1], a0[u], b0[u]);
+      dmma(c[0][1][0], c[0][1][1], a0[u], b1[u]);
+      dmma(c[1][0][0], c[1][0][1], a1[u], b0[u]);
+      dmma(c[1][1][0], c[1][1][1], a1[u], b1[u]);
+      dmma(e[0][0][0], e[0][0][1], a0[u + 1], b0[u + 1]);
+      dmma(e[0][1][0], e[0][1][1], a0[u + 1], b1[u + 1]);
+      dmma(e[1][0][0], e[1][0][1], a1[u + 1], b0[u + 1]);
+      dmma(e[1][1][0], e[1][1][1], a1[u + 1], b1[u + 1]);
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 8; ++q) (&s[0][0][0])[q] = (&c[0][0][0])[q] + (&e[0][0][0])[q];
+}
+
 // out(i, j) := sum_k A(i, k) B(k, j) for an M x N product over 16 x 16 tiles
-// distributed round-robin over the grid's CTAs.  In a CTA, warp w sums k in
-// its eighth of K for all four 8 x 8 quarters of the tile (2 x 2 register
-// blocking: four DMMAs per pair of A and B fragment loads) and the partial
-// tiles are added in warp order through shared memory (red: kGknWarps x 256
-// doubles), so the result does not depend on the grid size; every element
-// sees the same sequence of DMMA steps as with one 8 x 8 tile per pass.
+// distributed round-robin over the grid.  Every element is the same fold:
+// K is cut into kGknWarps chunks (a function of K alone), each chunk summed by
+// tile_chunk, and the chunk sums added in chunk order starting from zero.
+// Two ways to compute it, chosen per launch (the bits do not change):
+//  * fewer tiles than the grid has warps: a CTA takes one tile at a time,
+//    warp w sums chunk w, and the chunk sums are folded in warp order through
+//    shared memory (red: kGknWarps x 256 doubles, two block barriers);
+//  * otherwise a warp takes whole tiles and folds their chunks itself (no
+//    shared memory, no barrier) — on a small share of the SMs (a server
+//    worker's) the reduction and its barriers dominated.
 // fa(i, k), fb(k, j) load operands; fo(i, j, v) stores.
 template <class FA, class FB, class FO>
 __device__ void grid_tiles(FA fa, FB fb, FO fo, int M, int N, int K, double* red) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane >> 2, t4 = lane & 3;
-  const int mt = (M + 15) >> 4, ntl = (N + 15) >> 4;
+  const int mt = (M + 15) >> 4, ntl = (N + 15) >> 4, ntiles = mt * ntl;
   const int chunk = ((K + kGknWarps - 1) / kGknWarps + 3) & ~3;
+  if (ntiles >= int(gridDim.x) * kGknWarps) {
+    for (int t = int(blockIdx.x) * kGknWarps + warp; t < ntiles; t += int(gridDim.x) * kGknWarps) {
+      const int ti = (t / ntl) * 16, tj = (t % ntl) * 16;
+      const int i0 = ti + g, j0 = tj + g;
+      double acc[2][2][2];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) (&acc[0][0][0])[q] = 0.0;
+      for (int w = 0; w < kGknWarps; ++w) {
+        const int kb = min(K, w * chunk), ke = min(K, kb + chunk);
+        double cs[2][2][2];
+        tile_chunk(fa, fb, i0, j0, i0 < M, i0 + 8 < M, j0 < N, j0 + 8 < N, kb, ke, cs);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) (&acc[0][0][0])[q] += (&cs[0][0][0])[q];
+      }
+#pragma unroll
+      for (int ib = 0; ib < 2; ++ib)
+#pragma unroll
+        for (int jb = 0; jb < 2; ++jb)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int i = ti + 8 * ib + g, j = tj + 8 * jb + 2 * t4 + h;
+            if (i < M && j < N) fo(i, j, acc[ib][jb][h]);
+          }
+    }
+    return;
+  }
   const int kb = min(K, warp * chunk), ke = min(K, kb + chunk);
-  for (int t = blockIdx.x; t < mt * ntl; t += gridDim.x) {
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int ti = (t / ntl) * 16, tj = (t % ntl) * 16;
-    const int i0 = ti + g, i1 = i0 + 8, j0 = tj + g, j1 = j0 + 8;
-    const bool iv0 = i0 < M, iv1 = i1 < M, jv0 = j0 < N, jv1 = j1 < N;
-    double c[2][2][2], e[2][2][2];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      (&c[0][0][0])[q] = 0.0;
-      (&e[0][0][0])[q] = 0.0;
-    }
-    for (int k = kb; k < ke; k += 4 * kU) {
-      double a0[kU], a1[kU], b0[kU], b1[kU];
-#pragma unroll
-      for (int u = 0; u < kU; ++u) {
-        const int kk = k + 4 * u + t4;
-        const bool kv = kk < ke;
-        a0[u] = kv && iv0 ? fa(i0, kk) : 0.0;
-        a1[u] = kv && iv1 ? fa(i1, kk) : 0.0;
-        b0[u] = kv && jv0 ? fb(kk, j0) : 0.0;
-        b1[u] = kv && jv1 ? fb(kk, j1) : 0.0;
-      }
-#pragma unroll
-      for (int u = 0; u < kU; u += 2) {
-        dmma(c[0][0][0], c[0][0][1], a0[u], b0[u]);
-        dmma(c[0][1][0], c[0][1][1], a0[u], b1[u]);
-        dmma(c[1][0][0], c[1][0][1], a1[u], b0[u]);
-        dmma(c[1][1][0], c[1][1][1], a1[u], b1[u]);
-        dmma(e[0][0][0], e[0][0][1], a0[u + 1], b0[u + 1]);
-        dmma(e[0][1][0], e[0][1][1], a0[u + 1], b1[u + 1]);
-        dmma(e[1][0][0], e[1][0][1], a1[u + 1], b0[u + 1]);
-        dmma(e[1][1][0], e[1][1][1], a1[u + 1], b1[u + 1]);
-      }
-    }
+    const int i0 = ti + g, j0 = tj + g;
+    double cs[2][2][2];
+    tile_chunk(fa, fb, i0, j0, i0 < M, i0 + 8 < M, j0 < N, j0 + 8 < N, kb, ke, cs);
 #pragma unroll
     for (int ib = 0; ib < 2; ++ib)
 #pragma unroll
       for (int jb = 0; jb < 2; ++jb)
 #pragma unroll
-        for (int h = 0; h < 2; ++h)
-          red[warp * 256 + (8 * ib + g) * 16 + 8 * jb + 2 * t4 + h] = c[ib][jb][h] + e[ib][jb][h];
+        for (int h = 0; h < 2; ++h) red[warp * 256 + (8 * ib + g) * 16 + 8 * jb + 2 * t4 + h] = cs[ib][jb][h];
     __syncthreads();
     {
       const int r = threadIdx.x >> 4, cc = threadIdx.x & 15;   // kGknThreads = 256 outputs
