@@ -998,7 +998,8 @@ def run_served_trace(args, dev, count=500):
 
     out = {}
     for name, mixed in (("mixed", 3), ("fp64", False)):
-        with isvd.Server(workers=W, budget_bytes=int(90e9), device=dev) as srv:
+        cap = int(min(90e9, torch.cuda.mem_get_info(dev)[0] - 12e9))   # room left by the resident matrices
+        with isvd.Server(workers=W, budget_bytes=cap, device=dev) as srv:
             warm = [request(j, mixed) for j in range(32)]
             for r in warm:
                 srv.submit(r)

@@ -367,6 +367,11 @@ typedef struct mcnla_b200_server mcnla_b200_server;
 
 /* Device bytes a problem needs while in flight (workspaces and sketches).   */
 MCNLA_B200_API int64_t mcnla_b200_problem_bytes(const mcnla_b200_problem* problem);
+/* `workers` host threads, each with its own context and stream.  Admission
+ * keeps the workers' device memory within budget_bytes: an idle worker counts
+ * the workspaces it holds between solves, a running one the larger of those
+ * and its problem's bytes; when the next problem does not fit while work is
+ * running, idle workers release the workspaces they hold.                   */
 MCNLA_B200_API int mcnla_b200_server_create(mcnla_b200_server** server, int device, int workers,
                                             int64_t budget_bytes);
 /* Queues a copy of *problem; returns at once with a ticket.                  */
@@ -376,7 +381,8 @@ MCNLA_B200_API int mcnla_b200_server_submit(mcnla_b200_server* server, const mcn
  * status, seconds and latency filled) to *out.  Each ticket can be waited on
  * once.                                                                      */
 MCNLA_B200_API int mcnla_b200_server_wait(mcnla_b200_server* server, int64_t ticket, mcnla_b200_problem* out);
-/* Bytes admitted right now and the most ever admitted at once.              */
+/* Estimated bytes of the problems in flight right now, and the most ever in
+ * flight at once.                                                            */
 MCNLA_B200_API int mcnla_b200_server_stats(mcnla_b200_server* server, int64_t* in_flight_bytes, int64_t* peak_bytes,
                                            int64_t* completed);
 /* Finishes the queued work, stops the workers and frees everything.        */

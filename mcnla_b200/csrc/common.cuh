@@ -126,6 +126,10 @@ struct Context {
 // carves aligned sub-buffers in order.
 int ctx_reserve(Context* c, size_t bytes);
 int ctx_reserve_pipeline(Context* c, size_t bytes);
+// Device bytes the context's arenas hold between calls, and releasing them
+// (stream-ordered; the next call grows them again).
+int64_t ctx_held_bytes(const Context* c);
+void ctx_trim(Context* c);
 // Returns nullptr when the carve would pass the reservation (callers check).
 template <class T>
 T* ctx_take(Context* c, size_t count) {

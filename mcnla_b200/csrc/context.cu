@@ -1,3 +1,4 @@
+#include <algorithm>
 // Context lifecycle, workspace arena, stage timers and status strings.
 #include "common.cuh"
 #include <cstdio>
@@ -31,7 +32,7 @@ int ctx_reserve(Context* c, size_t bytes) {
     c->arena = nullptr;
     c->arena_bytes = 0;
   }
-  const size_t want = bytes + (bytes >> 1);   // grow with headroom
+  const size_t want = bytes + std::min(bytes >> 1, size_t(256) << 20);   // grow with headroom
   cudaError_t e = cudaMallocAsync(&c->arena, want, c->stream);
   if (e != cudaSuccess) {
     (void)cudaGetLastError();
@@ -50,7 +51,7 @@ int ctx_reserve_pipeline(Context* c, size_t bytes) {
     c->parena = nullptr;
     c->parena_bytes = 0;
   }
-  const size_t want = bytes + (bytes >> 1);
+  const size_t want = bytes + std::min(bytes >> 1, size_t(256) << 20);
   cudaError_t e = cudaMallocAsync(&c->parena, want, c->stream);
   if (e != cudaSuccess) {
     (void)cudaGetLastError();
@@ -60,6 +61,18 @@ int ctx_reserve_pipeline(Context* c, size_t bytes) {
   }
   c->parena_bytes = want;
   return MCNLA_B200_OK;
+}
+
+int64_t ctx_held_bytes(const Context* c) {
+  return int64_t(c->arena_bytes) + int64_t(c->parena_bytes) + int64_t(c->comm_tmp_bytes);
+}
+
+void ctx_trim(Context* c) {
+  if (c->arena) cudaFreeAsync(c->arena, c->stream);
+  if (c->parena) cudaFreeAsync(c->parena, c->stream);
+  c->arena = c->parena = nullptr;
+  c->arena_bytes = c->parena_bytes = 0;
+  c->arena_top = 0;
 }
 
 int ctx_tic(Context* c) {

@@ -1,10 +1,15 @@
 // Served solves: a pool of host workers, each owning a context (its own
 // stream and workspaces), takes problems from a FIFO queue and runs whole
 // solves concurrently on the device (the batch entry point, which groups the
-// integrator iterations of a whole batch, is in stages.cu).  Admission: the queue head is
-// started when a worker is free and the estimated bytes of the problems in
-// flight, plus its own, stay within the budget (a problem larger than the
-// budget runs alone).  Results do not depend on what else is in flight:
+// integrator iterations of a whole batch, is in stages.cu).  Admission counts
+// every worker's device memory: an idle worker's workspaces as they are held
+// between solves, a running one's as the larger of those and its problem's
+// estimated bytes.  The queue head starts on a free worker when that sum stays
+// within the budget (a problem larger than the budget runs alone).  When the
+// head does not fit while work is running, idle workers release the
+// workspaces they hold (and grow them again on their next solve), so large
+// requests do not leave every worker holding their size; workspaces that
+// block nothing are kept.  Results do not depend on what else is in flight:
 // every kernel reduces in a fixed order.
 #include "common.cuh"
 #include "solve.cuh"
@@ -34,6 +39,9 @@ struct Job {
 };
 
 int64_t round8(int64_t x) { return (x + 7) & ~int64_t(7); }
+
+// Workspaces a blocked worker keeps rather than releases (they cannot matter).
+constexpr int64_t kKeepBytes = int64_t(64) << 20;
 
 }  // namespace
 
@@ -72,14 +80,16 @@ struct mcnla_b200_server {
   std::deque<int64_t> queue;
   std::unordered_map<int64_t, mb::Job> jobs;
   int64_t next_ticket = 1, in_flight = 0, peak = 0, completed = 0;
+  std::vector<int64_t> committed;   // per worker: held workspaces, or max(held, problem bytes) while running
+  int64_t committed_total = 0;
   int running = 0;
   bool stop = false;
   std::atomic<int> init_failures{0};
 
-  void worker();
+  void worker(int me);
 };
 
-void mcnla_b200_server::worker() {
+void mcnla_b200_server::worker(int me) {
   cudaSetDevice(device);
   cudaStream_t stream = nullptr;
   mcnla_b200_ctx* ctx = nullptr;
@@ -98,18 +108,45 @@ void mcnla_b200_server::worker() {
     int64_t bytes = 0;
     {
       std::unique_lock<std::mutex> lock(mu);
+      // the head fits beside what every worker holds; or nothing runs and no other worker holds
+      // more than it keeps anyway (the head alone is over the budget)
+      auto fits = [&] {
+        const int64_t b = jobs[queue.front()].bytes;
+        return committed_total - committed[me] + std::max(committed[me], b) <= budget;
+      };
+      auto alone = [&] {
+        return running == 0 && committed_total - committed[me] <= int64_t(nworkers - 1) * mb::kKeepBytes;
+      };
       cv_work.wait(lock, [&] {
         if (queue.empty()) return stop;
-        const int64_t b = jobs[queue.front()].bytes;
-        return running == 0 || in_flight + b <= budget;
+        return fits() || alone() || committed[me] > mb::kKeepBytes;
       });
       if (queue.empty()) break;
+      if (!fits() && !alone()) {
+        // this worker's idle workspaces stand in the head's way: release them and wait again
+        lock.unlock();
+        if (ok) {
+          mb::solve_scratch_free(ctx, scratch);
+          mb::ctx_trim(ctx);
+          cudaStreamSynchronize(stream);
+        }
+        const int64_t held = ok ? mb::ctx_held_bytes(ctx) : 0;
+        lock.lock();
+        committed_total += held - committed[me];
+        committed[me] = held;
+        lock.unlock();
+        cv_work.notify_all();
+        continue;
+      }
       ticket = queue.front();
       queue.pop_front();
       p = jobs[ticket].p;
       bytes = jobs[ticket].bytes;
       in_flight += bytes;
       running++;
+      const int64_t c = std::max(committed[me], bytes);
+      committed_total += c - committed[me];
+      committed[me] = c;
       peak = std::max(peak, in_flight);
     }
     int st = MCNLA_B200_ERR_CUDA;
@@ -125,6 +162,7 @@ void mcnla_b200_server::worker() {
     p.seconds = ms * 1e-3;
     std::string err;
     if (st != MCNLA_B200_OK) err = ok ? mb::last_error_text() : "worker initialization failed";
+    const int64_t held = ok ? mb::ctx_held_bytes(ctx) + mb::solve_scratch_bytes(scratch) : 0;
     {
       std::lock_guard<std::mutex> lock(mu);
       mb::Job& j = jobs[ticket];
@@ -135,6 +173,8 @@ void mcnla_b200_server::worker() {
       in_flight -= bytes;
       running--;
       completed++;
+      committed_total += held - committed[me];
+      committed[me] = held;
     }
     cv_done.notify_all();
     cv_work.notify_all();
@@ -159,7 +199,8 @@ int mcnla_b200_server_create(mcnla_b200_server** out, int device, int workers, i
   s->device = device;
   s->budget = budget_bytes;
   s->nworkers = workers;
-  for (int i = 0; i < workers; ++i) s->threads.emplace_back([s] { s->worker(); });
+  s->committed.assign(size_t(workers), 0);
+  for (int i = 0; i < workers; ++i) s->threads.emplace_back([s, i] { s->worker(i); });
   *out = s;
   return MCNLA_B200_OK;
 }

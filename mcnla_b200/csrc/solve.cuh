@@ -17,6 +17,9 @@ struct SolveScratch {
   size_t tsplit_bytes = 0;
 };
 void solve_scratch_free(Context* c, SolveScratch& s);
+inline int64_t solve_scratch_bytes(const SolveScratch& s) {
+  return int64_t(s.a64_bytes) + int64_t(s.split_bytes) + int64_t(s.tsplit_bytes);
+}
 // Scratch bytes a problem needs beyond its stage workspaces.
 size_t problem_scratch_bytes(const mcnla_b200_problem& p);
 // One whole solve (mcnla_b200_isvd, or mcnla_b200_isvd_mixed with the
