@@ -97,3 +97,36 @@ def test_server_reports_bad_problem_and_continues(cuda):
         for r in reqs:
             srv.wait(r)
             assert r.result.status == 0
+
+
+def test_server_tight_budget_with_held_workspaces(cuda):
+    """A budget of about two large problems and six workers: the workers that served the large
+    problems keep their workspaces between solves, and those workspaces count against the budget,
+    so the queue head can find them in its way; the idle workers then release them.  Every
+    problem completes, and each result is the same bits as with an ample budget."""
+    from mcnla_b200 import isvd, synthetic
+    small = _problems(cuda, 12, seed=5)
+    rng = np.random.default_rng(9)
+    big = []
+    for i in range(3):
+        a = torch.as_tensor(synthetic.lowrank_np(6000, 2500, np.arange(1, 2501) ** -1.0, seed=70 + i), device=cuda)
+        big.append(isvd.Request(a, 48, 24, 8, seed=int(rng.integers(1 << 30)), integrator="rb_gramian_kn",
+                                former="svd", tol=1e-5))
+    reqs = big[:1] + small[:4] + big[1:2] + small[4:8] + big[2:] + small[8:]
+    budget = 2 * max(r.bytes() for r in reqs) + max(r.bytes() for r in small)
+    with isvd.Server(workers=6, budget_bytes=budget) as srv:
+        for r in reqs:
+            srv.submit(r)
+        for r in reqs:
+            srv.wait(r)
+    tight = [(r.s.clone(), r.u.clone(), r.result.iteration) for r in reqs]
+    for r in reqs:
+        assert r.result.status == 0
+    with isvd.Server(workers=6, budget_bytes=150 << 30) as srv:
+        for r in reqs:
+            srv.submit(r)
+        for r in reqs:
+            srv.wait(r)
+    for r, (s0, u0, it0) in zip(reqs, tight):
+        assert r.result.iteration == it0
+        assert torch.equal(r.s, s0) and torch.equal(r.u, u0)
