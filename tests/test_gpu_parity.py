@@ -529,3 +529,34 @@ def test_graph_loop_matches_direct(cuda, integrator, shape):
     for s1, u1, v1, it1 in out[1:]:
         assert it1 == it0
         assert torch.equal(s1, s0) and torch.equal(u1, u0) and torch.equal(v1, v0)
+
+
+@pytest.mark.parametrize("l,N", [(96, 8), (48, 8), (20, 16)])
+def test_persistent_integrator_bits_do_not_depend_on_its_cta_share(cuda, l, N):
+    """The persistent row-block Gramian KN kernel folds every product element's K chunks in one
+    fixed order, by one warp per tile (when the product has at least as many tiles as the grid has
+    warps) or by the CTA's warps through shared memory: the same bits on 8, 18, 37 CTAs and the
+    whole GPU, and the oracle's iteration count."""
+    from mcnla_b200 import isvd, synthetic
+    m, n = 3000, 1200
+    a = synthetic.lowrank_np(m, n, np.arange(1, n + 1) ** -1.0, seed=l)
+    omega = np.random.default_rng(l + 1).standard_normal((n, l * N))
+    qs = O.orthogonalize_gramian(a @ omega, l, N)
+    qo, it_ref = O.INTEGRATORS["rb_gramian_kn"](qs, l, N, 256, 1e-5)
+    prm = params(m, n, l, 0, N)
+    ctx = isvd.context()
+    outs = []
+    try:
+        for ctas in (8, 18, 37, 0):
+            ctx.set_cta_limit(ctas)
+            integ = isvd.RowBlockGramianKolmogorovNagumoIntegrator(prm, 256, 1e-5)
+            integ.initialize()
+            qbar = prm.createMatrixQbar()
+            integ(dev(qs, cuda), qbar)
+            assert integ.iteration() == it_ref, ctas
+            outs.append(qbar.clone())
+    finally:
+        ctx.set_cta_limit(0)
+    for q in outs[1:]:
+        assert torch.equal(q, outs[0])
+    assert np.abs(host(outs[-1]) - qo).max() < TOL
