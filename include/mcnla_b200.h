@@ -211,6 +211,23 @@ MCNLA_B200_API int mcnla_b200_isvd(mcnla_b200_ctx* ctx, const mcnla_b200_params*
 MCNLA_B200_API int mcnla_b200_isvd_host(mcnla_b200_ctx* ctx, const mcnla_b200_params* params, int integrator, int former,
                          const double* A_host, int a_layout, const double* omega_host, int max_iteration,
                          double tolerance, double* S_host, double* U_host, double* V_host, int* iteration);
+/* Streamed ingest: the whole solve of a row-major A that the caller produces
+ * row block by row block, e.g. from a file (the reference's row-block
+ * loaders, include/mcnla/core/io/binary/dense_load.hpp:70-141 and
+ * matrix_market/dense_load_block.hpp, read into a host matrix before its
+ * stages start).  read_rows(user, row0, rows, buf) fills buf (rows x ncol,
+ * row-major, pinned host memory the library owns) with rows [row0, row0 +
+ * rows) of A and returns 0, or non-zero to abort the solve
+ * (MCNLA_B200_ERR_ARG).  Rows come in order, in blocks of at least 128 rows
+ * (about 1 GB at most, at least four blocks); while the device copies block
+ * b and sketches it, the caller reads block b + 1.  A stays on the device
+ * for the former.  The result is bit-identical to mcnla_b200_isvd_host's on
+ * the same A and Omega.                                                      */
+typedef int (*mcnla_b200_read_rows_fn)(void* user, int64_t row0, int64_t rows, double* buf);
+MCNLA_B200_API int mcnla_b200_isvd_stream(mcnla_b200_ctx* ctx, const mcnla_b200_params* params, int integrator,
+                                          int former, mcnla_b200_read_rows_fn read_rows, void* user,
+                                          const double* omega_host, int max_iteration, double tolerance,
+                                          double* S_host, double* U_host, double* V_host, int* iteration);
 
 /* ---- files (the reference's io module; host only, no device work) -----------
  * Dense MatrixMarket "array" text (include/mcnla/core/io/matrix_market/

@@ -74,6 +74,7 @@ _INT = ctypes.c_int
 
 # mcnla_b200_allreduce_fn: int (*)(void* user, double* buf, int64_t count, void* stream)
 ALLREDUCE_FN = ctypes.CFUNCTYPE(_INT, _P, _P, _I64, _P)
+READ_ROWS_FN = ctypes.CFUNCTYPE(_INT, _P, _I64, _I64, _P)
 NCCL_ID_BYTES = 128
 
 # name -> (restype, argtypes), one line per entry point of the header
@@ -110,6 +111,8 @@ SIGNATURES = {
                                _P, _P, _P, ctypes.POINTER(_INT)]),
     "mcnla_b200_isvd_host": (_INT, [_P, ctypes.POINTER(Params), _INT, _INT, _P, _INT, _P, _INT, _D, _P, _P, _P,
                                     ctypes.POINTER(_INT)]),
+    "mcnla_b200_isvd_stream": (_INT, [_P, ctypes.POINTER(Params), _INT, _INT, READ_ROWS_FN, _P, _P, _INT, _D, _P, _P,
+                                      _P, ctypes.POINTER(_INT)]),
     "mcnla_b200_dgemm": (_INT, [_P, _I64, _I64, _I64, _D, _P, _I64, _I64, _P, _I64, _I64, _D, _P, _I64, _I64, _INT]),
     "mcnla_b200_syev_batched": (_INT, [_P, _INT, _INT, _P, _P, _P, _INT]),
     "mcnla_b200_inverse_batched": (_INT, [_P, _INT, _INT, _P]),

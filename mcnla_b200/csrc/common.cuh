@@ -64,6 +64,8 @@ struct Context {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaStream_t copy_stream = nullptr;   // host-to-device copies overlapped with compute (created on first use)
+  void* stage_host[2] = {nullptr, nullptr};   // pinned staging of the streamed ingest (grown on demand)
+  size_t stage_host_bytes = 0;
   bool own_stream = false;
   int num_sms = 148;
   size_t smem_optin = 0;

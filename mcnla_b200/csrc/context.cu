@@ -177,6 +177,8 @@ int mcnla_b200_destroy(mcnla_b200_ctx* c) {
   if (c->scal_host) cudaFreeHost(c->scal_host);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+  for (void* h : c->stage_host)
+    if (h) cudaFreeHost(h);
   delete c;
   return MCNLA_B200_OK;
 }

@@ -1075,46 +1075,119 @@ int run_isvd(Context* c, const Dims& d, int integrator, int former, const double
 // starts as soon as its block has landed, so the copy of A hides behind the
 // sketch.  Each block's GEMM uses the split-K count of the whole product, so
 // every element of Q equals the whole-product GEMM's.
-int run_sketch_streamed(Context* c, const Dims& d, const double* A_host, double* A, const double* omega_host,
-                        double* omega, double* Q) {
+// Row blocks of a sketch streamed from host memory: at least 128 rows, about
+// 1 GB at most, at least four blocks; each block's GEMM uses the split-K count
+// of the whole product, so the result is the device-resident sketch's bit for
+// bit.
+struct RowBlocks {
+  int64_t rows_per;
+  int nblocks;
+  int splits;
+};
+
+RowBlocks stream_blocks(Context* c, const Dims& d) {
   const size_t row_bytes = size_t(d.n) * sizeof(double);
-  const int64_t rows_per = std::max<int64_t>(
-      128, std::min<int64_t>(int64_t((size_t(1) << 30) / row_bytes), cdiv(d.m, 4)));
-  const int nblocks = int(cdiv(d.m, rows_per));
-  const int splits = dgemm_heuristic_splits(c, d.m, d.L, d.n, 1);
-  const size_t wsb = splits > 1 ? size_t(splits) * rows_per * d.L * sizeof(double) : 0;
+  RowBlocks rb;
+  rb.rows_per = std::max<int64_t>(128, std::min<int64_t>(int64_t((size_t(1) << 30) / row_bytes), cdiv(d.m, 4)));
+  rb.nblocks = int(cdiv(d.m, rb.rows_per));
+  rb.splits = dgemm_heuristic_splits(c, d.m, d.L, d.n, 1);
+  return rb;
+}
+
+// The common part of the streamed sketches: the GEMM workspace, the copy
+// stream, one event per block (plus one ordering the copies after the work
+// already queued on the compute stream) and Omega copied ahead of the blocks.
+struct StreamSetup {
+  std::vector<cudaEvent_t> ev;
+  double* ws = nullptr;
+  ~StreamSetup() {
+    for (auto e : ev)
+      if (e) cudaEventDestroy(e);
+  }
+};
+
+int stream_setup(Context* c, const Dims& d, const RowBlocks& rb, const double* omega_host, double* omega,
+                 StreamSetup& st) {
+  const size_t wsb = rb.splits > 1 ? size_t(rb.splits) * rb.rows_per * d.L * sizeof(double) : 0;
   Plan pl;
   pl.add(wsb / 8 + 1);
   MB_CHECK(ctx_reserve(c, pl.bytes));
-  double* ws = take_ws(c, wsb);
+  st.ws = take_ws(c, wsb);
   MB_CHECK(check_arena(c));
   if (!c->copy_stream) MB_CHECK_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
-  std::vector<cudaEvent_t> ev(size_t(nblocks) + 1, nullptr);
-  struct Events {
-    std::vector<cudaEvent_t>& v;
-    ~Events() { for (auto e : v) if (e) cudaEventDestroy(e); }
-  } release{ev};
-  for (auto& e : ev) MB_CHECK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  st.ev.assign(size_t(rb.nblocks) + 1, nullptr);
+  for (auto& e : st.ev) MB_CHECK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   // the copies start after the work already queued on the compute stream (which may still use the buffers)
-  MB_CHECK_CUDA(cudaEventRecord(ev[nblocks], c->stream));
-  MB_CHECK_CUDA(cudaStreamWaitEvent(c->copy_stream, ev[nblocks], 0));
+  MB_CHECK_CUDA(cudaEventRecord(st.ev[rb.nblocks], c->stream));
+  MB_CHECK_CUDA(cudaStreamWaitEvent(c->copy_stream, st.ev[rb.nblocks], 0));
   MB_CHECK_CUDA(cudaMemcpyAsync(omega, omega_host, size_t(d.n) * d.L * sizeof(double), cudaMemcpyHostToDevice,
                                 c->copy_stream));
-  for (int b = 0; b < nblocks; ++b) {
-    const int64_t r0 = b * rows_per, rows = std::min<int64_t>(rows_per, d.m - r0);
-    MB_CHECK_CUDA(cudaMemcpyAsync(A + r0 * d.n, A_host + r0 * d.n, size_t(rows) * row_bytes, cudaMemcpyHostToDevice,
-                                  c->copy_stream));
-    MB_CHECK_CUDA(cudaEventRecord(ev[b], c->copy_stream));
-  }
   MB_CHECK(ctx_tic(c));
   MB_CHECK(ctx_toc(c));   // "random generating" part: Omega is given
-  for (int b = 0; b < nblocks; ++b) {
-    const int64_t r0 = b * rows_per, rows = std::min<int64_t>(rows_per, d.m - r0);
-    MB_CHECK_CUDA(cudaStreamWaitEvent(c->stream, ev[b], 0));
-    MB_CHECK(dgemm(c, rows, d.L, d.n, 1.0, crow(A + r0 * d.n, d.n), crow(omega, d.L), 0.0, drow(Q + r0 * d.L, d.L),
-                   GemmBatch(), ws, splits));
+  return MCNLA_B200_OK;
+}
+
+int sketch_block(Context* c, const Dims& d, const RowBlocks& rb, const StreamSetup& st, int b, const double* A,
+                 const double* omega, double* Q) {
+  const int64_t r0 = b * rb.rows_per, rows = std::min<int64_t>(rb.rows_per, d.m - r0);
+  MB_CHECK_CUDA(cudaStreamWaitEvent(c->stream, st.ev[b], 0));
+  return dgemm(c, rows, d.L, d.n, 1.0, crow(A + r0 * d.n, d.n), crow(omega, d.L), 0.0, drow(Q + r0 * d.L, d.L),
+               GemmBatch(), st.ws, rb.splits);
+}
+
+int run_sketch_streamed(Context* c, const Dims& d, const double* A_host, double* A, const double* omega_host,
+                        double* omega, double* Q) {
+  const RowBlocks rb = stream_blocks(c, d);
+  StreamSetup st;
+  MB_CHECK(stream_setup(c, d, rb, omega_host, omega, st));
+  for (int b = 0; b < rb.nblocks; ++b) {
+    const int64_t r0 = b * rb.rows_per, rows = std::min<int64_t>(rb.rows_per, d.m - r0);
+    MB_CHECK_CUDA(cudaMemcpyAsync(A + r0 * d.n, A_host + r0 * d.n, size_t(rows) * d.n * sizeof(double),
+                                  cudaMemcpyHostToDevice, c->copy_stream));
+    MB_CHECK_CUDA(cudaEventRecord(st.ev[b], c->copy_stream));
+  }
+  for (int b = 0; b < rb.nblocks; ++b) MB_CHECK(sketch_block(c, d, rb, st, b, A, omega, Q));
+  MB_CHECK(ctx_toc(c));
+  return MCNLA_B200_OK;
+}
+
+// Streamed ingest: the caller's reader fills pinned staging buffers (two,
+// alternating) block by block; block b's copy and GEMM run on the device while
+// the reader fills block b + 1.
+int run_sketch_ingest(Context* c, const Dims& d, mcnla_b200_read_rows_fn read_rows, void* user, double* A,
+                      const double* omega_host, double* omega, double* Q) {
+  const RowBlocks rb = stream_blocks(c, d);
+  const size_t stage = size_t(rb.rows_per) * d.n * sizeof(double);
+  if (c->stage_host_bytes < stage) {
+    MB_CHECK_CUDA(cudaStreamSynchronize(c->copy_stream ? c->copy_stream : c->stream));
+    for (auto& h : c->stage_host) {
+      if (h) cudaFreeHost(h);
+      h = nullptr;
+    }
+    c->stage_host_bytes = 0;
+    for (auto& h : c->stage_host) MB_CHECK_CUDA(cudaHostAlloc(&h, stage, cudaHostAllocDefault));
+    c->stage_host_bytes = stage;
+  }
+  StreamSetup st;
+  MB_CHECK(stream_setup(c, d, rb, omega_host, omega, st));
+  for (int b = 0; b < rb.nblocks; ++b) {
+    const int64_t r0 = b * rb.rows_per, rows = std::min<int64_t>(rb.rows_per, d.m - r0);
+    double* buf = static_cast<double*>(c->stage_host[b & 1]);
+    if (b >= 2) MB_CHECK_CUDA(cudaEventSynchronize(st.ev[b - 2]));   // the buffer's last copy has landed
+    if (read_rows(user, r0, rows, buf) != 0) {
+      cudaStreamSynchronize(c->copy_stream);
+      set_last_message("the row reader returned an error for rows " + std::to_string(r0) + " .. " +
+                       std::to_string(r0 + rows));
+      return MCNLA_B200_ERR_ARG;
+    }
+    MB_CHECK_CUDA(cudaMemcpyAsync(A + r0 * d.n, buf, size_t(rows) * d.n * sizeof(double), cudaMemcpyHostToDevice,
+                                  c->copy_stream));
+    MB_CHECK_CUDA(cudaEventRecord(st.ev[b], c->copy_stream));
+    MB_CHECK(sketch_block(c, d, rb, st, b, A, omega, Q));
   }
   MB_CHECK(ctx_toc(c));
+  // the staging buffers are free again once the last copies have landed
+  MB_CHECK_CUDA(cudaStreamSynchronize(c->copy_stream));
   return MCNLA_B200_OK;
 }
 
@@ -1836,6 +1909,44 @@ int mcnla_b200_isvd_host(mcnla_b200_ctx* ctx, const mcnla_b200_params* params, i
     MB_CHECK(mb::run_isvd(ctx, d, integrator, former, A, a_layout, lda, omega_dev, 0, max_iteration, tolerance, S,
                           U, V, iteration, pbase));
   }
+  MB_CHECK_CUDA(cudaMemcpyAsync(S_host, S, size_t(d.k) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  if (U_host)
+    MB_CHECK_CUDA(cudaMemcpyAsync(U_host, U, size_t(d.m) * d.k * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  if (V_host)
+    MB_CHECK_CUDA(cudaMemcpyAsync(V_host, V, size_t(d.n) * d.k * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  MB_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
+  return MCNLA_B200_OK;
+}
+
+int mcnla_b200_isvd_stream(mcnla_b200_ctx* ctx, const mcnla_b200_params* params, int integrator, int former,
+                           mcnla_b200_read_rows_fn read_rows, void* user, const double* omega_host, int max_iteration,
+                           double tolerance, double* S_host, double* U_host, double* V_host, int* iteration) {
+  if (!ctx || !read_rows || !omega_host || !iteration || !S_host) return MCNLA_B200_ERR_ARG;
+  Dims d;
+  MB_CHECK(mb::get_dims(params, d));
+  MB_CHECK_CUDA(cudaSetDevice(ctx->device));
+  const size_t a_elems = size_t(d.m) * d.n;
+  const size_t io = mb::arena_bytes_for(a_elems, 8) + mb::arena_bytes_for(size_t(d.k), 8) +
+                    mb::arena_bytes_for(size_t(d.m) * d.k, 8) + mb::arena_bytes_for(size_t(d.n) * d.k, 8);
+  MB_CHECK(mb::ctx_reserve_pipeline(ctx, io + mb::pipeline_bytes(d)));
+  char* base = static_cast<char*>(ctx->parena);
+  double* A = reinterpret_cast<double*>(base);
+  base += mb::arena_bytes_for(a_elems, 8);
+  double* S = reinterpret_cast<double*>(base);
+  base += mb::arena_bytes_for(size_t(d.k), 8);
+  double* U = reinterpret_cast<double*>(base);
+  base += mb::arena_bytes_for(size_t(d.m) * d.k, 8);
+  double* V = reinterpret_cast<double*>(base);
+  base += mb::arena_bytes_for(size_t(d.n) * d.k, 8);
+  double* Q = reinterpret_cast<double*>(base);
+  double* Qbar = reinterpret_cast<double*>(base + mb::arena_bytes_for(size_t(d.m) * d.L, 8));
+  double* omega_dev = reinterpret_cast<double*>(base + mb::arena_bytes_for(size_t(d.m) * d.L, 8) +
+                                                mb::arena_bytes_for(size_t(d.m) * d.l, 8));
+  MB_CHECK_CUDA(cudaMemsetAsync(ctx->scal, 0, sizeof(mb::DevScalars), ctx->stream));
+  MB_CHECK(mb::run_sketch_ingest(ctx, d, read_rows, user, A, omega_host, omega_dev, Q));
+  MB_CHECK(mb::run_orthogonalize(ctx, d, Q));
+  MB_CHECK(mb::run_integrate(ctx, d, integrator, Q, max_iteration, tolerance, Qbar, iteration));
+  MB_CHECK(mb::run_form(ctx, d, former, A, MCNLA_B200_ROW_MAJOR, d.n, Qbar, S, U, V));
   MB_CHECK_CUDA(cudaMemcpyAsync(S_host, S, size_t(d.k) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   if (U_host)
     MB_CHECK_CUDA(cudaMemcpyAsync(U_host, U, size_t(d.m) * d.k * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));

@@ -87,6 +87,22 @@ def save_binary(path, a, comment=None):
                                                   comment.encode() if comment else None), "binary_save")
 
 
+def binary_row_reader(path):
+    """(m, n, read_rows) for a row-major MCNLA dense binary matrix file (dims {n, m}):
+    read_rows(row0, rows, buf) loads rows [row0, row0 + rows) straight into the float64 buffer
+    at address buf (the reference's loadBinaryRowBlock), for isvd.solve_stream."""
+    dims, _ = binary_size(path)
+    if len(dims) != 2:
+        raise ValueError("%s: not a matrix" % path)
+    n, m = dims
+    lib = _lib.load()
+    p = _path(path)
+
+    def read_rows(row0, rows, buf):
+        _lib.check(lib.mcnla_b200_binary_load(p, int(row0), int(rows), ctypes.c_void_p(buf)), "binary_load")
+    return m, n, read_rows
+
+
 def to_device(a, device="cuda"):
     """A host matrix on the device as float64, staged through pinned memory; a column-major
     array stays column-major (the transposed view of a row-major device tensor)."""

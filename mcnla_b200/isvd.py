@@ -34,7 +34,7 @@ __all__ = [
     "KolmogorovNagumoIntegrator", "RowBlockKolmogorovNagumoIntegrator", "RowBlockGramianKolmogorovNagumoIntegrator",
     "RowBlockWenYinIntegrator", "RowBlockGramianWenYinIntegrator",
     "SvdFormer", "GramianFormer", "RowBlockGramianFormer", "ColBlockGramianFormer",
-    "solve", "solve_host", "Split", "split_bf16", "gaussian_bf16", "gemm_bf16", "solve_mixed",
+    "solve", "solve_host", "solve_stream", "Split", "split_bf16", "gaussian_bf16", "gemm_bf16", "solve_mixed",
     "Request", "Server", "solve_batched", "solve_grouped", "grouped_times", "resident_parts",
 ]
 
@@ -628,6 +628,42 @@ def solve_host(a_host, omega_host, k, p, N, integrator="kn", former="svd", maxit
                                             _ptr(a_host), _lib.COL_MAJOR if colmajor else _lib.ROW_MAJOR,
                                             _ptr(omega_host), maxit, tol, _ptr(s), _ptr(u), _ptr(v),
                                             ctypes.byref(it)), "isvd_host")
+    return s, u, v, it.value
+
+
+def solve_stream(read_rows, m, n, omega_host, k, p, N, integrator="kn", former="svd", maxit=256, tol=1e-4,
+                 out=None, device=None):
+    """One whole iSVD of a row-major m x n A that ``read_rows(row0, rows, buf)`` produces block by
+    block (``buf``: the address of a pinned rows x n float64 buffer to fill; e.g.
+    io.binary_row_reader(path)), through ``mcnla_b200_isvd_stream``: each block is copied and
+    sketched on the device while the next one is read.  omega_host: CPU float64 n x (N*l).
+    Returns (S, U, V, iterations) as CPU tensors, bit-identical to solve_host on the same A."""
+    if omega_host.is_cuda or omega_host.dtype != torch.float64 or not omega_host.is_contiguous():
+        raise TypeError("Omega must be a contiguous CPU float64 tensor")
+    if out is None:
+        out = (torch.empty(k, dtype=torch.float64, pin_memory=True),
+               torch.empty(m, k, dtype=torch.float64, pin_memory=True),
+               torch.empty(n, k, dtype=torch.float64, pin_memory=True))
+    s, u, v = out
+    failure = []
+
+    def call(_user, row0, rows, buf):
+        try:
+            read_rows(int(row0), int(rows), int(buf))
+            return 0
+        except Exception as e:            # reported by the library as a reader error
+            failure.append(e)
+            return 1
+    cb = _lib.READ_ROWS_FN(call)
+    prm = _lib.Params(m, n, k, p, N)
+    ctx = context(device)
+    it = ctypes.c_int()
+    st = ctx.lib.mcnla_b200_isvd_stream(ctx.bind(), ctypes.byref(prm), INTEGRATORS[integrator], FORMERS[former], cb,
+                                        None, _ptr(omega_host), maxit, tol, _ptr(s), _ptr(u), _ptr(v),
+                                        ctypes.byref(it))
+    if failure:
+        raise failure[0]
+    _lib.check(st, "isvd_stream")
     return s, u, v, it.value
 
 

@@ -6,9 +6,11 @@
 
 The positional arguments and their defaults are the reference drivers' (N = 16, k = 20,
 p = 12, tol = 1e-3, maxiter = 256; src/isvd_dense_rb.cpp:66-94).  A is read from a dense
-MatrixMarket file (or an MCNLA dense binary file with --binary) into pinned host memory and
-solved through the host-buffer entry point (mcnla_b200_isvd_host), which copies a large
-row-major A to the device in row blocks behind the sketch.  The stages default to the drivers'
+MatrixMarket file into pinned host memory and solved through the host-buffer entry point
+(mcnla_b200_isvd_host), which copies a large row-major A to the device in row blocks behind the
+sketch.  An MCNLA dense binary file (--binary, row-block layout) is streamed instead: its row
+blocks are read into the library's pinned staging buffers while the device copies and sketches
+the previous ones (mcnla_b200_isvd_stream).  The stages default to the drivers'
 choices: the row-block driver's Gramian orthogonalizer, row-block Wen-Yin integrator and
 row-block Gramian former (src/isvd_dense_rb.cpp:12-34); --layout cb keeps A column-major and
 uses the column-block Gramian former (src/isvd_dense_cb.cpp:20-34).  Omega is drawn from the
@@ -100,6 +102,21 @@ def frobenius_error(a_dev, s, u, v, colmajor=False):
     return num, den
 
 
+def frobenius_error_stream(read_rows, m, n, s, u, v, block=8192):
+    """The drivers' check for a streamed A: the file's row blocks read again into pinned memory
+    and compared on the device block by block."""
+    import torch
+    buf = torch.empty(min(block, m), n, dtype=torch.float64, pin_memory=True)
+    num = den = 0.0
+    for r0 in range(0, m, block):
+        rows = min(block, m - r0)
+        read_rows(r0, rows, buf.data_ptr())
+        blk = buf[:rows].to(u.device)
+        num += float(((blk - (u[r0:r0 + rows] * s) @ v.t()) ** 2).sum().item())
+        den += float((blk * blk).sum().item())
+    return num, den
+
+
 def main(argv=None):
     args = parse(argv)
     import torch
@@ -123,6 +140,11 @@ def main(argv=None):
             m, n = dims[1], dims[0]
         r0, r1 = rowblock.row_range(m, world, rank)
         a_host, _, _ = load_a(args, rows=(r0, r1 - r0))
+    elif args.binary and args.layout == "rb":
+        # streamed ingest: the file's row blocks go to the device behind the sketch
+        m, n, read_rows = io.binary_row_reader(args.a_file)
+        a_host = None
+        r0, r1 = 0, m
     else:
         a_host, m, n = load_a(args)
         r0, r1 = 0, m
@@ -143,6 +165,10 @@ def main(argv=None):
         s, u, v, it = isvd.solve(a_dev, k, p, N, omega=omega, integrator=args.integrator, former=args.former,
                                  maxit=args.maxiter, tol=args.tolerance)
         torch.cuda.synchronize()
+    elif a_host is None:
+        s, u, v, it = isvd.solve_stream(read_rows, m, n, omega_host, k, p, N, integrator=args.integrator,
+                                        former=args.former, maxit=args.maxiter, tol=args.tolerance, device=dev)
+        s, u, v = s.to(dev), u.to(dev), v.to(dev)
     else:
         s, u, v, it = isvd.solve_host(a_host, omega_host, k, p, N, integrator=args.integrator, former=args.former,
                                       maxit=args.maxiter, tol=args.tolerance, colmajor=args.layout == "cb",
@@ -150,7 +176,10 @@ def main(argv=None):
         a_dev = a_host.to(dev)
         s, u, v = s.to(dev), u.to(dev), v.to(dev)
     elapsed = time.perf_counter() - t0
-    num, den = frobenius_error(a_dev, s, u, v, colmajor=args.layout == "cb")
+    if a_host is None:
+        num, den = frobenius_error_stream(read_rows, m, n, s, u, v)
+    else:
+        num, den = frobenius_error(a_dev, s, u, v, colmajor=args.layout == "cb")
     if world > 1:
         import torch.distributed as dist
         t = torch.tensor([num, den], dtype=torch.float64, device=dev)

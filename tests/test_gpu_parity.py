@@ -399,6 +399,44 @@ def test_host_entry_point_streams_large_a(cuda, m, n):
         assert torch.equal(s1.cpu(), s2) and torch.equal(u1.cpu(), u2) and torch.equal(v1.cpu(), v2)
 
 
+@pytest.mark.parametrize("m,n", [(2048, 4096), (101, 1001)])
+def test_streamed_ingest_from_a_binary_file(cuda, tmp_path, m, n):
+    """mcnla_b200_isvd_stream with the binary file's row reader (the reference's loadBinaryRowBlock):
+    the file's row blocks are read into pinned staging while the previous ones are copied and
+    sketched; the result is bit for bit the host-buffer solve's and the device-resident solve's.
+    A reader that fails stops the solve with its error."""
+    from mcnla_b200 import io, isvd, synthetic
+    a, omega = synthetic.config1_numpy(m=m, n=n, k=8, p=8, N=4, seed=3)
+    path = tmp_path / "a.bin"
+    io.save_binary(path, a)
+    mm, nn, read_rows = io.binary_row_reader(path)
+    assert (mm, nn) == (m, n)
+    calls = []
+
+    def reader(row0, rows, buf):
+        calls.append((row0, rows))
+        read_rows(row0, rows, buf)
+    o_h = torch.from_numpy(np.ascontiguousarray(omega)).pin_memory()
+    s1, u1, v1, it1 = isvd.solve_stream(reader, m, n, o_h, 8, 8, 4, integrator="rb_gramian_kn", former="rb_gramian")
+    assert calls[0][0] == 0 and sum(r for _, r in calls) == m
+    assert all(calls[i][0] + calls[i][1] == calls[i + 1][0] for i in range(len(calls) - 1))
+    a_h = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    s2, u2, v2, it2 = isvd.solve_host(a_h, o_h, 8, 8, 4, integrator="rb_gramian_kn", former="rb_gramian")
+    s3, u3, v3, it3 = isvd.solve(dev(a, cuda), 8, 8, 4, omega=dev(omega, cuda), integrator="rb_gramian_kn",
+                                 former="rb_gramian")
+    assert it1 == it2 == it3
+    assert torch.equal(s1, s2) and torch.equal(u1, u2) and torch.equal(v1, v2)
+    assert torch.equal(s1, s3.cpu()) and torch.equal(u1, u3.cpu())
+
+    def failing(row0, rows, buf):
+        if row0 > 0 or rows < m:
+            raise IOError("truncated file")
+        read_rows(row0, rows, buf)
+    if len(calls) > 1:
+        with pytest.raises(IOError):
+            isvd.solve_stream(failing, m, n, o_h, 8, 8, 4, integrator="rb_gramian_kn", former="rb_gramian")
+
+
 def test_stage_api_pipeline_with_device_omega(cuda):
     """Stages chained as the reference's driver does, Omega drawn on the device."""
     from mcnla_b200 import isvd, synthetic
