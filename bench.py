@@ -66,7 +66,8 @@ def parse():
                     help="reference arm: seconds of timed full solves; no step starts that would end past it")
     ap.add_argument("--quick", action="store_true", help="small shape for a smoke run")
     ap.add_argument("--no-serving", action="store_true", help="skip the batched / served leg")
-    ap.add_argument("--kernel", choices=["sketch_bf16", "gkn", "trace", "grouped", "served_trace", "gkn_scaling"],
+    ap.add_argument("--kernel", choices=["sketch_bf16", "gkn", "trace", "grouped", "served_trace", "gkn_scaling",
+                                         "ingest"],
                     default=None,
                     help="time one kernel alone (profiling case) instead of the benchmark: the BF16 sketch GEMM "
                          "on --m x --n x (--k + --p) --N with --parts parts, or the persistent row-block Gramian "
@@ -1082,6 +1083,54 @@ def run_gkn_scaling(args, dev):
     return {"kernel": "k_gkn_persistent", "rows": rows}
 
 
+def run_ingest(args, dev):
+    """Streamed ingest (mcnla_b200_isvd_stream) of an MCNLA binary file of the --m x --n workload
+    matrix, against reading the file alone and the host-buffer solve of the same A already in
+    pinned memory: wall seconds of each (best of 2; the file is read once before, so it comes
+    from the page cache)."""
+    import tempfile
+    import numpy as np
+    import torch
+    from mcnla_b200 import io, isvd, synthetic
+    m, n, k, p, N = args.m, args.n, args.k, args.p, args.N
+    L = (k + p) * N
+    a = workload_matrix(args, 0, device=dev).cpu().numpy()
+    omega = synthetic.omega_torch(n, L, seed=5, device=dev).cpu().pin_memory()
+    kw = dict(integrator=args.integrator, former=args.former, maxit=args.maxit, tol=args.tol)
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "a.bin")
+        io.save_binary(path, a)
+        _, _, read_rows = io.binary_row_reader(path)
+        buf = torch.empty(min(m, 8192), n, dtype=torch.float64, pin_memory=True)
+
+        def read_all():
+            for r0 in range(0, m, buf.shape[0]):
+                read_rows(r0, min(buf.shape[0], m - r0), buf.data_ptr())
+
+        def best(fn):
+            t = 1e9
+            for _ in range(2):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                fn()
+                torch.cuda.synchronize()
+                t = min(t, time.perf_counter() - t0)
+            return t
+        read_all()
+        t_read = best(read_all)
+        t_stream = best(lambda: isvd.solve_stream(read_rows, m, n, omega, k, p, N, device=dev, **kw))
+        a_h = torch.from_numpy(a).pin_memory()
+        del a
+        t_host = best(lambda: isvd.solve_host(a_h, omega, k, p, N, device=dev, **kw))
+    gb = m * n * 8 / 1e9
+    return {"case": "streamed ingest of a %d x %d FP64 binary file (%.2f GB), k=%d p=%d N=%d, %s / %s"
+                    % (m, n, gb, k, p, N, args.integrator, args.former),
+            "read_file_s": round(t_read, 4), "stream_solve_s": round(t_stream, 4),
+            "host_buffer_solve_s": round(t_host, 4),
+            "overlapped_s": round(max(0.0, t_read + t_host - t_stream), 4),
+            "file_gbs": round(gb / t_read, 2)}
+
+
 def run_kernel_case(args, dev):
     import numpy as np
     import torch
@@ -1095,6 +1144,8 @@ def run_kernel_case(args, dev):
         return run_served_trace(args, dev)
     if args.kernel == "gkn_scaling":
         return run_gkn_scaling(args, dev)
+    if args.kernel == "ingest":
+        return run_ingest(args, dev)
     if args.kernel == "grouped":
         # the grouped batch integrator on --batch-count copies of one shape (m x n, k, p = k/2, N = 8)
         shapes = [dict(sh, k=k, p=k // 2) for sh in synthetic.batch_shapes(args.batch_count, seed=4)]
