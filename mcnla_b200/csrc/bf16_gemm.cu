@@ -173,6 +173,27 @@ __device__ __forceinline__ void tmem_ld32_nowait(uint32_t taddr, uint32_t (&r)[3
       : "r"(taddr));
 }
 
+// Epilogue staging: a warp's 32 x 32 block of the output in shared memory, row
+// r at stg[r * 33 ..] (the odd pitch keeps a lane's row writes and the
+// row-wise reads on distinct banks), stored row by row: lane c writes column
+// col0 + c of rows row0 .. row0 + 31, so each store instruction covers 32
+// consecutive elements of one row.
+constexpr int kStageBlock = 32 * 33;   // doubles per epilogue warp
+static_assert(8 * kStageBlock * 8 <= 3 * (3 * 128 * 64 * 2 + 128 * 64 * 2), "epilogue staging fits in the ring");
+
+template <class OutT>
+__device__ __forceinline__ void store_block(const double* stg, OutT* D, const Args& g, int row0, int col0, int lane) {
+  const int col = col0 + lane;
+  if (col >= g.N) return;
+  for (int i = 0; i < 32; ++i) {
+    const int row = row0 + i;
+    if (row >= g.M) break;
+    OutT* d = D + int64_t(row) * g.ldd + col;
+    const double v = stg[i * 33 + lane];
+    *d = OutT(g.accumulate ? double(*d) + v : v);
+  }
+}
+
 template <class OutT, bool CHUNKED>
 __global__ void __launch_bounds__(TileCfg<CHUNKED>::THREADS, 1)
     bf16_gemm_kernel(const __grid_constant__ CUtensorMap tm_a_hi, const __grid_constant__ CUtensorMap tm_a_lo,
@@ -309,16 +330,18 @@ __global__ void __launch_bounds__(TileCfg<CHUNKED>::THREADS, 1)
     }
     if (!ok) {
       if (lane == 0) atomicExch(g.status, MCNLA_B200_ERR_DEVICE_TIMEOUT);
-    } else if (row < g.M) {
-      OutT* drow = dsplit + int64_t(row) * g.ldd;
+    } else {
+      // every MMA has completed, so the ring is idle: each warp stages its 32 x 32 blocks there
+      // and stores them a row at a time (32 consecutive columns per store instruction)
+      double* stg = reinterpret_cast<double*>(smem) + (warp - 2) * kStageBlock;
       const int col = n0 + h * (BN / 2);
-      if (col + BN / 2 <= g.N) {
 #pragma unroll
-        for (int j = 0; j < BN / 2; ++j) drow[col + j] = OutT(g.accumulate ? double(drow[col + j]) + acc[j] : acc[j]);
-      } else {
+      for (int hh = 0; hh < BN / 64; ++hh) {
 #pragma unroll
-        for (int j = 0; j < BN / 2; ++j)
-          if (col + j < g.N) drow[col + j] = OutT(g.accumulate ? double(drow[col + j]) + acc[j] : acc[j]);
+        for (int j = 0; j < 32; ++j) stg[lane * 33 + j] = acc[hh * 32 + j];
+        __syncwarp();
+        store_block<OutT>(stg, dsplit, g, m0 + q * 32, col + hh * 32, lane);
+        __syncwarp();
       }
     }
   } else if (!CHUNKED && warp >= 4) {
@@ -330,27 +353,18 @@ __global__ void __launch_bounds__(TileCfg<CHUNKED>::THREADS, 1)
     if (!ok) {
       if (lane == 0) atomicExch(g.status, MCNLA_B200_ERR_DEVICE_TIMEOUT);
     } else {
-      const int row = m0 + q * 32 + lane;
-      OutT* drow = dsplit + int64_t(row) * g.ldd;
+      // every MMA has completed, so the ring is idle: each warp stages its 32 x 32 blocks there
+      // and stores them a row at a time (32 consecutive columns per store instruction)
+      double* stg = reinterpret_cast<double*>(smem) + (warp - 4) * kStageBlock;
 #pragma unroll 1
       for (int c = 0; c < BN / 32; ++c) {
         uint32_t r[32];
         tmem_ld32(tmem + (uint32_t(q * 32) << 16) + uint32_t(c * 32), r);
-        const int col = n0 + c * 32;
-        if (row < g.M) {
-          if (col + 32 <= g.N) {
 #pragma unroll
-            for (int j = 0; j < 32; ++j) {
-              const double v = __uint_as_float(r[j]);
-              drow[col + j] = OutT(g.accumulate ? double(drow[col + j]) + v : v);
-            }
-          } else {
-            for (int j = 0; j < 32 && col + j < g.N; ++j) {
-              const double v = __uint_as_float(r[j]);
-              drow[col + j] = OutT(g.accumulate ? double(drow[col + j]) + v : v);
-            }
-          }
-        }
+        for (int j = 0; j < 32; ++j) stg[lane * 33 + j] = double(__uint_as_float(r[j]));
+        __syncwarp();
+        store_block<OutT>(stg, dsplit, g, m0 + q * 32, n0 + c * 32, lane);
+        __syncwarp();
       }
     }
   }
