@@ -62,7 +62,7 @@ def parse():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-row-block", action="store_true", help="N > 1: skip the row-block (one matrix over all ranks) leg")
     ap.add_argument("--cpu-rows", type=int, default=0, help="row sample of the CPU baseline (0: auto)")
-    ap.add_argument("--ref-budget", type=float, default=1200.0,
+    ap.add_argument("--ref-budget", type=float, default=420.0,
                     help="reference arm: seconds of timed full solves; no step starts that would end past it")
     ap.add_argument("--quick", action="store_true", help="small shape for a smoke run")
     ap.add_argument("--no-serving", action="store_true", help="skip the batched / served leg")
