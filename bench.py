@@ -679,7 +679,10 @@ def run_b200(args, world, rank, local):
     if world > 1 and not args.no_row_block:
         del a
         torch.cuda.empty_cache()
-        row_block = run_row_block_b200(args, world, rank, local)
+        try:
+            row_block = run_row_block_b200(args, world, rank, local)
+        except Exception as e:              # reported on the line; the replicas' value stands
+            row_block = {"error": "%s: %s" % (type(e).__name__, e)}
     result = {
         "metric": METRIC, "value": round(value, 5), "unit": "iSVD/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(total / args.steps * 1e3, 3), "higher_is_better": True,
