@@ -326,11 +326,13 @@ Plan make_plan(const Context* ctx, int64_t M, int64_t N, int64_t K, int batch, i
   return p;
 }
 
-// The large-output plan for K-contiguous A and N-contiguous B (the sketch A Omega):
-// 64 x 128 tiles of four 32 x 64 warps, two CTAs per SM, so one CTA's barrier
-// bubbles are filled by the other's MMAs (33.4 vs 30.9 TFLOP/s on 16384 x 4096 x 20000).
-Plan prefer_two_cta(Plan p, bool AK, bool BKM, int64_t M, int64_t N) {
-  if (AK && !BKM && (p.shape == S128x128k32 || p.shape == S128x128w16) && M > 64 && N > 64) {
+// The large-output plan for N-contiguous B with K-contiguous A (the sketch A Omega) or
+// for a lower-triangle product (the Gramian Qs' Qs, A read M-major): 64 x 128 tiles of
+// four 32 x 64 warps, two CTAs per SM, so one CTA's barrier bubbles are filled by the
+// other's MMAs (sketch 33.4 vs 30.9 TFLOP/s on 16384 x 4096 x 20000; Gramian 4096 x 4096
+// x 100000 lower triangle 60.3 -> 58.0 ms).
+Plan prefer_two_cta(Plan p, bool AK, bool BKM, int64_t M, int64_t N, bool lower_only) {
+  if ((AK || lower_only) && !BKM && (p.shape == S128x128k32 || p.shape == S128x128w16) && M > 64 && N > 64) {
     p.shape = S64x128;
     p.bm = 64;
     p.bn = 128;
@@ -479,7 +481,7 @@ int dgemm(Context* ctx, int64_t M, int64_t N, int64_t K, double alpha, CMat A, C
   auto al16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
   const bool vec2 = al16(A.p) && al16(B.p) && (lda % 2 == 0 || (AK ? M == 1 : K == 1)) &&
                     (ldb % 2 == 0 || (BKM ? N == 1 : K == 1)) && batch.a % 2 == 0 && batch.b % 2 == 0;
-  Plan p = prefer_two_cta(make_plan(ctx, M, N, K, batch.count, force_splits), AK, BKM, M, N);
+  Plan p = prefer_two_cta(make_plan(ctx, M, N, K, batch.count, force_splits), AK, BKM, M, N, lower_only);
   KArgs g;
   g.M = M; g.N = N; g.K = K; g.alpha = alpha; g.beta = beta;
   g.A = A.p; g.a_rs = A.rs; g.a_cs = A.cs; g.a_bs = batch.a;
@@ -528,7 +530,7 @@ int dgemm_rows_in_place(Context* ctx, int64_t M, int64_t N, int64_t K, CMat A, C
   auto al16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
   const bool vec2 = al16(A.p) && al16(B.p) && (lda % 2 == 0 || (AK ? M == 1 : K == 1)) &&
                     (ldb % 2 == 0 || (BKM ? N == 1 : K == 1)) && batch.a % 2 == 0 && batch.b % 2 == 0;
-  const Plan p = prefer_two_cta(make_plan(ctx, M, N, K, batch.count, 1), AK, BKM, M, N);
+  const Plan p = prefer_two_cta(make_plan(ctx, M, N, K, batch.count, 1), AK, BKM, M, N, false);
   // one CTA per row panel: it reads all of its rows' K before its epilogue writes them
   if (p.bn < N || p.splits != 1) return MCNLA_B200_ERR_UNSUPPORTED;
   KArgs g;
