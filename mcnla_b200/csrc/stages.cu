@@ -1076,20 +1076,25 @@ int run_isvd(Context* c, const Dims& d, int integrator, int former, const double
 // sketch.  Each block's GEMM uses the split-K count of the whole product, so
 // every element of Q equals the whole-product GEMM's.
 // Row blocks of a sketch streamed from host memory: at least 128 rows, about
-// 1 GB at most, at least four blocks; each block's GEMM uses the split-K count
-// of the whole product, so the result is the device-resident sketch's bit for
-// bit.
+// 1 GB at most, at least four blocks, and a first block of about 128 MB so the
+// first GEMM starts early; each block's GEMM uses the split-K count of the
+// whole product, so every row of the result is the device-resident sketch's
+// bit for bit whatever the block boundaries.
 struct RowBlocks {
-  int64_t rows_per;
+  int64_t rows_per;   // rows of every block after the first (the largest block)
+  int64_t first;      // rows of the first block
   int nblocks;
   int splits;
+  int64_t start(int b) const { return b == 0 ? 0 : first + int64_t(b - 1) * rows_per; }
+  int64_t rows(int b, int64_t m) const { return std::min<int64_t>(b == 0 ? first : rows_per, m - start(b)); }
 };
 
 RowBlocks stream_blocks(Context* c, const Dims& d) {
   const size_t row_bytes = size_t(d.n) * sizeof(double);
   RowBlocks rb;
   rb.rows_per = std::max<int64_t>(128, std::min<int64_t>(int64_t((size_t(1) << 30) / row_bytes), cdiv(d.m, 4)));
-  rb.nblocks = int(cdiv(d.m, rb.rows_per));
+  rb.first = std::min<int64_t>(rb.rows_per, std::max<int64_t>(128, int64_t((size_t(128) << 20) / row_bytes)));
+  rb.nblocks = 1 + int(cdiv(std::max<int64_t>(0, d.m - rb.first), rb.rows_per));
   rb.splits = dgemm_heuristic_splits(c, d.m, d.L, d.n, 1);
   return rb;
 }
@@ -1129,7 +1134,7 @@ int stream_setup(Context* c, const Dims& d, const RowBlocks& rb, const double* o
 
 int sketch_block(Context* c, const Dims& d, const RowBlocks& rb, const StreamSetup& st, int b, const double* A,
                  const double* omega, double* Q) {
-  const int64_t r0 = b * rb.rows_per, rows = std::min<int64_t>(rb.rows_per, d.m - r0);
+  const int64_t r0 = rb.start(b), rows = rb.rows(b, d.m);
   MB_CHECK_CUDA(cudaStreamWaitEvent(c->stream, st.ev[b], 0));
   return dgemm(c, rows, d.L, d.n, 1.0, crow(A + r0 * d.n, d.n), crow(omega, d.L), 0.0, drow(Q + r0 * d.L, d.L),
                GemmBatch(), st.ws, rb.splits);
@@ -1141,7 +1146,7 @@ int run_sketch_streamed(Context* c, const Dims& d, const double* A_host, double*
   StreamSetup st;
   MB_CHECK(stream_setup(c, d, rb, omega_host, omega, st));
   for (int b = 0; b < rb.nblocks; ++b) {
-    const int64_t r0 = b * rb.rows_per, rows = std::min<int64_t>(rb.rows_per, d.m - r0);
+    const int64_t r0 = rb.start(b), rows = rb.rows(b, d.m);
     MB_CHECK_CUDA(cudaMemcpyAsync(A + r0 * d.n, A_host + r0 * d.n, size_t(rows) * d.n * sizeof(double),
                                   cudaMemcpyHostToDevice, c->copy_stream));
     MB_CHECK_CUDA(cudaEventRecord(st.ev[b], c->copy_stream));
@@ -1171,7 +1176,7 @@ int run_sketch_ingest(Context* c, const Dims& d, mcnla_b200_read_rows_fn read_ro
   StreamSetup st;
   MB_CHECK(stream_setup(c, d, rb, omega_host, omega, st));
   for (int b = 0; b < rb.nblocks; ++b) {
-    const int64_t r0 = b * rb.rows_per, rows = std::min<int64_t>(rb.rows_per, d.m - r0);
+    const int64_t r0 = rb.start(b), rows = rb.rows(b, d.m);
     double* buf = static_cast<double*>(c->stage_host[b & 1]);
     if (b >= 2) MB_CHECK_CUDA(cudaEventSynchronize(st.ev[b - 2]));   // the buffer's last copy has landed
     if (read_rows(user, r0, rows, buf) != 0) {
