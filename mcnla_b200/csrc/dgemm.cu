@@ -326,13 +326,15 @@ Plan make_plan(const Context* ctx, int64_t M, int64_t N, int64_t K, int batch, i
   return p;
 }
 
-// The large-output plan for N-contiguous B with K-contiguous A (the sketch A Omega) or
-// for a lower-triangle product (the Gramian Qs' Qs, A read M-major): 64 x 128 tiles of
-// four 32 x 64 warps, two CTAs per SM, so one CTA's barrier bubbles are filled by the
-// other's MMAs (sketch 33.4 vs 30.9 TFLOP/s on 16384 x 4096 x 20000; Gramian 4096 x 4096
-// x 100000 lower triangle 60.3 -> 58.0 ms).
+// The large-output plan for N-contiguous B (the sketch A Omega with A row- or
+// column-major, the Gramian Qs' Qs): 64 x 128 tiles of four 32 x 64 warps, two CTAs per
+// SM, so one CTA's barrier bubbles are filled by the other's MMAs (sketch 33.4 vs 30.9
+// TFLOP/s on 16384 x 4096 x 20000; Gramian 4096 x 4096 x 100000 lower triangle 60.3 ->
+// 58.0 ms).
 Plan prefer_two_cta(Plan p, bool AK, bool BKM, int64_t M, int64_t N, bool lower_only) {
-  if ((AK || lower_only) && !BKM && (p.shape == S128x128k32 || p.shape == S128x128w16) && M > 64 && N > 64) {
+  (void)AK;
+  (void)lower_only;
+  if (!BKM && (p.shape == S128x128k32 || p.shape == S128x128w16) && M > 64 && N > 64) {
     p.shape = S64x128;
     p.bm = 64;
     p.bn = 128;
