@@ -114,3 +114,21 @@ def test_error_statuses(tmp_path):
     notbin = tmp_path / "x.bin"
     notbin.write_bytes(b"\0" * 200)
     assert lib.mcnla_b200_binary_size(str(notbin).encode(), dims, ctypes.byref(nd), None) == _lib.ERR_IO
+
+
+def test_binary_row_reader_fills_row_blocks(tmp_path):
+    """The streamed ingest's reader (the reference's loadBinaryRowBlock): rows [row0, row0 + rows)
+    of a row-major binary matrix land in a caller's buffer given by address, in any block split."""
+    a = np.random.default_rng(3).standard_normal((37, 11))
+    p = tmp_path / "a.bin"
+    io.save_binary(p, a)
+    m, n, read_rows = io.binary_row_reader(p)
+    assert (m, n) == (37, 11)
+    out = np.empty_like(a)
+    for r0, rows in ((0, 5), (5, 16), (21, 16)):
+        buf = np.zeros((rows, n))
+        read_rows(r0, rows, buf.ctypes.data)
+        out[r0:r0 + rows] = buf
+    np.testing.assert_array_equal(out, a)
+    with pytest.raises(Exception):
+        read_rows(30, 10, np.zeros((10, n)).ctypes.data)          # past the last row
