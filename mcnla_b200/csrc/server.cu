@@ -102,6 +102,7 @@ void mcnla_b200_server::worker(int me) {
   if (ok) ctx->coop_cta_limit = std::max(1, ctx->num_sms / nworkers);
   if (!ok) init_failures++;
   mb::SolveScratch scratch;
+  int64_t held_floor = 0;   // what this worker still held after its last release (it cannot go lower)
   while (true) {
     int64_t ticket = 0;
     mcnla_b200_problem p;
@@ -119,11 +120,12 @@ void mcnla_b200_server::worker(int me) {
       };
       cv_work.wait(lock, [&] {
         if (queue.empty()) return stop;
-        return fits() || alone() || committed[me] > mb::kKeepBytes;
+        return fits() || alone() || committed[me] > std::max(mb::kKeepBytes, held_floor);
       });
       if (queue.empty()) break;
       if (!fits() && !alone()) {
         // this worker's idle workspaces stand in the head's way: release them and wait again
+        // (woken by the next completion, or to release again only if it grew past the floor)
         lock.unlock();
         if (ok) {
           mb::solve_scratch_free(ctx, scratch);
@@ -131,6 +133,7 @@ void mcnla_b200_server::worker(int me) {
           cudaStreamSynchronize(stream);
         }
         const int64_t held = ok ? mb::ctx_held_bytes(ctx) : 0;
+        held_floor = held;
         lock.lock();
         committed_total += held - committed[me];
         committed[me] = held;
