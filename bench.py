@@ -67,7 +67,7 @@ def parse():
     ap.add_argument("--quick", action="store_true", help="small shape for a smoke run")
     ap.add_argument("--no-serving", action="store_true", help="skip the batched / served leg")
     ap.add_argument("--kernel", choices=["sketch_bf16", "gkn", "trace", "grouped", "served_trace", "gkn_scaling",
-                                         "ingest"],
+                                         "ingest", "syev"],
                     default=None,
                     help="time one kernel alone (profiling case) instead of the benchmark: the BF16 sketch GEMM "
                          "on --m x --n x (--k + --p) --N with --parts parts, or the persistent row-block Gramian "
@@ -1143,6 +1143,52 @@ def run_ingest(args, dev):
             "file_gbs": round(gb / t_read, 2)}
 
 
+def run_syev(args, dev):
+    """The batched Jacobi eigensolver (mcnla_b200_syev_batched, descending |lambda|, as the
+    orthogonalizer and the formers call it) on sketch Gram matrices Y'Y, Y = A Omega with
+    sigma_j = 1/j: l = 12 .. 160, 8 matrices (16 for l >= 128).  CUDA events, best of 3; the
+    residual max |W v - lambda v| / lambda_1 and max |V'V - I|."""
+    import numpy as np
+    import torch
+    from mcnla_b200 import isvd, _lib
+    ctx = isvd.context(dev)
+    rows = []
+    for l in (12, 24, 48, 64, 96, 128, 160):
+        batch = 16 if l >= 128 else 8
+        rng = np.random.default_rng(l)
+        m, n = 4 * l + 64, 6 * l + 64
+        u, _ = np.linalg.qr(rng.standard_normal((m, min(m, n))))
+        v, _ = np.linalg.qr(rng.standard_normal((n, min(m, n))))
+        a = (u / np.arange(1, min(m, n) + 1)) @ v.T
+        grams = []
+        for _ in range(batch):
+            y = a @ rng.standard_normal((n, l))
+            grams.append(y.T @ y)
+        g = torch.as_tensor(np.stack(grams), device=dev)
+        w = torch.empty(batch, l, dtype=torch.float64, device=dev)
+        vv = torch.empty(batch, l, l, dtype=torch.float64, device=dev)
+
+        def call():
+            _lib.check(ctx.lib.mcnla_b200_syev_batched(ctx.bind(), l, batch, isvd._ptr(g), isvd._ptr(w), isvd._ptr(vv),
+                                                       1), "syev_batched")
+        call()
+        stream = torch.cuda.current_stream(dev)
+        best = 1e9
+        for _ in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            call()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        gn, wn, vn = g.cpu().numpy(), w.cpu().numpy(), vv.cpu().numpy()
+        resid = max(float(np.abs(gn[b] @ vn[b] - vn[b] * wn[b]).max() / wn[b].max()) for b in range(batch))
+        orth = max(float(np.abs(vn[b].T @ vn[b] - np.eye(l)).max()) for b in range(batch))
+        rows.append({"l": l, "batch": batch, "ms": round(best, 3), "residual": resid, "orthogonality": orth})
+    return {"kernel": "k_syev (batched Jacobi, 1024 threads per matrix)", "rows": rows}
+
+
 def run_kernel_case(args, dev):
     import numpy as np
     import torch
@@ -1158,6 +1204,8 @@ def run_kernel_case(args, dev):
         return run_gkn_scaling(args, dev)
     if args.kernel == "ingest":
         return run_ingest(args, dev)
+    if args.kernel == "syev":
+        return run_syev(args, dev)
     if args.kernel == "grouped":
         # the grouped batch integrator on --batch-count copies of one shape (m x n, k, p = k/2, N = 8)
         shapes = [dict(sh, k=k, p=k // 2) for sh in synthetic.batch_shapes(args.batch_count, seed=4)]
