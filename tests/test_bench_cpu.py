@@ -47,3 +47,32 @@ def test_default_arguments_follow_the_contract(monkeypatch):
     assert (a.m, a.n, a.k, a.p, a.N) == (100000, 20000, 50, 14, 64)
     w = bench.workload(a)
     assert "m=100000" in w["workload"] and w["sketch_gemm"] == "100000x20000x4096"
+
+
+def test_svd_metrics_against_a_known_rotation():
+    """The accuracy report of the precision-form legs: sigma relative error, largest principal
+    angle of U, ||U'U - I||_F, on a case with known answers."""
+    import numpy as np
+    rng = np.random.default_rng(0)
+    q, _ = np.linalg.qr(rng.standard_normal((50, 4)))
+    s_ref = np.array([4.0, 3.0, 2.0, 1.0])
+    theta = 1e-3
+    rot = np.eye(4)
+    rot[0, 0] = rot[1, 1] = np.cos(theta)
+    rot[0, 1], rot[1, 0] = -np.sin(theta), np.sin(theta)
+    # the same subspace (a rotation within it) with the last column tilted out of it by theta
+    u = q @ rot
+    out, _ = np.linalg.qr(np.concatenate([q, rng.standard_normal((50, 1))], axis=1))
+    u[:, 3] = np.cos(theta) * q[:, 3] + np.sin(theta) * out[:, 4]
+    m = bench._svd_metrics(s_ref * (1 + 1e-7), u, s_ref, q)
+    assert abs(m["sigma_rel_err"] - 1e-7) < 1e-12
+    assert abs(m["max_principal_angle_U"] - theta) < 1e-9
+    assert m["UtU_minus_I_fro"] < 1e-12
+
+
+def test_reference_arm_default_budget_is_minutes(monkeypatch):
+    """The reference arm times whole solves of the full matrix until its budget (seconds) would be
+    exceeded: a few minutes by default."""
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--impl", "reference"])
+    a = bench.parse()
+    assert 60 <= a.ref_budget <= 600
