@@ -431,7 +431,7 @@ int gramian_form_qbar(Context* c, const Dims& d, const double* Qs, const double*
 // shapes, so a problem gives the same bits either way.
 size_t gkn_ws_bytes(const Context* c, const Dims& d) {
   const int64_t L = d.L, l = d.l, m = d.m;
-  return gemm_ws(c, {{L, L, m, 1}, {L, l, L, 1}, {l, 2 * l, L, 1}, {L, l, 2 * l, 1}, {m, l, L, 1}});
+  return gemm_ws(c, {{L, L, m, 1}, {L, l, L, 1}, {l, 2 * l, L, 1}, {L, l, 2 * l, 2}, {m, l, L, 1}});
 }
 
 // Visits the buffers in carve order: fn(count, element bytes).
@@ -565,9 +565,11 @@ int gkn_iteration(Context* c, const Dims& d, const GknBufs& b, int i, bool allow
   MB_CHECK(launch_kn_step(c, l, nullptr, b.DD, inv_n, b.FC, b.FCN, b.FF[cur], b.FF[1 - cur], b.vwork, tol,
                           allow_series));
   // E~+ := E~c Fc + 1/N Bc inv(C) = [E~c Bc] [Fc; inv(C)/N]   (:194, :200)
-  MB_CHECK(dgemm(c, L, l, l2, 1.0, crow(Ec, l3), crow(b.FCN, l), 0.0, drow(b.EB[1 - cur], l3), GemmBatch(), ws));
   // B+ := [Bc Bgc] [Fc; inv(C)]   (:203-204)
-  MB_CHECK(dgemm(c, L, l, l2, 1.0, crow(Bc, l3), crow(b.FC, l), 0.0, drow(b.EB[1 - cur] + l, l3), GemmBatch(), ws));
+  // one batched launch: member 0 reads columns [0, 2l) of the state and [Fc; inv(C)/N], member 1
+  // columns [l, 3l) and [Fc; inv(C)], writing E~+ and B+ side by side
+  MB_CHECK(dgemm(c, L, l, l2, 1.0, crow(Ec, l3), crow(b.FCN, l), 0.0, drow(b.EB[1 - cur], l3),
+                 GemmBatch{2, l, int64_t(b.FC - b.FCN), l}, ws));
   return MCNLA_B200_OK;
 }
 

@@ -200,7 +200,7 @@ def test_kn_step_methods_agree(cuda, golden, cls_name):
 def test_gramian_kn_runs_persistent(cuda, golden):
     """With the default step method the row-block Gramian KN integrator runs
     whole iterations in one cooperative kernel: far fewer launches than the
-    five or more per iteration of the launch-per-product loop."""
+    four or more per iteration of the launch-per-product loop."""
     from mcnla_b200 import isvd, _lib
     m, l, N = golden["m"], golden["l"], golden["N"]
     prm = params(m, l, l, 0, N)
@@ -216,7 +216,7 @@ def test_gramian_kn_runs_persistent(cuda, golden):
         counts.append(ctx.kernels_launched() - k0)
         assert integ.iteration() == 81
     ctx.set_kn_method(_lib.KN_AUTO)
-    assert counts[0] < 40 and counts[1] > 5 * 81, counts
+    assert counts[0] < 40 and counts[1] > 4 * 81, counts
 
 
 @pytest.mark.parametrize("l", [5, 48, 96, 160])
