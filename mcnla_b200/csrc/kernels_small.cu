@@ -13,7 +13,8 @@ namespace {
 constexpr int kSmallThreads = 512;
 constexpr int kSyevThreads = 1024;   // the Jacobi rounds are latency-bound: more warps hide more of it
 constexpr int kMaxSweeps = 40;
-constexpr int kKnNsMaxDim = 80;   // the matrix-function KN step keeps four padded l x l matrices on chip
+constexpr int kKnNsMaxDim = 80;
+static_assert(2 * MCNLA_B200_MAX_DIM_SKETCH_WENYIN <= kSmallThreads, "cta_gj_inverse needs n <= blockDim.x");   // the matrix-function KN step keeps four padded l x l matrices on chip
 
 // Shared-memory carve-up shared by the one-CTA solvers.
 struct SmemCarve {
@@ -46,6 +47,21 @@ __device__ small::JacobiScratch carve_jacobi(SmemCarve& sc, int n) {
   js.count = sc.take<int>(1);
   js.red = sc.take<double>(32);
   return js;
+}
+
+__host__ __device__ inline size_t gj_scratch_bytes(int n) {   // piv, col, prow, cand_v, cand_i
+  return (size_t(n) * 4 + 16) + (size_t(n) * 16 + 16) + (size_t(n) * 8 + 16) + (small::kGjMaxGroups * 8 + 16) +
+         (small::kGjMaxGroups * 4 + 16);
+}
+
+__device__ small::GjScratch carve_gj(SmemCarve& sc, int n) {
+  small::GjScratch g;
+  g.piv = sc.take<int>(n);
+  g.col = sc.take<double>(2 * size_t(n));
+  g.prow = sc.take<double>(n);
+  g.cand_v = sc.take<double>(small::kGjMaxGroups);
+  g.cand_i = sc.take<int>(small::kGjMaxGroups);
+  return g;
 }
 
 // rank[j] = position of eigenvalue j in the requested order (ties by index).
@@ -485,11 +501,7 @@ __global__ void __launch_bounds__(kSmallThreads) k_wy_trial(int l, const double*
   SmemCarve sc(smem_raw);
   const int n = 2 * l, ld = n + 1, ldd = 2 * l;
   double* cm = sc.take<double>(size_t(n) * ld);
-  int* piv = sc.take<int>(n);
-  double* col = sc.take<double>(n);
-  double* rv = sc.take<double>(4);
-  int* ri = sc.take<int>(4);
-  int* flag = sc.take<int>(4);
+  const small::GjScratch gs = carve_gj(sc, n);
   const int tid = threadIdx.x, nt = blockDim.x;
   const double it = 1.0 / tau;
   // C := [ Dc/2 - I/tau , I/2 ; -Dgc/2 , -Dc/2 - I/tau ]
@@ -505,7 +517,7 @@ __global__ void __launch_bounds__(kSmallThreads) k_wy_trial(int l, const double*
     cm[i * ld + j] = x;
   }
   __syncthreads();
-  const int sing = small::cta_gj_inverse(cm, ld, n, piv, col, rv, ri, flag);
+  const int sing = small::cta_gj_inverse(cm, ld, n, gs);
   if (sing) {
     if (tid == 0) scal->status = MCNLA_B200_ERR_SINGULAR;
     return;
@@ -671,15 +683,11 @@ __global__ void __launch_bounds__(kSmallThreads) k_inverse(int n, double* A, Dev
   SmemCarve sc(smem_raw);
   const int ld = n + 1;
   double* a = sc.take<double>(size_t(n) * ld);
-  int* piv = sc.take<int>(n);
-  double* col = sc.take<double>(n);
-  double* rv = sc.take<double>(4);
-  int* ri = sc.take<int>(4);
-  int* flag = sc.take<int>(4);
+  const small::GjScratch gs = carve_gj(sc, n);
   double* Ab = A + size_t(blockIdx.x) * n * n;
   for (int e = threadIdx.x; e < n * n; e += blockDim.x) a[(e / n) * ld + (e % n)] = Ab[e];
   __syncthreads();
-  const int sing = small::cta_gj_inverse(a, ld, n, piv, col, rv, ri, flag);
+  const int sing = small::cta_gj_inverse(a, ld, n, gs);
   if (sing) {
     if (threadIdx.x == 0) scal->status = MCNLA_B200_ERR_SINGULAR;
     return;
@@ -948,7 +956,7 @@ int launch_kn_step(Context* c, int l, const double* z, const double* dd, double 
 int launch_wy_trial(Context* c, int l, const double* dd, double tau, double inv_n, double* F, double* FN) {
   if (l < 1 || l > MCNLA_B200_MAX_DIM_SKETCH_WENYIN) return MCNLA_B200_ERR_UNSUPPORTED;
   const int n = 2 * l;
-  const size_t smem = size_t(n) * (n + 1) * 8 + 16 + n * 4 + 16 + n * 8 + 16 + 3 * 64 + 64;
+  const size_t smem = size_t(n) * (n + 1) * 8 + 16 + gj_scratch_bytes(n) + 64;
   if (smem > c->smem_optin) return MCNLA_B200_ERR_UNSUPPORTED;
   MB_CHECK(set_smem(c, reinterpret_cast<const void*>(k_wy_trial), smem));
   k_wy_trial<<<1, kSmallThreads, smem, c->stream>>>(l, dd, tau, inv_n, F, FN, c->scal);
@@ -1082,7 +1090,7 @@ int launch_gwy_small_dots(Context* c, int l, const double* phi1, const double* p
 
 int launch_inverse(Context* c, int n, int batch, double* A) {
   if (n < 1 || n > 2 * MCNLA_B200_MAX_DIM_SKETCH_WENYIN || batch < 1) return MCNLA_B200_ERR_UNSUPPORTED;
-  const size_t smem = size_t(n) * (n + 1) * 8 + 16 + n * 4 + 16 + n * 8 + 16 + 3 * 64 + 64;
+  const size_t smem = size_t(n) * (n + 1) * 8 + 16 + gj_scratch_bytes(n) + 64;
   if (smem > c->smem_optin) return MCNLA_B200_ERR_UNSUPPORTED;
   MB_CHECK(set_smem(c, reinterpret_cast<const void*>(k_inverse), smem));
   k_inverse<<<batch, kSmallThreads, smem, c->stream>>>(n, A, c->scal);

@@ -207,75 +207,105 @@ __device__ inline int cta_jacobi_eig(double* a, int lda, double* v, int ldv, int
   return sweep;
 }
 
-// In-place inverse of the n x n matrix a (row stride lda) by Gauss-Jordan
-// elimination with partial pivoting.  piv (n ints) and col (n doubles) are
-// scratch.  Returns 0, or k+1 when the k-th pivot is exactly zero (the matrix
-// is singular; a is then left partially reduced, as LAPACK's getri would
-// refuse).  All threads return the same value.
-__device__ inline int cta_gj_inverse(double* a, int lda, int n, int* piv, double* col, double* red_v, int* red_i,
-                                     int* flag) {
+// Scratch of cta_gj_inverse (shared memory).
+constexpr int kGjMaxGroups = 32;
+struct GjScratch {
+  int* piv;        // n: the pivot position of each step
+  double* col;     // 2 n: the pivot column, double-buffered across steps
+  double* prow;    // n: the scaled pivot row
+  double* cand_v;  // kGjMaxGroups: pivot candidates, one per row group
+  int* cand_i;     // kGjMaxGroups
+};
+
+// In-place inverse of the n x n matrix a (row stride lda, n <= blockDim.x) by
+// Gauss-Jordan elimination with partial pivoting: the same operations, pivots
+// and rounding as the row-interchange form (pivot = first position of the
+// largest |a(i, k)|, i >= k, as idamax; rows swapped, the pivot row scaled,
+// every other row eliminated; the interchanges undone as column swaps at the
+// end).  Each thread owns one column and every R-th row of it (R row groups,
+// R = min(blockDim.x / n, kGjMaxGroups)), so a step takes two block barriers
+// and no index division: (1) every thread picks the pivot from the candidates
+// of the row groups, and one thread per column moves the old row k to the
+// pivot's position and scales the pivot row into prow; (2) the elimination,
+// in which the owners of column k+1 keep the new column and leave the next
+// candidates.  Returns 0, or k+1 when the k-th pivot is exactly zero (the
+// matrix is singular; a is then left partially reduced, as LAPACK's getri
+// would refuse).  All threads return the same value.
+__device__ inline int cta_gj_inverse(double* a, int lda, int n, const GjScratch& s) {
   const int tid = threadIdx.x, nt = blockDim.x;
-  if (tid == 0) *flag = 0;
+  const int R = min(nt / n, kGjMaxGroups);
+  const bool own = tid < R * n;
+  const int j = own ? tid % n : 0, r0 = own ? tid / n : 0;
+  if (own && j == 0) {
+    double best = -1.0;
+    int bi = 0;
+    for (int i = r0; i < n; i += R) {
+      const double v = a[i * lda];
+      s.col[i] = v;
+      if (fabs(v) > best) { best = fabs(v); bi = i; }
+    }
+    s.cand_v[r0] = best;
+    s.cand_i[r0] = bi;
+  }
   __syncthreads();
   for (int k = 0; k < n; ++k) {
-    // pivot: argmax_{i >= k} |a[i][k]| (first maximum wins, as idamax)
-    if (tid < 32) {
-      double best = -1.0;
-      int bi = k;
-      for (int i = k + tid; i < n; i += 32) {
-        const double v = fabs(a[i * lda + k]);
-        if (v > best) { best = v; bi = i; }
-      }
-      for (int o = 16; o > 0; o >>= 1) {
-        const double ov = __shfl_xor_sync(0xffffffffu, best, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-        if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
-      }
-      if (tid == 0) { red_v[0] = best; red_i[0] = bi; piv[k] = bi; }
+    const double* colk = s.col + (k & 1) * n;
+    double* coln = s.col + ((k + 1) & 1) * n;
+    double best = s.cand_v[0];
+    int p = s.cand_i[0];
+    for (int g = 1; g < R; ++g) {
+      const double v = s.cand_v[g];
+      const int i = s.cand_i[g];
+      if (v > best || (v == best && i < p)) { best = v; p = i; }
     }
-    __syncthreads();
-    const int pr = red_i[0];
-    if (pr != k) {
-      for (int j = tid; j < n; j += nt) {
-        const double t = a[k * lda + j];
-        a[k * lda + j] = a[pr * lda + j];
-        a[pr * lda + j] = t;
-      }
-    }
-    __syncthreads();
-    const double pivot = a[k * lda + k];
-    if (pivot == 0.0) {
-      if (tid == 0) *flag = k + 1;
-      __syncthreads();
-      return k + 1;
-    }
+    const double pivot = colk[p];
+    if (pivot == 0.0) return k + 1;
     const double inv = 1.0 / pivot;
-    // column k (original values) for the elimination
-    for (int i = tid; i < n; i += nt) col[i] = a[i * lda + k];
+    if (own && r0 == 0) {
+      const double x = a[p * lda + j];
+      s.prow[j] = (j == k) ? inv : x * inv;
+      a[p * lda + j] = a[k * lda + j];
+    }
+    if (tid == 0) s.piv[k] = p;
     __syncthreads();
-    for (int j = tid; j < n; j += nt) a[k * lda + j] = (j == k) ? inv : a[k * lda + j] * inv;
-    __syncthreads();
-    for (int e = tid; e < n * n; e += nt) {
-      const int i = e / n, j = e % n;
-      if (i == k) continue;
-      const double f = col[i];
-      if (j == k) a[i * lda + k] = -f * inv;
-      else a[i * lda + j] -= f * a[k * lda + j];
+    if (own) {
+      const double pj = s.prow[j];
+      const double fk = colk[k];
+      double nb = -1.0;
+      int ni = k + 1;
+      for (int i = r0; i < n; i += R) {
+        double v;
+        if (i == k) {
+          v = pj;
+        } else {
+          const double f = (i == p) ? fk : colk[i];
+          v = (j == k) ? -f * inv : a[i * lda + j] - f * pj;
+        }
+        a[i * lda + j] = v;
+        if (j == k + 1) {
+          coln[i] = v;
+          if (i > k && fabs(v) > nb) { nb = fabs(v); ni = i; }
+        }
+      }
+      if (j == k + 1) {
+        s.cand_v[r0] = nb;
+        s.cand_i[r0] = ni;
+      }
     }
     __syncthreads();
   }
-  // undo the row interchanges as column interchanges, last first
-  for (int k = n - 1; k >= 0; --k) {
-    const int pr = piv[k];
-    if (pr != k) {
-      for (int i = tid; i < n; i += nt) {
+  // undo the row interchanges as column interchanges, last first; one thread per row
+  for (int i = tid; i < n; i += nt) {
+    for (int k = n - 1; k >= 0; --k) {
+      const int pr = s.piv[k];
+      if (pr != k) {
         const double t = a[i * lda + k];
         a[i * lda + k] = a[i * lda + pr];
         a[i * lda + pr] = t;
       }
     }
-    __syncthreads();
   }
+  __syncthreads();
   return 0;
 }
 
