@@ -67,7 +67,7 @@ def parse():
     ap.add_argument("--quick", action="store_true", help="small shape for a smoke run")
     ap.add_argument("--no-serving", action="store_true", help="skip the batched / served leg")
     ap.add_argument("--kernel", choices=["sketch_bf16", "gkn", "trace", "grouped", "served_trace", "gkn_scaling",
-                                         "ingest", "syev"],
+                                         "ingest", "syev", "inverse"],
                     default=None,
                     help="time one kernel alone (profiling case) instead of the benchmark: the BF16 sketch GEMM "
                          "on --m x --n x (--k + --p) --N with --parts parts, or the persistent row-block Gramian "
@@ -1143,6 +1143,48 @@ def run_ingest(args, dev):
             "file_gbs": round(gb / t_read, 2)}
 
 
+def run_inverse(args, dev):
+    """The one-CTA Gauss-Jordan inverse (mcnla_b200_inverse_batched, the kernel of the Wen-Yin step's
+    2l x 2l solve) on one matrix per launch, n = 16 .. 160: C = M - I / tau with M = [D/2, I/2;
+    -Dg/2, -D/2] from seeded Gram-like D, Dg, as the Wen-Yin trial builds it.  CUDA events around
+    one call from Python, best of 5, so each time includes the host side of the call (tens of us,
+    most of the time at small n); the residual max |C X - I|."""
+    import numpy as np
+    import torch
+    from mcnla_b200 import isvd, _lib
+    ctx = isvd.context(dev)
+    rows = []
+    for n in (16, 32, 64, 96, 128, 160):
+        l = n // 2
+        rng = np.random.default_rng(n)
+        y = rng.standard_normal((4 * l, l)) / np.sqrt(4 * l)
+        d = y.T @ y
+        dg = d @ d
+        eye = np.eye(l)
+        c = np.block([[d / 2 - eye / 0.5, eye / 2], [-dg / 2, -d / 2 - eye / 0.5]])
+        src = torch.as_tensor(c, device=dev)
+        work = src.clone()
+
+        def call():
+            work.copy_(src)
+            _lib.check(ctx.lib.mcnla_b200_inverse_batched(ctx.bind(), n, 1, isvd._ptr(work)), "inverse_batched")
+        call()
+        stream = torch.cuda.current_stream(dev)
+        best = 1e9
+        for _ in range(5):
+            work.copy_(src)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            _lib.check(ctx.lib.mcnla_b200_inverse_batched(ctx.bind(), n, 1, isvd._ptr(work)), "inverse_batched")
+            e1.record(stream)
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        x = work.cpu().numpy()
+        rows.append({"n": n, "ms": round(best, 4), "residual": float(np.abs(c @ x - np.eye(n)).max())})
+    return {"kernel": "k_inverse (one-CTA Gauss-Jordan, the Wen-Yin step's solve)", "rows": rows}
+
+
 def run_syev(args, dev):
     """The batched Jacobi eigensolver (mcnla_b200_syev_batched, descending |lambda|, as the
     orthogonalizer and the formers call it) on sketch Gram matrices Y'Y, Y = A Omega with
@@ -1206,6 +1248,8 @@ def run_kernel_case(args, dev):
         return run_ingest(args, dev)
     if args.kernel == "syev":
         return run_syev(args, dev)
+    if args.kernel == "inverse":
+        return run_inverse(args, dev)
     if args.kernel == "grouped":
         # the grouped batch integrator on --batch-count copies of one shape (m x n, k, p = k/2, N = 8)
         shapes = [dict(sh, k=k, p=k // 2) for sh in synthetic.batch_shapes(args.batch_count, seed=4)]

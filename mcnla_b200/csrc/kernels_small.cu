@@ -13,8 +13,9 @@ namespace {
 constexpr int kSmallThreads = 512;
 constexpr int kSyevThreads = 1024;   // the Jacobi rounds are latency-bound: more warps hide more of it
 constexpr int kMaxSweeps = 40;
-constexpr int kKnNsMaxDim = 80;
-static_assert(2 * MCNLA_B200_MAX_DIM_SKETCH_WENYIN <= kSmallThreads, "cta_gj_inverse needs n <= blockDim.x");   // the matrix-function KN step keeps four padded l x l matrices on chip
+constexpr int kKnNsMaxDim = 80;   // the matrix-function KN step keeps four padded l x l matrices on chip
+constexpr int kGjThreads = 1024;   // the Gauss-Jordan steps are latency-bound: fewer rows per thread per step
+static_assert(2 * MCNLA_B200_MAX_DIM_SKETCH_WENYIN <= kGjThreads, "cta_gj_inverse needs n <= blockDim.x");
 
 // Shared-memory carve-up shared by the one-CTA solvers.
 struct SmemCarve {
@@ -495,7 +496,7 @@ __global__ void __launch_bounds__(GMEM ? kSyevThreads : kSmallThreads)
 // ---------------------------------------------------------------------------
 // Wen-Yin trial
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kSmallThreads) k_wy_trial(int l, const double* dd, double tau, double inv_n,
+__global__ void __launch_bounds__(kGjThreads) k_wy_trial(int l, const double* dd, double tau, double inv_n,
                                                             double* F, double* FN, DevScalars* scal) {
   extern __shared__ __align__(16) char smem_raw[];
   SmemCarve sc(smem_raw);
@@ -678,7 +679,7 @@ __global__ void k_sqrt_vec(int n, const double* w, double* out) {
   for (int i = threadIdx.x + blockIdx.x * blockDim.x; i < n; i += blockDim.x * gridDim.x) out[i] = sqrt(w[i]);
 }
 
-__global__ void __launch_bounds__(kSmallThreads) k_inverse(int n, double* A, DevScalars* scal) {
+__global__ void __launch_bounds__(kGjThreads) k_inverse(int n, double* A, DevScalars* scal) {
   extern __shared__ __align__(16) char smem_raw[];
   SmemCarve sc(smem_raw);
   const int ld = n + 1;
@@ -959,7 +960,7 @@ int launch_wy_trial(Context* c, int l, const double* dd, double tau, double inv_
   const size_t smem = size_t(n) * (n + 1) * 8 + 16 + gj_scratch_bytes(n) + 64;
   if (smem > c->smem_optin) return MCNLA_B200_ERR_UNSUPPORTED;
   MB_CHECK(set_smem(c, reinterpret_cast<const void*>(k_wy_trial), smem));
-  k_wy_trial<<<1, kSmallThreads, smem, c->stream>>>(l, dd, tau, inv_n, F, FN, c->scal);
+  k_wy_trial<<<1, kGjThreads, smem, c->stream>>>(l, dd, tau, inv_n, F, FN, c->scal);
   c->kernels_launched++;
   MB_CHECK_CUDA(cudaGetLastError());
   return MCNLA_B200_OK;
@@ -1093,7 +1094,7 @@ int launch_inverse(Context* c, int n, int batch, double* A) {
   const size_t smem = size_t(n) * (n + 1) * 8 + 16 + gj_scratch_bytes(n) + 64;
   if (smem > c->smem_optin) return MCNLA_B200_ERR_UNSUPPORTED;
   MB_CHECK(set_smem(c, reinterpret_cast<const void*>(k_inverse), smem));
-  k_inverse<<<batch, kSmallThreads, smem, c->stream>>>(n, A, c->scal);
+  k_inverse<<<batch, kGjThreads, smem, c->stream>>>(n, A, c->scal);
   c->kernels_launched++;
   MB_CHECK_CUDA(cudaGetLastError());
   return MCNLA_B200_OK;

@@ -209,6 +209,7 @@ __device__ inline int cta_jacobi_eig(double* a, int lda, double* v, int ldv, int
 
 // Scratch of cta_gj_inverse (shared memory).
 constexpr int kGjMaxGroups = 32;
+constexpr int kGjBatch = 2;
 struct GjScratch {
   int* piv;        // n: the pivot position of each step
   double* col;     // 2 n: the pivot column, double-buffered across steps
@@ -273,18 +274,30 @@ __device__ inline int cta_gj_inverse(double* a, int lda, int n, const GjScratch&
       const double fk = colk[k];
       double nb = -1.0;
       int ni = k + 1;
-      for (int i = r0; i < n; i += R) {
-        double v;
-        if (i == k) {
-          v = pj;
-        } else {
-          const double f = (i == p) ? fk : colk[i];
-          v = (j == k) ? -f * inv : a[i * lda + j] - f * pj;
+      // rows in batches of kGjBatch: all loads of a batch before its stores, so they overlap
+      for (int i0 = r0; i0 < n; i0 += kGjBatch * R) {
+        double x[kGjBatch], f[kGjBatch];
+#pragma unroll
+        for (int u = 0; u < kGjBatch; ++u) {
+          const int i = i0 + u * R;
+          x[u] = 0.0;
+          f[u] = 0.0;
+          if (i < n) {
+            x[u] = a[i * lda + j];
+            f[u] = (i == p) ? fk : colk[i];
+          }
         }
-        a[i * lda + j] = v;
-        if (j == k + 1) {
-          coln[i] = v;
-          if (i > k && fabs(v) > nb) { nb = fabs(v); ni = i; }
+#pragma unroll
+        for (int u = 0; u < kGjBatch; ++u) {
+          const int i = i0 + u * R;
+          if (i < n) {
+            const double v = (i == k) ? pj : ((j == k) ? -f[u] * inv : x[u] - f[u] * pj);
+            a[i * lda + j] = v;
+            if (j == k + 1) {
+              coln[i] = v;
+              if (i > k && fabs(v) > nb) { nb = fabs(v); ni = i; }
+            }
+          }
         }
       }
       if (j == k + 1) {
